@@ -1,0 +1,193 @@
+"""Seeded parity problems shared by the golden-fixture script, the tests and smoke().
+
+Every builder takes ``api`` -- this package, torchls itself, or the oracle
+adapter -- and returns a ``Problem`` built through that API's
+``Problem.add_residual`` with identical arrays, plus the solve options the
+fixture records.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from torchls_b200 import synthetic
+from torchls_b200.residuals import reprojection, se3_between
+
+
+# ---------------------------------------------------------------- residuals used by fixtures
+def point_prior(point, reference):
+    return point - reference
+
+
+def curve_residual(params, x, y):
+    """Exponential decay fit a * exp(-b x) + c - y (Euclidean, bounded)."""
+    return (params[0] * torch.exp(-params[1] * x) + params[2] - y).reshape(1)
+
+
+def rotation_error(rot_i, rot_j, measured):
+    from torchls_b200.geometry import so3_log
+
+    return so3_log(rot_j @ rot_i.T @ measured.T)
+
+
+def alias_residual(a, b, target):
+    """Two slots that may reference the same variable (aliasing)."""
+    return torch.stack((a[0] * b[1] - target[0], a[1] + 2 * b[0] - target[1], a[0] - b[0]))
+
+
+def cam_point_link(cam_offset, point, target):
+    """Joint-group residual: a Euclidean camera offset and a point."""
+    return cam_offset + point - target
+
+
+def cauchy_loss(api, scale=0.05):
+    """rho(s) = c^2 log(1 + s/c^2); rho'' < 0, so the curvature correction is skipped."""
+
+    class CauchyLoss(api.Loss):
+        def evaluate(self, s):
+            c2 = scale**2
+            return c2 * torch.log1p(s / c2), 1 / (1 + s / c2), -1 / (c2 * (1 + s / c2) ** 2)
+
+    return CauchyLoss()
+
+
+def soft_square_loss(api):
+    """rho(s) = s + s^2/4: rho'' > 0 exercises the full Triggs correction."""
+
+    class SoftSquareLoss(api.Loss):
+        def evaluate(self, s):
+            return s + 0.25 * s * s, 1 + 0.5 * s, 0.5 + 0 * s
+
+    return SoftSquareLoss()
+
+
+# ---------------------------------------------------------------- builders
+def ba_small(api, device="cpu", dtype=torch.float64, data=None):
+    data = data if data is not None else synthetic.small_bundle_adjustment(0)
+    return synthetic.build_bundle_adjustment(data, api, device=device, dtype=dtype, loss=api.HuberLoss(0.01))
+
+
+def ba_tiny(api, device="cpu", dtype=torch.float64, loss=True):
+    """4 cameras, 40 points, 3 views: 120 observations (fast per-kernel parity)."""
+    data = synthetic.make_bundle_adjustment(4, 40, 3, seed=7)
+    return synthetic.build_bundle_adjustment(
+        data, api, device=device, dtype=dtype, loss=api.HuberLoss(0.01) if loss else None)
+
+
+def pose_small(api, device="cpu", dtype=torch.float64):
+    data = synthetic.make_pose_graph(80, 300, seed=3, yaw_sigma=0.5)
+    return synthetic.build_pose_graph(data, api, device=device, dtype=dtype)
+
+
+def curve_bounds(api, device="cpu", dtype=torch.float64):
+    g = torch.Generator().manual_seed(5)
+    x = torch.linspace(0, 4, 60, dtype=torch.float64)
+    y = 2.0 * torch.exp(-1.3 * x) + 0.5 + 0.01 * torch.randn(60, generator=g, dtype=torch.float64)
+    p = api.Problem({"params": torch.tensor([[1.0, 0.5, 0.7]], dtype=dtype, device=device)})
+    p.add_residual(curve_residual, ("params", torch.zeros(60, dtype=torch.long)),
+                   x.to(device=device, dtype=dtype), y.to(device=device, dtype=dtype))
+    return p
+
+
+CURVE_BOUNDS = {"params": ([0.0, 0.0, 0.6], [1.8, 5.0, 1.0])}
+
+
+def rotations_small(api, device="cpu", dtype=torch.float64):
+    from torchls_b200.geometry import so3_exp
+
+    g = torch.Generator().manual_seed(11)
+    n = 12
+    truth = so3_exp(0.4 * torch.randn(n, 3, generator=g, dtype=torch.float64))
+    ii, jj = torch.triu_indices(n, n, offset=1)
+    noise = so3_exp(0.01 * torch.randn(len(ii), 3, generator=g, dtype=torch.float64))
+    rel = noise @ truth[jj] @ truth[ii].transpose(-1, -2)
+    init = truth @ so3_exp(0.1 * torch.randn(n, 3, generator=g, dtype=torch.float64))
+    p = api.Problem({"rot": init[1:].to(device=device, dtype=dtype)}, manifolds={"rot": api.SO3Var})
+    free = (ii > 0)
+    p.add_residual(rotation_error, ("rot", ii[free] - 1), ("rot", jj[free] - 1),
+                   rel[free].to(device=device, dtype=dtype), loss=api.HuberLoss(math.radians(2)))
+    p.add_residual(rotation_error, truth[0].to(device=device, dtype=dtype), ("rot", jj[~free] - 1),
+                   rel[~free].to(device=device, dtype=dtype), in_dims=(None, 0, 0))
+    return p
+
+
+def alias_weights(api, device="cpu", dtype=torch.float64, loss=None):
+    g = torch.Generator().manual_seed(13)
+    m = 30
+    vals = torch.randn(6, 2, generator=g, dtype=torch.float64)
+    a = torch.randint(0, 6, (m,), generator=g)
+    b = torch.randint(0, 6, (m,), generator=g)
+    b[:8] = a[:8]  # aliased slots
+    tgt = torch.randn(m, 3, generator=g, dtype=torch.float64)
+    w = torch.rand(m, generator=g, dtype=torch.float64) + 0.5
+    p = api.Problem({"v": vals.to(device=device, dtype=dtype)})
+    p.add_residual(alias_residual, ("v", a), ("v", b), tgt[:, :2].to(device=device, dtype=dtype),
+                   weights=w.to(device=device, dtype=dtype), loss=loss)
+    p.add_residual(point_prior, ("v", torch.arange(6)), torch.zeros(6, 2, dtype=dtype, device=device))
+    return p
+
+
+def joint_groups(api, device="cpu", dtype=torch.float64):
+    """Two Euclidean groups with identical IDs, coupled per observation."""
+    g = torch.Generator().manual_seed(17)
+    n, m = 8, 40
+    off0 = 0.1 * torch.randn(n, 3, generator=g, dtype=torch.float64)
+    pts0 = torch.randn(n, 3, generator=g, dtype=torch.float64)
+    idx = torch.randint(0, n, (m,), generator=g)
+    tgt = torch.randn(m, 3, generator=g, dtype=torch.float64)
+    p = api.Problem({"off": off0.to(device=device, dtype=dtype), "pts": pts0.to(device=device, dtype=dtype)})
+    p.add_residual(cam_point_link, ("off", idx), ("pts", idx), tgt.to(device=device, dtype=dtype))
+    p.add_residual(point_prior, ("off", torch.arange(n)), torch.zeros(n, 3, dtype=dtype, device=device))
+    p.add_residual(point_prior, ("pts", torch.arange(n)), torch.zeros(n, 3, dtype=dtype, device=device))
+    return p
+
+
+# ---------------------------------------------------------------- oracle adapter
+class OracleAPI:
+    """Exposes the oracle through the same Problem / Var / loss names."""
+
+    SE3Var = "se3"
+    SO3Var = "so3"
+    Sim3Var = "sim3"
+    Loss = object
+
+    @staticmethod
+    def HuberLoss(delta):
+        from oracle.model import huber_loss
+
+        return huber_loss(delta)
+
+    class Problem:
+        def __init__(self, parameters, manifolds=None):
+            from oracle.model import OracleProblem
+
+            params = {k: np.asarray(v.detach().cpu().numpy(), dtype=np.float64) for k, v in parameters.items()}
+            self.inner = OracleProblem(params, dict(manifolds or {}))
+
+        def add_residual(self, fn, *args, in_dims=None, loss=None, weights=None, **_):
+            from oracle.model import generic_loss, huber_loss
+
+            conv = []
+            for a in args:
+                if isinstance(a, tuple):
+                    conv.append((a[0], np.asarray(torch.as_tensor(a[1]).cpu().numpy())))
+                else:
+                    conv.append(np.asarray(torch.as_tensor(a).detach().cpu().numpy()))
+            if loss is not None and not isinstance(loss, huber_loss):
+                inner_loss = loss
+
+                def ev(s):
+                    out = inner_loss.evaluate(torch.as_tensor(s))
+                    return tuple(np.broadcast_to(np.asarray(o, dtype=np.float64), s.shape) for o in out)
+
+                loss = generic_loss(ev)
+            w = None if weights is None else np.asarray(torch.as_tensor(weights).cpu().numpy())
+            self.inner.add_residual(fn, *conv, in_dims=in_dims, loss=loss, weights=w)
+            return self
+
+
+def oracle_problem(builder, **kw):
+    return builder(OracleAPI, **kw).inner

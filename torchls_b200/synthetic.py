@@ -1,0 +1,263 @@
+"""Seeded synthetic problems: bundle adjustment and SE(3) pose graphs.
+
+There is no public dataset for these workloads; every problem is generated on
+the CPU from a ``torch.Generator`` seed, in float64, and then moved to the
+requested device. The same arrays feed the CUDA solver, the CPU oracle and the
+reference implementation.
+
+Bundle adjustment (``make_bundle_adjustment``)
+    Cameras: ``num_cameras`` world-to-camera SE(3) poses at angle 2*pi*k/C on
+    a circle of radius ``radius`` at height ``height``, looking at the origin
+    (rows x, y, z of R; z = -c/|c|, x = z cross (0,0,1), y = z cross x).
+    Points: uniform in [-1, 1]^3. Each point is observed by ``views`` distinct
+    cameras chosen uniformly from the candidates (all cameras, or those within
+    ``azimuth_window`` radians of the point's azimuth). Observations are
+    point-major. uv = normalized pinhole projection + N(0, noise^2).
+    Initial values: T0 = T * se3_exp([N(0, tn^2)^3, N(0, rn^2)^3]),
+    P0 = P + N(0, pn^2). Camera 0 is held fixed: it is constant data for its
+    observations and the optimised group holds cameras 1..C-1.
+
+Pose graph (``make_pose_graph``)
+    A 3D random walk of unit steps with yaw increments N(0, yaw^2) and a small
+    vertical drift. Odometry edges (i, i+1) plus loop edges sampled uniformly
+    with replacement among pose pairs (i, j), j > i + 1, with |p_i - p_j| <= 3.
+    Measurements Z = T_i^-1 T_j * se3_exp(noise); initial poses integrate the
+    noisy odometry; pose 0 is held fixed (constant data for its edges).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import torch
+from torch import Tensor
+
+from .geometry import se3_exp, se3_inverse
+
+
+@dataclass
+class BundleAdjustmentData:
+    cameras_true: Tensor  # [C, 4, 4]
+    points_true: Tensor  # [P, 3]
+    cameras_init: Tensor  # [C, 4, 4]
+    points_init: Tensor  # [P, 3]
+    camera_index: Tensor  # [M] int64
+    point_index: Tensor  # [M] int64
+    uv: Tensor  # [M, 2]
+
+    @property
+    def num_observations(self) -> int:
+        return int(self.camera_index.numel())
+
+    def split_fixed_camera(self):
+        """Return (free-camera obs mask, camera-0 obs mask)."""
+        fixed = self.camera_index == 0
+        return ~fixed, fixed
+
+
+def look_at_cameras(num_cameras: int, radius: float = 5.0, height: float = 1.0) -> Tensor:
+    angles = torch.arange(num_cameras, dtype=torch.float64) * (2 * math.pi / num_cameras)
+    centers = torch.stack(
+        (radius * angles.cos(), radius * angles.sin(), torch.full_like(angles, height)), -1
+    )
+    z = -centers / centers.norm(dim=-1, keepdim=True)
+    up = torch.tensor([0.0, 0.0, 1.0], dtype=torch.float64).expand_as(z)
+    x = torch.linalg.cross(z, up)
+    x = x / x.norm(dim=-1, keepdim=True)
+    y = torch.linalg.cross(z, x)
+    rot = torch.stack((x, y, z), dim=-2)
+    trans = -(rot @ centers[..., None]).squeeze(-1)
+    poses = torch.eye(4, dtype=torch.float64).repeat(num_cameras, 1, 1)
+    poses[:, :3, :3] = rot
+    poses[:, :3, 3] = trans
+    return poses
+
+
+def project(poses: Tensor, points: Tensor) -> Tensor:
+    local = (poses[..., :3, :3] @ points[..., None]).squeeze(-1) + poses[..., :3, 3]
+    return local[..., :2] / local[..., 2:3]
+
+
+def make_bundle_adjustment(
+    num_cameras: int = 10,
+    num_points: int = 500,
+    views: int = 8,
+    *,
+    seed: int = 0,
+    azimuth_window: float | None = None,
+    noise: float = 1e-3,
+    translation_noise: float = 0.05,
+    rotation_noise: float = 0.01,
+    point_noise: float = 0.05,
+    radius: float = 5.0,
+    height: float = 1.0,
+) -> BundleAdjustmentData:
+    """Generate one seeded bundle-adjustment problem (float64, CPU)."""
+    if views > num_cameras:
+        raise ValueError("views must not exceed num_cameras")
+    g = torch.Generator().manual_seed(seed)
+    cams = look_at_cameras(num_cameras, radius, height)
+    pts = torch.rand(num_points, 3, generator=g, dtype=torch.float64) * 2 - 1
+    keys = torch.rand(num_points, num_cameras, generator=g, dtype=torch.float64)
+    if azimuth_window is not None:
+        cam_angle = torch.arange(num_cameras, dtype=torch.float64) * (2 * math.pi / num_cameras)
+        pt_angle = torch.atan2(pts[:, 1], pts[:, 0])
+        diff = torch.remainder(cam_angle[None, :] - pt_angle[:, None] + math.pi, 2 * math.pi) - math.pi
+        allowed = diff.abs() <= azimuth_window
+        if bool((allowed.sum(-1) < views).any()):
+            raise ValueError("azimuth window leaves fewer candidate cameras than views")
+        keys = torch.where(allowed, keys, torch.full_like(keys, 2.0))
+    # A uniformly random subset of the allowed cameras: the `views` smallest keys.
+    chosen = keys.topk(views, dim=-1, largest=False).indices
+    cam_idx = chosen.reshape(-1)
+    pt_idx = torch.arange(num_points).repeat_interleave(views)
+    uv = project(cams[cam_idx], pts[pt_idx])
+    uv = uv + noise * torch.randn(uv.shape, generator=g, dtype=torch.float64)
+    perturb = torch.cat(
+        (
+            translation_noise * torch.randn(num_cameras, 3, generator=g, dtype=torch.float64),
+            rotation_noise * torch.randn(num_cameras, 3, generator=g, dtype=torch.float64),
+        ),
+        -1,
+    )
+    cams0 = cams @ se3_exp(perturb)
+    pts0 = pts + point_noise * torch.randn(num_points, 3, generator=g, dtype=torch.float64)
+    return BundleAdjustmentData(cams, pts, cams0, pts0, cam_idx, pt_idx, uv)
+
+
+def small_bundle_adjustment(seed: int = 0) -> BundleAdjustmentData:
+    """10 cameras, 500 points, 8 views each: 4,000 observations."""
+    return make_bundle_adjustment(10, 500, 8, seed=seed)
+
+
+def mid_bundle_adjustment(seed: int = 0) -> BundleAdjustmentData:
+    """256 cameras, 100,000 points, 10 views within +-60 degrees: 1,000,000 observations."""
+    return make_bundle_adjustment(256, 100_000, 10, seed=seed, azimuth_window=math.pi / 3)
+
+
+def build_bundle_adjustment(data: BundleAdjustmentData, api, *, device="cpu", dtype=torch.float64,
+                            loss=None, residual=None):
+    """Build a ``Problem`` with camera 0 fixed, using ``api`` (this package or torchls).
+
+    ``residual`` defaults to this package's built-in :func:`reprojection`.
+    Group "cams" holds cameras 1..C-1; observations of camera 0 form a second
+    residual batch in which the camera is shared constant data.
+    """
+    if residual is None:
+        from .residuals import reprojection as residual
+    free, fixed = data.split_fixed_camera()
+    problem = api.Problem(
+        {
+            "cams": data.cameras_init[1:].to(device=device, dtype=dtype),
+            "points": data.points_init.to(device=device, dtype=dtype),
+        },
+        manifolds={"cams": api.SE3Var},
+    )
+    problem.add_residual(
+        residual,
+        ("cams", data.camera_index[free] - 1),
+        ("points", data.point_index[free]),
+        data.uv[free].to(device=device, dtype=dtype),
+        loss=loss,
+    )
+    if bool(fixed.any()):
+        problem.add_residual(
+            residual,
+            data.cameras_true[0].to(device=device, dtype=dtype),
+            ("points", data.point_index[fixed]),
+            data.uv[fixed].to(device=device, dtype=dtype),
+            in_dims=(None, 0, 0),
+            loss=loss,
+        )
+    return problem
+
+
+@dataclass
+class PoseGraphData:
+    poses_true: Tensor  # [N, 4, 4]
+    poses_init: Tensor  # [N, 4, 4]
+    edge_i: Tensor  # [E]
+    edge_j: Tensor  # [E]
+    measurements: Tensor  # [E, 4, 4]  Z_ij ~ T_i^-1 T_j
+
+
+def make_pose_graph(
+    num_poses: int = 1000,
+    num_loops: int = 3000,
+    *,
+    seed: int = 0,
+    yaw_sigma: float = 0.1,
+    rotation_noise: float = 0.01,
+    translation_noise: float = 0.02,
+    loop_radius: float = 3.0,
+) -> PoseGraphData:
+    g = torch.Generator().manual_seed(seed)
+    yaw = torch.cumsum(yaw_sigma * torch.randn(num_poses, generator=g, dtype=torch.float64), 0)
+    pitch = 0.05 * torch.randn(num_poses, generator=g, dtype=torch.float64)
+    step = torch.stack((yaw.cos() * pitch.cos(), yaw.sin() * pitch.cos(), pitch.sin()), -1)
+    pos = torch.cat((torch.zeros(1, 3, dtype=torch.float64), torch.cumsum(step[:-1], 0)))
+    rot_vec = torch.zeros(num_poses, 3, dtype=torch.float64)
+    rot_vec[:, 2] = yaw
+    tangent = torch.cat((torch.zeros_like(rot_vec), rot_vec), -1)
+    poses = se3_exp(tangent)
+    poses[:, :3, 3] = pos
+    # Loop candidates: pairs within loop_radius, j > i + 1 (vectorised in blocks).
+    cand_i, cand_j = [], []
+    block = 2048
+    for s in range(0, num_poses, block):
+        d = torch.cdist(pos[s : s + block], pos)
+        ii, jj = (d <= loop_radius).nonzero(as_tuple=True)
+        ii = ii + s
+        keep = jj > ii + 1
+        cand_i.append(ii[keep])
+        cand_j.append(jj[keep])
+    cand_i, cand_j = torch.cat(cand_i), torch.cat(cand_j)
+    if cand_i.numel() == 0 and num_loops > 0:
+        raise ValueError("no loop-closure candidates")
+    pick = torch.randint(cand_i.numel(), (num_loops,), generator=g)
+    ei = torch.cat((torch.arange(num_poses - 1), cand_i[pick]))
+    ej = torch.cat((torch.arange(1, num_poses), cand_j[pick]))
+    rel = se3_inverse(poses[ei]) @ poses[ej]
+    noise = torch.cat(
+        (
+            translation_noise * torch.randn(len(ei), 3, generator=g, dtype=torch.float64),
+            rotation_noise * torch.randn(len(ei), 3, generator=g, dtype=torch.float64),
+        ),
+        -1,
+    )
+    meas = rel @ se3_exp(noise)
+    init = [poses[0]]
+    for k in range(num_poses - 1):
+        init.append(init[-1] @ meas[k])
+    return PoseGraphData(poses, torch.stack(init), ei, ej, meas)
+
+
+def build_pose_graph(data: PoseGraphData, api, *, device="cpu", dtype=torch.float64, loss=None,
+                     residual=None):
+    """``Problem`` over poses 1..N-1; pose 0 is constant data in its edges."""
+    if residual is None:
+        from .residuals import se3_between as residual
+    problem = api.Problem(
+        {"poses": data.poses_init[1:].to(device=device, dtype=dtype)},
+        manifolds={"poses": api.SE3Var},
+    )
+    free = (data.edge_i > 0) & (data.edge_j > 0)
+    problem.add_residual(
+        residual,
+        ("poses", data.edge_i[free] - 1),
+        ("poses", data.edge_j[free] - 1),
+        data.measurements[free].to(device=device, dtype=dtype),
+        loss=loss,
+    )
+    first = data.edge_i == 0
+    if bool(first.any()):
+        problem.add_residual(
+            residual,
+            data.poses_true[0].to(device=device, dtype=dtype),
+            ("poses", data.edge_j[first] - 1),
+            data.measurements[first].to(device=device, dtype=dtype),
+            in_dims=(None, 0, 0),
+            loss=loss,
+        )
+    return problem
