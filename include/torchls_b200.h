@@ -1,0 +1,359 @@
+/*
+ * torchls_b200 -- C ABI of the B200 (sm_100a) block-sparse LM/GN inner loop.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t and
+ * returns an int status (TLS_OK = 0). Nothing here allocates device memory:
+ * callers pass every buffer and workspace. Calls are asynchronous on `stream`
+ * unless stated otherwise; there is no global mutable state except the
+ * thread-local last-error message.
+ *
+ * Layout conventions (shared by all calls):
+ *   tangent vector   : variable groups in declaration order; group g occupies
+ *                      [offset_g, offset_g + count_g * dim_g), variable i at
+ *                      offset_g + i * dim_g  (torchls variables.py:100-117).
+ *   Jacobian (jac)   : per factor group, structure-of-arrays [r * D][N]:
+ *                      element (row i, column c) of factor f at
+ *                      (i * D + c) * N + f, columns grouped by slot.
+ *   residuals        : per factor group, factor-major [N][r] float64.
+ *   contributions    : per factor group, factor-major [N][W] (W = D for
+ *                      vectors, sum_s d_s (d_s + 1) / 2 for Gram blocks).
+ *   segments         : CSR lists of contribution offsets per target
+ *                      (variable or Schur edge); reductions follow list order,
+ *                      so every result is deterministic (no atomics).
+ */
+#ifndef TORCHLS_B200_H
+#define TORCHLS_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TLS_API __attribute__((visibility("default")))
+#else
+#define TLS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* tls_stream_t; /* == cudaStream_t */
+
+enum {
+  TLS_OK = 0,
+  TLS_ERR_INVALID = 1,   /* bad argument; maps to ValueError */
+  TLS_ERR_CUDA = 2,      /* CUDA launch/runtime error */
+  TLS_ERR_UNSUPPORTED = 3,
+  TLS_ERR_NOT_PD = 4     /* a damped block is not positive definite; maps to LinAlgError */
+};
+
+enum { TLS_F32 = 0, TLS_F64 = 1 };
+
+enum {
+  TLS_LOSS_NONE = 0,     /* plain least squares */
+  TLS_LOSS_HUBER = 1,    /* Huber on the block squared norm (torchls losses.py:56-107) */
+  TLS_LOSS_GENERIC = 2   /* caller supplies rho', rho'' per factor (losses.py:30-50) */
+};
+
+enum {
+  TLS_RES_PACKED = 0,       /* residual + blocks supplied by the caller (torch.func path) */
+  TLS_RES_REPROJECTION = 1, /* depth-guarded normalized pinhole reprojection, r = 2 */
+  TLS_RES_SE3_BETWEEN = 2,  /* log(Z^-1 Ti^-1 Tj), r = 6 */
+  TLS_RES_SIM3_BETWEEN = 3  /* log(Z^-1 Si^-1 Sj), r = 7 */
+};
+
+enum { TLS_KIND_EUCLIDEAN = 0, TLS_KIND_SO3 = 1, TLS_KIND_SE3 = 2, TLS_KIND_SIM3 = 3, TLS_KIND_SE2 = 4 };
+
+#define TLS_MAX_SLOTS 8
+#define TLS_MAX_GROUPS 8
+#define TLS_MAX_FACTOR_GROUPS 16
+
+typedef struct tls_var_group {
+  int64_t offset; /* tangent offset */
+  int32_t count;  /* number of variables */
+  int32_t dim;    /* tangent dim */
+} tls_var_group;
+
+typedef struct tls_factor_group {
+  int64_t count;                            /* N factors */
+  int32_t rdim;                             /* residual dim r */
+  int32_t nslots;                           /* variable slots S */
+  int32_t total_dim;                        /* D = sum of slot dims */
+  int32_t jac_dtype;                        /* TLS_F32 / TLS_F64 */
+  int32_t slot_group[TLS_MAX_SLOTS];        /* variable group per slot */
+  int32_t slot_dim[TLS_MAX_SLOTS];
+  int32_t slot_col[TLS_MAX_SLOTS];          /* first column of the slot inside D */
+  int32_t slot_gram[TLS_MAX_SLOTS];         /* first Gram entry of the slot inside W */
+  const int32_t* index[TLS_MAX_SLOTS];      /* [N] variable index (within its group) */
+  void* jac;                                /* [r*D][jac_stride] SoA */
+  int64_t jac_stride;                       /* leading dimension of jac (0: count) */
+} tls_factor_group;
+
+/* A deterministic segmented reduction: target t sums src[ptr[t]..ptr[t+1])
+ * blocks of `width` values from a contribution buffer, in list order. */
+typedef struct tls_segments {
+  int32_t count;       /* targets */
+  int32_t width;       /* values per contribution block */
+  int32_t lanes;       /* lanes cooperating per target (1..32, power of two) */
+  int32_t pad_;
+  const int32_t* ptr;  /* [count + 1] */
+  const int32_t* src;  /* [nnz] element offset of each block */
+} tls_segments;
+
+/* ---------------------------------------------------------------- linearization
+ * Replaces: torchls linearization.py:62-128 (vmap(jacrev) + loss transform),
+ * problem.py:157-221 (weights, gather) and the per-linearization halves of
+ * sparse.py:43-55 (J^T r) and sparse.py:104-121 / warp_diagonal.py:14-66
+ * (Gram blocks). One kernel per factor group writes J (SoA, jac_dtype), the
+ * model and raw residuals, the per-factor objective, and FP64 per-factor
+ * gradient and Gram contributions (aliased slots include their cross terms).
+ */
+typedef struct tls_linearize_args {
+  tls_factor_group fg;
+  int32_t residual_kind;      /* TLS_RES_* */
+  int32_t loss_kind;          /* TLS_LOSS_* */
+  double loss_delta;          /* Huber delta */
+  int32_t has_loss;           /* problem-level: any loss or weights (problem.py:264-270) */
+  int32_t want_jacobian;      /* 0: residual/objective only (trial evaluation) */
+  /* residual inputs; for TLS_RES_PACKED `packed_blocks[s]` are [N][r][d_s] and
+   * `packed_residual` is [N][r], in float64 */
+  const double* packed_residual;
+  const double* packed_blocks[TLS_MAX_SLOTS];
+  /* built-in residual arguments: per argument position, a float64 pointer and
+   * a per-factor stride in doubles (0 broadcasts one value to every factor);
+   * variable arguments point at the group's value storage and use the slot's
+   * index array; `arg_slot[a]` is the slot of argument a, or -1 for data. */
+  const double* arg_data[4];
+  int64_t arg_stride[4];
+  int32_t arg_slot[4];
+  const double* weights;      /* [N] or NULL */
+  const double* rho1;         /* generic loss: rho'(s) per factor */
+  const double* rho2;         /* generic loss: rho''(s) per factor */
+  /* outputs (any may be NULL when not wanted) */
+  double* residual;           /* [N][r] model residual */
+  double* raw_residual;       /* [N][r] */
+  double* squared_norm;       /* [N] s = |r_raw|^2 */
+  double* objective;          /* [N] w * rho(s) (or s) */
+  double* grad_contrib;       /* [N][D] */
+  double* gram_contrib;       /* [N][W] */
+  /* Schur cross blocks J_s^T (sum of eliminated slots) for every retained slot
+   * s with slot_cross[s] >= 0, written at cross_contrib[f*cross_width + slot_cross[s]]
+   * as a (d_s x elim_dim) row-major block (schur.py:213-224). */
+  int32_t elim_mask;          /* bitmask of eliminated slots (0: none) */
+  int32_t elim_dim;
+  int32_t slot_cross[TLS_MAX_SLOTS];
+  int32_t cross_width;
+  int32_t pad2_;
+  double* cross_contrib;      /* [N][cross_width] or NULL */
+} tls_linearize_args;
+
+TLS_API int tls_linearize(const tls_linearize_args* args, tls_stream_t stream);
+
+/* Segmented reduction to dense outputs.
+ * mode 0: vector targets, out[t*width + k] (out_dtype).
+ * mode 1: packed-upper Gram targets of dimension d -> out[t][d][d] float64,
+ *         symmetrised. */
+TLS_API int tls_segment_reduce(const tls_segments* seg, const void* contrib, int32_t contrib_dtype,
+                       int32_t mode, int32_t dim, void* out, int32_t out_dtype, tls_stream_t stream);
+
+/* ---------------------------------------------------------------- normal operator
+ * Replaces: torchls sparse.py:83-84 BlockJacobian.normal_matvec and
+ * warp_normal.py:125-294 WarpNormalPlan(J).bind(J).normal_matvec(v, damping).
+ * y = diag(s) J^T J diag(s) x + damping * x, deterministic.
+ * `contrib` is a caller workspace of sum_k N_k * D_k elements of vec_dtype.
+ */
+typedef struct tls_normal_args {
+  int32_t nfactor_groups;
+  int32_t nvar_groups;
+  int32_t vec_dtype;          /* x, y, scale dtype */
+  int32_t pad_;
+  tls_factor_group fg[TLS_MAX_FACTOR_GROUPS];
+  int64_t contrib_offset[TLS_MAX_FACTOR_GROUPS];  /* element offset of group k in contrib */
+  tls_var_group vg[TLS_MAX_GROUPS];
+  tls_segments seg[TLS_MAX_GROUPS];               /* width = dim_g; src offsets into contrib */
+  const void* scale;          /* [n] or NULL */
+  void* contrib;
+  double damping;
+} tls_normal_args;
+
+TLS_API int tls_normal_matvec(const tls_normal_args* args, const void* x, void* y, tls_stream_t stream);
+
+/* J diag(s) x per factor row -> out [rows] (factor groups concatenated,
+ * factor-major [N][r]); replaces sparse.py:31-41 BlockJacobian.matvec. */
+TLS_API int tls_jacobian_matvec(const tls_normal_args* args, const void* x, void* out_rows, tls_stream_t stream);
+
+/* sum_f |J_f diag(s) x|^2 in float64 (x float64), written to *out (device);
+ * replaces sparse.py:57-81 squared_matvec_norm. `partials` holds at least
+ * ceil(N_k / 128) doubles for the largest factor group. */
+TLS_API int tls_squared_matvec_norm(const tls_normal_args* args, const double* x, double* partials,
+                            double* out, tls_stream_t stream);
+
+/* J^T u (times diag(s) when scale is set) for u in factor-major row layout,
+ * through the contribution workspace; replaces sparse.py:43-55 rmatvec. */
+TLS_API int tls_jacobian_rmatvec(const tls_normal_args* args, const void* rows, void* out, tls_stream_t stream);
+
+/* ---------------------------------------------------------------- block Jacobi
+ * Replaces: solvers.py:259-285 block_jacobi, preconditioning.py:12-17,117-134.
+ * A block group is `count` blocks of dimension `dim` whose columns are the
+ * concatenation of up to 4 member ranges (joint groups, preconditioning.py:47-88).
+ */
+typedef struct tls_block_group {
+  int32_t count;
+  int32_t dim;
+  int32_t nmembers;
+  int32_t pad_;
+  int64_t member_offset[4];   /* tangent offset of each member group */
+  int32_t member_dim[4];
+  const double* blocks;       /* [count][dim][dim] float64 */
+  double* factor;             /* [count][dim][dim] float64 lower Cholesky factor */
+  const double* scale;        /* full-vector column scale s: factor of s B s + damping I; or NULL */
+} tls_block_group;
+
+/* factor[i] = chol(S blocks[i] S + damping * I), S = diag of `scale` over the
+ * block's columns (identity when NULL). Writes the number of blocks that
+ * are not positive definite (or non-finite) to *bad (device int32). */
+TLS_API int tls_block_cholesky(const tls_block_group* groups, int32_t ngroups, double damping,
+                       int32_t* bad, tls_stream_t stream);
+
+/* z = (L L^T)^-1 r per block; r, z of vec_dtype, arithmetic in float64. */
+TLS_API int tls_block_solve(const tls_block_group* groups, int32_t ngroups, const void* r, void* z,
+                    int32_t vec_dtype, tls_stream_t stream);
+
+/* ---------------------------------------------------------------- PCG
+ * Replaces: solvers.py:167-256 pcg and warp_pcg.py:33-214. The state machine
+ * mirrors torchls's PCG step for step (true-residual checks, adaptive or
+ * periodic restarts, reason codes); all decisions are taken on the device
+ * from float64 scalars, so iterations need no host synchronisation.
+ */
+enum { TLS_PCG_ACTIVE = 0, TLS_PCG_CONVERGED = 1, TLS_PCG_NONFINITE = 2,
+       TLS_PCG_NONPOSITIVE = 3, TLS_PCG_MAX_ITERATIONS = 4 };
+
+typedef struct tls_pcg_control {
+  /* host-visible result, float64 scalars first */
+  double rhs_norm, threshold, residual_norm;
+  double rz, curvature, alpha, beta, rz_new, rr, true_rr, drift_rr, rz_true;
+  int32_t iterations, status, restarts, checks;
+  int32_t mode, stop_at, max_iterations, check_interval;
+  int32_t periodic, pad_[3];
+  double drift_tolerance;
+  uint32_t ticket[4];
+} tls_pcg_control;
+
+typedef struct tls_schur_args tls_schur_args;
+
+typedef struct tls_pcg_args {
+  int64_t n;
+  int32_t vec_dtype;
+  int32_t op_kind;               /* 0: normal operator, 1: Schur reduced operator */
+  const tls_normal_args* normal; /* op_kind 0 */
+  const tls_schur_args* schur;   /* op_kind 1 */
+  const tls_block_group* pre;    /* preconditioner blocks, or NULL (identity) */
+  int32_t npre;
+  int32_t pad_;
+  const void* rhs;
+  void *x, *r, *z, *p, *ap, *ztrue, *psave;   /* [n] workspaces of vec_dtype */
+  double* partials;              /* >= 65536 + 3 * 1024 doubles */
+  tls_pcg_control* control;      /* device buffer of tls_pcg_state_bytes() bytes */
+} tls_pcg_args;
+
+/* Initialise: x = 0, r = rhs, norms, threshold = max(atol, rtol |rhs|),
+ * z = M r, p = z, rz. */
+TLS_API int tls_pcg_start(const tls_pcg_args* args, double rtol, double atol, int32_t max_iterations,
+                  int32_t check_interval, int32_t periodic, double drift_tolerance, tls_stream_t stream);
+
+/* Run `steps` state-machine steps (each = one operator application plus its
+ * vector updates); steps after termination leave x unchanged. Launches only:
+ * a sequence of calls can be captured into a CUDA graph. */
+TLS_API int tls_pcg_run(const tls_pcg_args* args, int32_t steps, tls_stream_t stream);
+
+/* Size in bytes of the device control block (tls_pcg_control first). */
+TLS_API int tls_pcg_state_bytes(void);
+
+/* ---------------------------------------------------------------- Schur complement
+ * Replaces: schur.py:192-397 (SchurLinearization, DampedSchurSystem) for one
+ * retained group of dimension dr <= 8 and an eliminated group of dimension
+ * de <= 4. Edges (retained i, eliminated p) are stored in a chunked order:
+ * each chunk holds whole eliminated variables; inside a chunk edges are sorted
+ * by retained variable so that retained sums are contiguous runs. Every
+ * reduction follows a fixed order (deterministic).
+ */
+struct tls_schur_args {
+  int32_t nedges;
+  int32_t nchunks;
+  int32_t dr, de;
+  int32_t nretained;            /* retained variables */
+  int32_t nelim;                /* eliminated variables */
+  int32_t wdtype;               /* TLS_F32 / TLS_F64 storage of W */
+  int32_t vec_dtype;            /* reduced vectors */
+  int32_t max_chunk_edges;      /* shared memory: max_chunk_edges * (dr + de) doubles */
+  int32_t nruns;
+  int64_t retained_offset;      /* tangent offset of the retained group (full vector) */
+  int64_t elim_offset;          /* tangent offset of the eliminated group (full vector) */
+  const int32_t* chunk_ptr;     /* [nchunks+1] edge ranges */
+  const int32_t* chunk_run_ptr; /* [nchunks+1] run ranges */
+  const int32_t* edge_r;        /* [E] retained variable per edge (chunk order) */
+  const int32_t* edge_e;        /* [E] eliminated variable per edge */
+  const int32_t* elim_ptr;      /* [nelim+1] CSR: edges of each eliminated variable */
+  const int32_t* elim_edges;    /* [E] edge positions, ascending */
+  const int32_t* run_ptr;       /* [nruns+1] edge ranges of equal retained variable */
+  const int32_t* rrun_ptr;      /* [nretained+1] CSR: runs of each retained variable */
+  const int32_t* rrun_list;     /* [nruns] run ids in chunk order */
+  const double* cross;          /* [E][dr][de] J_r^T J_e per edge (unscaled) */
+  const double* elim_diag;      /* [nelim][de][de] eliminated diagonal blocks (unscaled) */
+  const double* ret_diag;       /* [nretained][dr][dr] retained diagonal blocks (unscaled) */
+  const double* scale;          /* [n_full] column scale or NULL */
+  double* inv_l;                /* [nelim][de][de] L^-1, L = chol(s C s + lambda I) */
+  void* w;                      /* [dr*de][E] whitened W (SoA, wdtype) */
+  double* run_partial;          /* [nruns][dr] workspace */
+  double* ybuf;                 /* [nelim][de] workspace: L^-1 b_e */
+  double damping;
+  int32_t* bad;                 /* device: number of non-PD eliminated blocks */
+};
+
+/* Factor eliminated blocks and whiten every edge (schur.py:263-283). */
+TLS_API int tls_schur_damp(const tls_schur_args* a, tls_stream_t stream);
+/* out = (s U s + lambda I) x - W W^T x on the reduced vector (schur.py:303-328). */
+TLS_API int tls_schur_matvec(const tls_schur_args* a, const void* x, void* out, tls_stream_t stream);
+/* rhs_c = b_c - W (L^-1 b_e); stores y_e = L^-1 b_e in a->ybuf (schur.py:285-290).
+ * b is the full scaled right-hand side (float64, full tangent layout). */
+TLS_API int tls_schur_reduced_rhs(const tls_schur_args* a, const double* b, void* rhs_c, tls_stream_t stream);
+/* delta_e = L^-T (y_e - W^T x_c); writes the full tangent step (schur.py:292-301). */
+TLS_API int tls_schur_backsubstitute(const tls_schur_args* a, const void* x_c, double* delta_full,
+                             tls_stream_t stream);
+/* Preconditioner blocks s U s - sum_e W_e W_e^T -> out [nretained][dr][dr]
+ * (schur.py:353-363); the damping is added by tls_block_cholesky. */
+TLS_API int tls_schur_preconditioner_blocks(const tls_schur_args* a, double* out, tls_stream_t stream);
+
+/* ---------------------------------------------------------------- retraction
+ * Replaces: variables.py:153-160 / 242-249 with geometry.py:40-160 retractions.
+ * out[i] = values[i] * Exp(delta[i]) (right update) for Lie groups,
+ * values + delta for Euclidean. Storage float64: SO3 [3][3], SE3/Sim3 [4][4],
+ * SE2 [3]. Optional clamping to [lower, upper] (Euclidean only, bounds.py:61-75)
+ * rewrites delta_out with the effective step. */
+TLS_API int tls_retract(int32_t kind, int32_t count, int32_t dim, const double* values, const double* delta,
+                double* out, const double* lower, const double* upper, double* delta_out,
+                tls_stream_t stream);
+
+/* ---------------------------------------------------------------- reductions
+ * Deterministic float64 sums used by the LM driver (cost, trial reduction,
+ * gradient norms). `partials` holds >= 1024 doubles. */
+enum { TLS_SUM_PLAIN = 0, TLS_SUM_SQUARES = 1, TLS_SUM_ABSMAX = 2 };
+TLS_API int tls_reduce(const void* x, int32_t dtype, int64_t n, int32_t op, double* partials, double* out,
+               tls_stream_t stream);
+
+/* Trial objective and exact reduction per factor group (problem.py:315-348,
+ * losses.py:92-107): adds 0.5 * sum w*rho(s_new) and 0.5 * sum w*reduction to
+ * out[0], out[1] (device). old/new raw residuals are [N][r] float64. */
+TLS_API int tls_trial_terms(int64_t count, int32_t rdim, const double* old_raw, const double* new_raw,
+                    int32_t loss_kind, double delta, const double* rho_old, const double* rho_new,
+                    const double* weights, int32_t has_loss, double* partials, double* out,
+                    tls_stream_t stream);
+
+/* ---------------------------------------------------------------- misc */
+TLS_API const char* tls_last_error(void);
+TLS_API int tls_version(void);
+TLS_API int tls_device_init(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TORCHLS_B200_H */

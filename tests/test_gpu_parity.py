@@ -1,0 +1,175 @@
+"""CUDA path vs fixtures produced by torchls itself (float64) and vs the oracle.
+
+Tolerances: float64 CUDA results match the reference to 1e-12 relative for
+per-linearization quantities and 1e-10 relative for final costs; parameters to
+1e-8 (the reference's own final-iterate precision). Mixed precision (float32
+Jacobian and PCG vectors, float64 reductions) must reach the float64 final
+cost within 1e-8 relative.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_helpers import SUMMARIES, check_summary, close, load, needs_gpu, stored_ba, to_np
+from golden import problems as P
+
+pytestmark = [pytest.mark.gpu, needs_gpu]
+
+DEV = "cuda"
+
+
+@pytest.fixture(scope="module")
+def tls():
+    import torchls_b200
+
+    return torchls_b200
+
+
+@pytest.fixture(scope="module")
+def ba(tls):
+    fx = load("ba_small")
+    prob = P.ba_small(tls, device=DEV, data=stored_ba(fx))
+    return fx, prob
+
+
+def test_ba_linearization(tls, ba):
+    fx, prob = ba
+    lin = prob.linearize()
+    close(lin.residual, fx["residual"], 1e-12, what="residual")
+    close(lin.raw_residual, fx["raw_residual"], 1e-12, what="raw")
+    close(lin.cost, fx["cost"], 1e-13, what="cost")
+    close(lin.gradient, fx["gradient"], 1e-11, what="gradient")
+    for i, d in enumerate(lin.jacobian.diagonal_blocks()):
+        close(d, fx[f"diag{i}"], 1e-11, what=f"diag{i}")
+    for gi, g in enumerate(lin.jacobian.groups):
+        for si, b in enumerate(g.blocks):
+            close(b, fx[f"block{gi}_{si}"], 1e-11, what=f"block{gi}_{si}")
+
+
+def test_ba_products_and_determinism(tls, ba):
+    fx, prob = ba
+    J = prob.linearize().jacobian
+    v = torch.from_numpy(fx["v"]).to(DEV)
+    u = torch.from_numpy(fx["u"]).to(DEV)
+    y1 = J.normal_matvec(v, 1e-3)
+    close(y1, fx["normal_matvec"], 1e-12, what="normal_matvec")
+    assert torch.equal(y1, J.normal_matvec(v, 1e-3)), "normal matvec is not bitwise reproducible"
+    close(J.matvec(v), fx["matvec"], 1e-12, what="matvec")
+    close(J.rmatvec(u), fx["rmatvec"], 1e-12, what="rmatvec")
+    close(J.squared_matvec_norm(v), fx["squared_matvec_norm"], 1e-12, what="sqnorm")
+    apply = tls.block_jacobi(J, 1e-3)
+    close(apply(v), fx["block_jacobi_apply"], 1e-10, what="block_jacobi")
+
+
+def test_ba_device_pcg(tls, ba):
+    from functools import partial
+
+    fx, prob = ba
+    lin = prob.linearize()
+    J = lin.jacobian
+    res = tls.pcg(partial(J.normal_matvec, damping=1e-3), -lin.gradient, preconditioner=tls.block_jacobi(J, 1e-3),
+                  config=tls.ConjugateGradientConfig())
+    ref = SUMMARIES["ba_small_pcg"]
+    assert (res.iterations, res.reason, res.restarts, res.residual_checks) == (
+        ref["iterations"], ref["reason"], ref["restarts"], ref["residual_checks"])
+    close(res.solution, fx["pcg_solution"], 1e-8, what="pcg solution")
+    close(res.rhs_norm, ref["rhs_norm"], 1e-12, what="rhs_norm")
+
+
+def test_ba_schur_system(tls, ba):
+    from torchls_b200.schur import SchurLinearization, SchurPlan
+
+    fx, prob = ba
+    an = prob._ensure_analyzed()
+    plan = SchurPlan(an, "points", torch.device(DEV))
+    np.testing.assert_array_equal(to_np(plan.edges[0][0]), fx["schur_edges_r"])
+    np.testing.assert_array_equal(to_np(plan.edges[0][1]), fx["schur_edges_e"])
+    lin = prob.linearize(schur=plan)
+    raw = lin.jacobian.diagonal_blocks()
+    slin = SchurLinearization(plan, lin, raw, None, wdtype=torch.float64, vec_dtype=torch.float64)
+    cross_ref = fx["schur_cross"][plan.order]
+    close(slin.cross, cross_ref, 1e-12, what="cross")
+    sys_ = slin.damped(1e-3)
+    close(sys_.reduced_rhs(-lin.gradient), fx["schur_reduced_rhs"], 1e-11, what="reduced_rhs")
+    vc = torch.from_numpy(fx["vc"]).to(DEV)
+    close(sys_.matvec(vc), fx["schur_matvec"], 1e-11, what="schur matvec")
+    close(sys_.preconditioner()(vc), fx["schur_preconditioner"], 1e-10, what="schur preconditioner")
+    close(sys_.backsubstitute(vc), fx["schur_backsubstitute"], 1e-11, what="backsubstitute")
+    close(sys_.dense_matrix(), fx["schur_dense"], 1e-11, what="dense")
+
+
+BA_RUNS = {
+    "schur_cg": dict(linear_solver="schur_cg", eliminate="points", record_trials=True),
+    "conjugate_gradient": dict(linear_solver="conjugate_gradient"),
+    "schur_dense": dict(linear_solver="schur_dense", eliminate="points"),
+    "scaled_adaptive": dict(linear_solver="schur_cg", eliminate="points", jacobi_scaling=True,
+                            trust_region=dict(strategy="adaptive", damping_mode="diagonal")),
+}
+
+
+@pytest.mark.parametrize("run", list(BA_RUNS))
+def test_ba_solve(tls, run):
+    fx = load("ba_small")
+    opts = dict(BA_RUNS[run])
+    if "trust_region" in opts:
+        opts["trust_region"] = tls.TrustRegionConfig(**opts["trust_region"])
+    prob = P.ba_small(tls, device=DEV, data=stored_ba(fx))
+    sol, s = prob.solve(return_summary=True, termination=tls.TerminationConfig(max_iterations=30), **opts)
+    check_summary(s, SUMMARIES[f"ba_small_{run}"])
+    close(sol["cams"], fx[f"solve_{run}_cams"], 1e-8, what="cams")
+    close(sol["points"], fx[f"solve_{run}_points"], 1e-8, what="points")
+
+
+def test_ba_mixed_precision_reaches_fp64_cost(tls):
+    fx = load("ba_small")
+    prob = P.ba_small(tls, device=DEV, data=stored_ba(fx))
+    cfg = tls.ConjugateGradientConfig(precision="mixed")
+    _, s = prob.solve(return_summary=True, linear_solver="schur_cg", eliminate="points", conjugate_gradient=cfg,
+                      termination=tls.TerminationConfig(max_iterations=30))
+    ref = SUMMARIES["ba_small_schur_cg"]["final_cost"]
+    assert abs(s.final_cost - ref) <= 1e-8 * ref, (s.final_cost, ref)
+
+
+OTHERS = {
+    "ba_tiny": (P.ba_tiny, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_tiny_gn": (P.ba_tiny, dict(linear_solver="conjugate_gradient", trust_region=None,
+                                   termination=dict(max_iterations=8))),
+    "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
+    "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
+    "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
+        lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
+    "alias_weights": (P.alias_weights, dict()),
+    "alias_cauchy": (lambda api, **k: P.alias_weights(api, loss=P.cauchy_loss(api), **k), dict()),
+    "alias_softsq": (lambda api, **k: P.alias_weights(api, loss=P.soft_square_loss(api), **k), dict()),
+    "joint_groups": (P.joint_groups, dict(conjugate_gradient=dict(preconditioner_groups=(("off", "pts"),)))),
+}
+
+
+@pytest.mark.parametrize("name", list(OTHERS))
+def test_other_problems(tls, name):
+    builder, opts = OTHERS[name]
+    opts = dict(opts)
+    if "termination" in opts:
+        opts["termination"] = tls.TerminationConfig(**opts["termination"])
+    if isinstance(opts.get("trust_region"), dict):
+        opts["trust_region"] = tls.TrustRegionConfig(**opts["trust_region"])
+    if "conjugate_gradient" in opts:
+        opts["conjugate_gradient"] = tls.ConjugateGradientConfig(**opts["conjugate_gradient"])
+    fx = load(name)
+    lin = builder(tls, device=DEV).linearize()
+    close(lin.residual, fx["residual"], 1e-11, 1e-15, what="residual")
+    close(lin.gradient, fx["gradient"], 1e-10, 1e-13, what="gradient")
+    for i, d in enumerate(lin.jacobian.diagonal_blocks()):
+        close(d, fx[f"diag{i}"], 1e-10, 1e-13, what=f"diag{i}")
+    for gi, g in enumerate(lin.jacobian.groups):
+        for si, (b, c) in enumerate(zip(g.blocks, g.columns)):
+            close(b, fx[f"block{gi}_{si}"], 1e-10, 1e-13, what=f"block{gi}_{si}")
+            np.testing.assert_array_equal(to_np(c), fx[f"columns{gi}_{si}"])
+    prob = builder(tls, device=DEV)
+    sol, s = prob.solve(return_summary=True, **opts)
+    check_summary(s, SUMMARIES[name])
+    for key, val in sol.items():
+        close(val, fx[f"solve_{key}"], 1e-7, 1e-12, what=key)

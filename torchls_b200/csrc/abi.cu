@@ -1,0 +1,27 @@
+// C-ABI plumbing: error reporting and version.
+#include <stdio.h>
+#include <string.h>
+
+#include "common.cuh"
+
+static thread_local char g_last_error[512] = "";
+
+int tls_set_error(int code, const char* msg) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+  return code;
+}
+
+int tls_set_cuda_error(cudaError_t e) {
+  snprintf(g_last_error, sizeof(g_last_error), "CUDA error: %s", cudaGetErrorString(e));
+  return TLS_ERR_CUDA;
+}
+
+extern "C" const char* tls_last_error(void) { return g_last_error; }
+
+extern "C" int tls_version(void) { return 1; }
+
+extern "C" int tls_device_init(int32_t device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return tls_set_cuda_error(e);
+  return TLS_OK;
+}

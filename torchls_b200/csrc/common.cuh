@@ -1,0 +1,72 @@
+// Shared device helpers for the torchls_b200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "torchls_b200.h"
+
+#define TLS_CHECK_LAUNCH()                                   \
+  do {                                                       \
+    cudaError_t _e = cudaGetLastError();                     \
+    if (_e != cudaSuccess) return tls_set_cuda_error(_e);    \
+  } while (0)
+
+int tls_set_cuda_error(cudaError_t e);
+int tls_set_error(int code, const char* msg);
+
+namespace tls {
+
+constexpr int kWarp = 32;
+
+template <typename T>
+__device__ __forceinline__ T ldg(const T* p) {
+  return __ldg(p);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum within aligned groups of `lanes` lanes (power of two <= 32); fixed
+// butterfly order, so the result is deterministic for a fixed `lanes`.
+template <typename T>
+__device__ __forceinline__ T group_sum(T v, int lanes) {
+  for (int o = lanes >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block reduction of one double (fixed tree order).
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v, double* smem /*[BLOCK/32]*/) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (warp == 0) {
+    t = (lane < BLOCK / 32) ? smem[lane] : 0.0;
+    t = warp_sum(t);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+template <typename T>
+__device__ __forceinline__ double to_d(T x) {
+  return static_cast<double>(x);
+}
+
+inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return static_cast<int>(g);
+}
+
+}  // namespace tls

@@ -1,0 +1,352 @@
+// Block-sparse Jacobian products on the SoA layout.
+//
+// normal_matvec: y = diag(s) J^T J diag(s) x + lambda x (torchls sparse.py:83-84,
+// warp_normal.py:26-122). One factor-major pass computes q_f = J_f (s.x)
+// and each slot's J_s^T q_f into a contribution buffer (coalesced SoA loads of
+// J, coalesced contribution stores); a second pass sums each variable's
+// contributions in a fixed list order. No atomics: results are bitwise
+// reproducible run to run.
+#include "common.cuh"
+
+namespace tls {
+
+struct FactorPass {
+  int64_t n;
+  int32_t R, D;
+  int8_t col_slot[32];
+  int32_t slot_col[TLS_MAX_SLOTS];
+  int32_t slot_dim[TLS_MAX_SLOTS];
+  int64_t slot_off[TLS_MAX_SLOTS];
+  const int32_t* index[TLS_MAX_SLOTS];
+  const void* jac;
+  int64_t ld;
+};
+
+__host__ FactorPass make_pass(const tls_factor_group& fg, const tls_var_group* vg) {
+  FactorPass p{};
+  p.n = fg.count;
+  p.R = fg.rdim;
+  p.D = fg.total_dim;
+  for (int c = 0; c < 32; ++c) p.col_slot[c] = -1;
+  for (int s = 0; s < fg.nslots; ++s) {
+    p.slot_col[s] = fg.slot_col[s];
+    p.slot_dim[s] = fg.slot_dim[s];
+    p.slot_off[s] = vg[fg.slot_group[s]].offset;
+    p.index[s] = fg.index[s];
+    for (int j = 0; j < fg.slot_dim[s]; ++j) p.col_slot[fg.slot_col[s] + j] = (int8_t)s;
+  }
+  p.jac = fg.jac;
+  p.ld = fg.jac_stride ? fg.jac_stride : fg.count;
+  return p;
+}
+
+// MODE 0: contributions J^T J x (per factor)   MODE 1: rows J x   MODE 2: |J x|^2 partial
+// MODE 3: contributions J^T u for factor rows u (x holds u, [N][R])
+template <int RM, int DM, int MODE, typename TJ, typename TV, typename TA>
+__global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV* __restrict__ x,
+                                                          const TV* __restrict__ scale, TV* __restrict__ out,
+                                                          double* __restrict__ partials) {
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  TA q[RM];
+#pragma unroll
+  for (int i = 0; i < RM; ++i) q[i] = TA(0);
+  TA xv[DM];
+  const TJ* __restrict__ jac = reinterpret_cast<const TJ*>(p.jac);
+  const bool live = f < p.n;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < DM; ++c) {
+      const int s = p.col_slot[c];
+      xv[c] = TA(0);
+      if (MODE != 3 && s >= 0) {
+        const int64_t col = p.slot_off[s] + (int64_t)__ldg(p.index[s] + f) * p.slot_dim[s] + (c - p.slot_col[s]);
+        TA v = static_cast<TA>(__ldg(x + col));
+        if (scale) v *= static_cast<TA>(__ldg(scale + col));
+        xv[c] = v;
+      }
+    }
+    TJ J[RM][DM];
+#pragma unroll
+    for (int i = 0; i < RM; ++i)
+#pragma unroll
+      for (int c = 0; c < DM; ++c)
+        J[i][c] = (i < p.R && c < p.D) ? __ldg(jac + (int64_t)(i * p.D + c) * p.ld + f) : TJ(0);
+    if constexpr (MODE == 3) {
+#pragma unroll
+      for (int i = 0; i < RM; ++i)
+        if (i < p.R) q[i] = static_cast<TA>(x[f * p.R + i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < RM; ++i)
+#pragma unroll
+        for (int c = 0; c < DM; ++c) q[i] += static_cast<TA>(J[i][c]) * xv[c];
+    }
+    if constexpr (MODE == 0 || MODE == 3) {
+#pragma unroll
+      for (int c = 0; c < DM; ++c) {
+        TA y = TA(0);
+#pragma unroll
+        for (int i = 0; i < RM; ++i) y += static_cast<TA>(J[i][c]) * q[i];
+        if (c < p.D) out[f * p.D + c] = static_cast<TV>(y);
+      }
+    } else if constexpr (MODE == 1) {
+#pragma unroll
+      for (int i = 0; i < RM; ++i)
+        if (i < p.R) out[f * p.R + i] = static_cast<TV>(q[i]);
+    }
+  }
+  if constexpr (MODE == 2) {
+    __shared__ double sm[4];
+    double acc = 0.0;
+    if (live) {
+#pragma unroll
+      for (int i = 0; i < RM; ++i) acc += to_d(q[i]) * to_d(q[i]);
+    }
+    const double s = block_sum<128>(acc, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+  }
+}
+
+template <int MODE, typename TJ, typename TV, typename TA>
+static int launch_factor_pass(const FactorPass& p, const TV* x, const TV* scale, TV* out, double* partials,
+                              cudaStream_t st) {
+  if (p.n == 0) return TLS_OK;
+  const int block = 128;
+  const int64_t grid = (p.n + block - 1) / block;
+#define TLS_FP(RM, DM)                                                                                    \
+  if (p.R <= RM && p.D <= DM) {                                                                          \
+    factor_pass_kernel<RM, DM, MODE, TJ, TV, TA><<<grid, block, 0, st>>>(p, x, scale, out, partials); \
+    TLS_CHECK_LAUNCH();                                                                                   \
+    return TLS_OK;                                                                                        \
+  }
+  TLS_FP(1, 4)
+  TLS_FP(2, 4)
+  TLS_FP(3, 4)
+  TLS_FP(2, 9)
+  TLS_FP(3, 6)
+  TLS_FP(3, 9)
+  TLS_FP(4, 8)
+  TLS_FP(6, 12)
+  TLS_FP(7, 14)
+  TLS_FP(8, 16)
+#undef TLS_FP
+  return tls_set_error(TLS_ERR_UNSUPPORTED, "factor shape beyond r <= 8, D <= 16");
+}
+
+// Gather: y[col] = s[col] * sum(contrib) + lambda * x[col], deterministic order.
+struct GatherGroups {
+  int32_t ngroups;
+  int32_t block_begin[TLS_MAX_GROUPS + 1];
+  int64_t offset[TLS_MAX_GROUPS];
+  int32_t dim[TLS_MAX_GROUPS];
+  tls_segments seg[TLS_MAX_GROUPS];
+};
+
+template <int WM, typename TV>
+__global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, const TV* __restrict__ contrib,
+                                                            const TV* __restrict__ x, const TV* __restrict__ scale,
+                                                            double damping, TV* __restrict__ y,
+                                                            double* __restrict__ dot_partials) {
+  int gi = 0;
+#pragma unroll 1
+  while (gi + 1 < g.ngroups && (int)blockIdx.x >= g.block_begin[gi + 1]) ++gi;
+  const tls_segments& seg = g.seg[gi];
+  const int L = seg.lanes;
+  const int64_t local = (int64_t)(blockIdx.x - g.block_begin[gi]) * blockDim.x + threadIdx.x;
+  const int64_t t = local / L;
+  const int lane = (int)(local % L);
+  const int d = g.dim[gi];
+  double acc[WM];
+#pragma unroll
+  for (int k = 0; k < WM; ++k) acc[k] = 0.0;
+  if (t < seg.count) {
+    const int b = seg.ptr[t], e = seg.ptr[t + 1];
+    for (int j = b + lane; j < e; j += L) {
+      const TV* src = contrib + seg.src[j];
+#pragma unroll
+      for (int k = 0; k < WM; ++k)
+        if (k < d) acc[k] += to_d(src[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < WM; ++k) acc[k] = group_sum(acc[k], L);
+  double dot = 0.0;
+  if (t < seg.count && lane == 0) {
+    const int64_t base = g.offset[gi] + t * d;
+#pragma unroll
+    for (int k = 0; k < WM; ++k) {
+      if (k < d) {
+        const int64_t col = base + k;
+        double v = acc[k];
+        if (scale) v *= to_d(scale[col]);
+        const double xv = x ? to_d(x[col]) : 0.0;
+        v += damping * xv;
+        const TV out = static_cast<TV>(v);
+        y[col] = out;
+        dot += xv * to_d(out);
+      }
+    }
+  }
+  if (dot_partials) {
+    __shared__ double sm[8];
+    const double s = block_sum<256>(dot, sm);
+    if (threadIdx.x == 0) dot_partials[blockIdx.x] = s;
+  }
+}
+
+}  // namespace tls
+
+using namespace tls;
+
+int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
+                      cudaStream_t st);
+
+// Shared by tls_normal_matvec and the PCG driver. Returns the number of gather
+// blocks (for dot partials) through *gather_blocks.
+int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
+                     cudaStream_t st) {
+  if (a->nfactor_groups > TLS_MAX_FACTOR_GROUPS || a->nvar_groups > TLS_MAX_GROUPS)
+    return tls_set_error(TLS_ERR_INVALID, "too many groups");
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    const tls_factor_group& fg = a->fg[k];
+    FactorPass p = make_pass(fg, a->vg);
+    int rc;
+    if (a->vec_dtype == TLS_F64) {
+      double* out = (double*)a->contrib + a->contrib_offset[k];
+      if (fg.jac_dtype == TLS_F64)
+        rc = launch_factor_pass<0, double, double, double>(p, (const double*)x, (const double*)a->scale, out, nullptr, st);
+      else
+        rc = launch_factor_pass<0, float, double, double>(p, (const double*)x, (const double*)a->scale, out, nullptr, st);
+    } else {
+      float* out = (float*)a->contrib + a->contrib_offset[k];
+      if (fg.jac_dtype == TLS_F32)
+        rc = launch_factor_pass<0, float, float, float>(p, (const float*)x, (const float*)a->scale, out, nullptr, st);
+      else
+        return tls_set_error(TLS_ERR_UNSUPPORTED, "float64 Jacobian with float32 vectors");
+    }
+    if (rc) return rc;
+  }
+  return tls_normal_gather(a, x, y, dot_partials, gather_blocks, st);
+}
+
+int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
+                      cudaStream_t st) {
+  GatherGroups g{};
+  g.ngroups = a->nvar_groups;
+  int blocks = 0, wmax = 1;
+  for (int i = 0; i < a->nvar_groups; ++i) {
+    g.block_begin[i] = blocks;
+    g.offset[i] = a->vg[i].offset;
+    g.dim[i] = a->vg[i].dim;
+    g.seg[i] = a->seg[i];
+    const int64_t threads = (int64_t)a->seg[i].count * a->seg[i].lanes;
+    blocks += (int)((threads + 255) / 256);
+    if (a->vg[i].dim > wmax) wmax = a->vg[i].dim;
+  }
+  g.block_begin[a->nvar_groups] = blocks;
+  if (gather_blocks) *gather_blocks = blocks;
+  if (blocks == 0) return TLS_OK;
+#define TLS_G(WM)                                                                                        \
+  if (wmax <= WM) {                                                                                      \
+    if (a->vec_dtype == TLS_F64)                                                                         \
+      normal_gather_kernel<WM, double><<<blocks, 256, 0, st>>>(g, (const double*)a->contrib, (const double*)x, \
+                                                               (const double*)a->scale, a->damping,     \
+                                                               (double*)y, dot_partials);                \
+    else                                                                                                 \
+      normal_gather_kernel<WM, float><<<blocks, 256, 0, st>>>(g, (const float*)a->contrib, (const float*)x,   \
+                                                              (const float*)a->scale, a->damping,       \
+                                                              (float*)y, dot_partials);                  \
+    TLS_CHECK_LAUNCH();                                                                                  \
+    return TLS_OK;                                                                                       \
+  }
+  TLS_G(3)
+  TLS_G(6)
+  TLS_G(8)
+  TLS_G(16)
+#undef TLS_G
+  return tls_set_error(TLS_ERR_UNSUPPORTED, "variable dim > 16");
+}
+
+extern "C" int tls_normal_matvec(const tls_normal_args* a, const void* x, void* y, tls_stream_t stream) {
+  return tls_normal_apply(a, x, y, nullptr, nullptr, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tls_jacobian_matvec(const tls_normal_args* a, const void* x, void* out_rows, tls_stream_t stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int64_t row = 0;
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    const tls_factor_group& fg = a->fg[k];
+    FactorPass p = make_pass(fg, a->vg);
+    int rc;
+    if (a->vec_dtype == TLS_F64) {
+      double* out = (double*)out_rows + row;
+      rc = fg.jac_dtype == TLS_F64
+               ? launch_factor_pass<1, double, double, double>(p, (const double*)x, (const double*)a->scale, out, nullptr, st)
+               : launch_factor_pass<1, float, double, double>(p, (const double*)x, (const double*)a->scale, out, nullptr, st);
+    } else {
+      float* out = (float*)out_rows + row;
+      if (fg.jac_dtype != TLS_F32) return tls_set_error(TLS_ERR_UNSUPPORTED, "float64 Jacobian with float32 vectors");
+      rc = launch_factor_pass<1, float, float, float>(p, (const float*)x, (const float*)a->scale, out, nullptr, st);
+    }
+    if (rc) return rc;
+    row += fg.count * fg.rdim;
+  }
+  return TLS_OK;
+}
+
+__global__ void sum_partials_kernel(const double* partials, int count, double* out, int accumulate) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) acc += partials[i];
+  const double s = block_sum<256>(acc, sm);
+  if (threadIdx.x == 0) out[0] = accumulate ? out[0] + s : s;
+}
+
+extern "C" int tls_squared_matvec_norm(const tls_normal_args* a, const double* x, double* partials, double* out,
+                                       tls_stream_t stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // One launch per factor group; each writes its block partials, then one
+  // fixed-order sum accumulates into *out.
+  bool first = true;
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    const tls_factor_group& fg = a->fg[k];
+    if (fg.count == 0) continue;
+    FactorPass p = make_pass(fg, a->vg);
+    const int blocks = (int)((fg.count + 127) / 128);
+    if (blocks > (1 << 20)) return tls_set_error(TLS_ERR_UNSUPPORTED, "too many factors for one pass");
+    int rc = fg.jac_dtype == TLS_F64
+                 ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, nullptr, partials, st)
+                 : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, nullptr, partials, st);
+    if (rc) return rc;
+    sum_partials_kernel<<<1, 256, 0, st>>>(partials, blocks, out, first ? 0 : 1);
+    TLS_CHECK_LAUNCH();
+    first = false;
+  }
+  if (first) cudaMemsetAsync(out, 0, sizeof(double), st);
+  return TLS_OK;
+}
+
+extern "C" int tls_jacobian_rmatvec(const tls_normal_args* a, const void* rows, void* out, tls_stream_t stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int64_t row = 0;
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    const tls_factor_group& fg = a->fg[k];
+    FactorPass p = make_pass(fg, a->vg);
+    int rc;
+    if (a->vec_dtype == TLS_F64) {
+      double* c = (double*)a->contrib + a->contrib_offset[k];
+      const double* u = (const double*)rows + row;
+      rc = fg.jac_dtype == TLS_F64 ? launch_factor_pass<3, double, double, double>(p, u, nullptr, c, nullptr, st)
+                                   : launch_factor_pass<3, float, double, double>(p, u, nullptr, c, nullptr, st);
+    } else {
+      if (fg.jac_dtype != TLS_F32) return tls_set_error(TLS_ERR_UNSUPPORTED, "float64 Jacobian with float32 vectors");
+      rc = launch_factor_pass<3, float, float, float>(p, (const float*)rows + row, nullptr,
+                                                      (float*)a->contrib + a->contrib_offset[k], nullptr, st);
+    }
+    if (rc) return rc;
+    row += fg.count * fg.rdim;
+  }
+  tls_normal_args b = *a;
+  b.damping = 0.0;
+  return tls_normal_gather(&b, nullptr, out, nullptr, nullptr, st);
+}

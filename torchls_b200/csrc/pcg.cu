@@ -1,0 +1,582 @@
+// Block-Jacobi factor/apply and the device-resident PCG state machine.
+//
+// The PCG mirrors torchls solvers.py:167-256 step for step: x0 = 0,
+// threshold = max(atol, rtol |b|), stop on nonfinite or nonpositive
+// curvature, a true-residual check when the recurrence converges or every
+// `check_interval` iterations, restarts on drift (adaptive) or always
+// (periodic), and a final true-residual check. Every decision is taken on the
+// device from float64 scalars reduced in a fixed order, so a run needs no
+// host synchronisation and is bitwise reproducible.
+//
+// One state-machine step = operator (ap = A p) -> update -> decide -> direction.
+// During a true-residual check p temporarily holds x (the operator always
+// reads p); the saved direction is restored if the iteration continues.
+#include "blocks.cuh"
+#include "common.cuh"
+
+int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
+                     cudaStream_t st);
+int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* dot_partials, int* gather_blocks,
+                    cudaStream_t st);
+
+namespace tls {
+
+enum { M_ITER = 0, M_CHECK = 1, M_FINAL = 2, M_DONE = 3 };
+enum { A_NONE = 0, A_DIR = 1, A_RESTART = 2, A_RESTORE_DIR = 3, A_SWAP_TO_X = 4 };
+
+// Extended control block kept after the public tls_pcg_control fields.
+struct PcgState {
+  tls_pcg_control pub;
+  int32_t action;
+  int32_t pending;       // reason when the loop broke early
+  int32_t op_blocks;     // number of operator dot partials
+  int32_t upd_blocks;    // number of update partial blocks
+  double rec;            // recurrence norm of the last iteration
+  int32_t rec_hit;       // rec <= threshold at the last iteration
+  int32_t periodic_hit;  // periodic check due at the last iteration
+  int32_t alpha_ok;      // curvature and r.z finite and positive this step
+  int32_t pad2_;
+};
+
+struct BlockSet {
+  int32_t ngroups;
+  int32_t identity;            // no preconditioner: unit blocks
+  int64_t block_begin[TLS_MAX_GROUPS + 1];  // prefix of block counts
+  tls_block_group g[TLS_MAX_GROUPS];
+};
+
+constexpr int kUpdThreads = 128;
+constexpr int kMaxUpdBlocks = 1024;
+
+__device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
+  int gi = 0;
+  while (gi + 1 < bs.ngroups && b >= bs.block_begin[gi + 1]) ++gi;
+  return gi;
+}
+
+template <typename TV>
+__device__ __forceinline__ void apply_block(const BlockSet& bs, int gi, int64_t i, const TV* src, TV* dst,
+                                            double* rbuf, double* zbuf, int& dim, int64_t* cols) {
+  const tls_block_group& g = bs.g[gi];
+  dim = g.dim;
+  for (int k = 0; k < dim; ++k) {
+    cols[k] = block_column(g, i, k);
+    rbuf[k] = to_d(src[cols[k]]);
+  }
+  if (bs.identity || g.factor == nullptr) {
+    for (int k = 0; k < dim; ++k) zbuf[k] = rbuf[k];
+  } else {
+    cholesky_solve_block(g.factor + i * dim * dim, dim, rbuf, zbuf);
+  }
+  if (dst)
+    for (int k = 0; k < dim; ++k) dst[cols[k]] = static_cast<TV>(zbuf[k]);
+}
+
+__device__ __forceinline__ double sum_fixed(const double* p, int n) {
+  // fixed sequential order: every caller gets the identical value
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += p[i];
+  return s;
+}
+
+// ---------------------------------------------------------------- start
+template <typename TV>
+__global__ void __launch_bounds__(kUpdThreads) pcg_init_kernel(int64_t n, const TV* __restrict__ rhs, TV* x, TV* r,
+                                                               double* partials) {
+  __shared__ double sm[kUpdThreads / 32];
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const TV v = rhs[i];
+    x[i] = TV(0);
+    r[i] = v;
+    acc += to_d(v) * to_d(v);
+  }
+  const double s = block_sum<kUpdThreads>(acc, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void pcg_init_finish_kernel(PcgState* st, const double* partials, int blocks, double rtol, double atol,
+                                       int max_it, int interval, int periodic, double drift_tol) {
+  if (threadIdx.x != 0) return;
+  tls_pcg_control& c = st->pub;
+  const double nrm = sqrt(sum_fixed(partials, blocks));
+  c.rhs_norm = nrm;
+  c.threshold = fmax(atol, rtol * nrm);
+  c.residual_norm = nrm;
+  c.iterations = 0;
+  c.restarts = 0;
+  c.checks = 0;
+  c.max_iterations = max_it;
+  c.check_interval = interval;
+  c.periodic = periodic;
+  c.drift_tolerance = drift_tol;
+  c.status = TLS_PCG_ACTIVE;
+  c.mode = M_ITER;
+  st->action = A_NONE;
+  st->pending = TLS_PCG_MAX_ITERATIONS;
+  st->rec = nrm;
+  st->rec_hit = 0;
+  st->periodic_hit = 0;
+  if (!isfinite(nrm)) {
+    c.status = TLS_PCG_NONFINITE;
+    c.mode = M_DONE;
+  } else if (nrm <= c.threshold) {
+    c.status = TLS_PCG_CONVERGED;
+    c.mode = M_DONE;
+  }
+}
+
+// z = M r, p = z, partial r.z (only while ACTIVE)
+template <typename TV>
+__global__ void __launch_bounds__(kUpdThreads) pcg_precondition_kernel(BlockSet bs, int64_t nblocks, const PcgState* st,
+                                                                       const TV* r, TV* z, TV* p, double* partials) {
+  __shared__ double sm[kUpdThreads / 32];
+  double acc = 0.0;
+  if (st->pub.status == TLS_PCG_ACTIVE) {
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks;
+         b += (int64_t)gridDim.x * blockDim.x) {
+      const int gi = find_group(bs, b);
+      const int64_t i = b - bs.block_begin[gi];
+      double rb[kMaxBlock], zb[kMaxBlock];
+      int64_t cols[kMaxBlock];
+      int dim;
+      apply_block(bs, gi, i, r, z, rb, zb, dim, cols);
+      for (int k = 0; k < dim; ++k) {
+        p[cols[k]] = static_cast<TV>(zb[k]);
+        acc += rb[k] * static_cast<double>(static_cast<TV>(zb[k]));
+      }
+    }
+  }
+  const double s = block_sum<kUpdThreads>(acc, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void pcg_rz_finish_kernel(PcgState* st, const double* partials, int blocks) {
+  if (threadIdx.x != 0) return;
+  if (st->pub.status != TLS_PCG_ACTIVE) return;
+  st->pub.rz = sum_fixed(partials, blocks);
+}
+
+// ---------------------------------------------------------------- one step
+// partials layout: [0, kOpPartials) operator dots; update partials at
+// kOpPartials + k * kMaxUpdBlocks (k = 0, 1, 2).
+constexpr int kOpPartials = 65536;
+
+// Deterministic block-wide sum of p[0..n) (fixed strided order + fixed tree).
+__device__ __forceinline__ double block_sum_list(const double* p, int n, double* sm) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
+  return block_sum<256>(acc, sm);
+}
+
+// curvature = p.Ap from the operator's partials; alpha = rz / curvature.
+__global__ void __launch_bounds__(256) pcg_alpha_kernel(PcgState* st, const double* partials) {
+  __shared__ double sm[8];
+  tls_pcg_control& c = st->pub;
+  if (c.status != TLS_PCG_ACTIVE || c.mode != M_ITER) {
+    if (threadIdx.x == 0) st->alpha_ok = 0;
+    return;
+  }
+  const double curv = block_sum_list(partials, st->op_blocks, sm);
+  if (threadIdx.x == 0) {
+    const double rz = c.rz;
+    c.curvature = curv;
+    const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
+    st->alpha_ok = ok;
+    c.alpha = ok ? rz / curv : 0.0;
+  }
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, int64_t nblocks, const PcgState* st,
+                                                                 const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
+                                                                 const TV* p, TV* ap, TV* ztrue,
+                                                                 double* partials) {
+  __shared__ double sm[kUpdThreads / 32];
+  const tls_pcg_control& c = st->pub;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  const int mode = c.mode;
+  bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
+  double alpha = 0.0;
+  if (work && mode == M_ITER) {
+    if (!st->alpha_ok) work = false;
+    else alpha = c.alpha;
+  }
+  if (work) {
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks;
+         b += (int64_t)gridDim.x * blockDim.x) {
+      const int gi = find_group(bs, b);
+      const int64_t i = b - bs.block_begin[gi];
+      const tls_block_group& g = bs.g[gi];
+      const int dim = g.dim;
+      int64_t cols[kMaxBlock];
+      for (int k = 0; k < dim; ++k) cols[k] = block_column(g, i, k);
+      double rb[kMaxBlock], zb[kMaxBlock];
+      if (mode == M_ITER) {
+        for (int k = 0; k < dim; ++k) {
+          const int64_t col = cols[k];
+          const TV pk = p[col];
+          x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(pk));
+          const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
+          r[col] = rn;
+          rb[k] = to_d(rn);
+        }
+      } else {
+        // ap holds A x: true residual tr = rhs - A x (stored into ap)
+        for (int k = 0; k < dim; ++k) {
+          const int64_t col = cols[k];
+          const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
+          ap[col] = tr;
+          const double t = to_d(tr);
+          rb[k] = t;
+          a0 += t * t;
+          const double dr = t - to_d(r[col]);
+          a1 += dr * dr;
+        }
+      }
+      if (mode == M_FINAL) continue;
+      if (bs.identity || g.factor == nullptr) {
+        for (int k = 0; k < dim; ++k) zb[k] = rb[k];
+      } else {
+        cholesky_solve_block(g.factor + i * dim * dim, dim, rb, zb);
+      }
+      TV* zdst = (mode == M_ITER) ? z : ztrue;
+      for (int k = 0; k < dim; ++k) {
+        const TV zk = static_cast<TV>(zb[k]);
+        zdst[cols[k]] = zk;
+        const double zd = static_cast<double>(zk);
+        if (mode == M_ITER) {
+          a0 += rb[k] * rb[k];
+          a1 += rb[k] * zd;
+        } else {
+          a2 += rb[k] * zd;
+        }
+      }
+    }
+  }
+  const double s0 = block_sum<kUpdThreads>(a0, sm);
+  const double s1 = block_sum<kUpdThreads>(a1, sm);
+  const double s2 = block_sum<kUpdThreads>(a2, sm);
+  if (threadIdx.x == 0) {
+    partials[kOpPartials + blockIdx.x] = s0;
+    partials[kOpPartials + kMaxUpdBlocks + blockIdx.x] = s1;
+    partials[kOpPartials + 2 * kMaxUpdBlocks + blockIdx.x] = s2;
+  }
+}
+
+__global__ void __launch_bounds__(256) pcg_decide_kernel(PcgState* st, const double* partials) {
+  __shared__ double sm[8];
+  tls_pcg_control& c = st->pub;
+  const bool live = c.status == TLS_PCG_ACTIVE && c.mode != M_DONE;
+  const int nb = st->upd_blocks;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  if (live) {
+    s0 = block_sum_list(partials + kOpPartials, nb, sm);
+    s1 = block_sum_list(partials + kOpPartials + kMaxUpdBlocks, nb, sm);
+    s2 = block_sum_list(partials + kOpPartials + 2 * kMaxUpdBlocks, nb, sm);
+  }
+  if (threadIdx.x != 0) return;
+  st->action = A_NONE;
+  if (!live) return;
+  const double thr = c.threshold;
+  if (c.mode == M_ITER) {
+    const double curv = c.curvature;
+    const double rz = c.rz;
+    const int it = ++c.iterations;
+    if (!isfinite(curv) || !isfinite(rz)) {
+      st->pending = TLS_PCG_NONFINITE;
+      c.mode = M_FINAL;
+      st->action = A_SWAP_TO_X;
+      return;
+    }
+    if (curv <= 0.0 || rz <= 0.0) {
+      st->pending = TLS_PCG_NONPOSITIVE;
+      c.mode = M_FINAL;
+      st->action = A_SWAP_TO_X;
+      return;
+    }
+    c.alpha = rz / curv;
+    c.rr = s0;
+    c.rz_new = s1;
+    const double rec = sqrt(s0);
+    st->rec = rec;
+    const bool periodic = c.check_interval > 0 && (it % c.check_interval) == 0;
+    st->rec_hit = rec <= thr;
+    st->periodic_hit = periodic;
+    if (rec <= thr || periodic) {
+      c.mode = M_CHECK;
+      st->action = A_SWAP_TO_X;
+      return;
+    }
+    if (it >= c.max_iterations) {
+      c.mode = M_FINAL;
+      st->action = A_SWAP_TO_X;
+      return;
+    }
+    c.beta = s1 / rz;
+    c.rz = s1;
+    c.mode = M_ITER;
+    st->action = A_DIR;
+    return;
+  }
+  if (c.mode == M_CHECK) {
+    const double tn = sqrt(s0);
+    c.checks += 1;
+    c.true_rr = s0;
+    c.residual_norm = tn;
+    if (!isfinite(tn)) {
+      c.status = TLS_PCG_NONFINITE;
+      c.mode = M_DONE;
+      return;
+    }
+    if (tn <= thr) {
+      c.status = TLS_PCG_CONVERGED;
+      c.mode = M_DONE;
+      return;
+    }
+    const double drift = sqrt(s1);
+    c.drift_rr = s1;
+    const bool last = c.iterations >= c.max_iterations;
+    if (st->rec_hit || c.periodic || drift > c.drift_tolerance * fmax(tn, thr)) {
+      c.rz = s2;
+      c.rz_true = s2;
+      c.restarts += 1;
+      st->action = A_RESTART;
+      c.mode = last ? M_FINAL : M_ITER;
+      return;
+    }
+    c.beta = c.rz_new / c.rz;
+    c.rz = c.rz_new;
+    st->action = A_RESTORE_DIR;
+    c.mode = last ? M_FINAL : M_ITER;
+    return;
+  }
+  // M_FINAL
+  const double tn = sqrt(s0);
+  c.checks += 1;
+  c.true_rr = s0;
+  c.residual_norm = tn;
+  if (isfinite(tn) && tn <= thr) c.status = TLS_PCG_CONVERGED;
+  else if (!isfinite(tn)) c.status = TLS_PCG_NONFINITE;
+  else c.status = st->pending;
+  c.mode = M_DONE;
+}
+
+// Direction / restart / swap. When the next mode is FINAL after a restart or
+// a direction update, p is additionally replaced by x (the operator reads p).
+template <typename TV>
+__global__ void __launch_bounds__(256) pcg_direction_kernel(int64_t n, const PcgState* st, const TV* x, TV* r,
+                                                            const TV* z, TV* p, TV* psave, const TV* ap,
+                                                            const TV* ztrue) {
+  const int action = st->action;
+  if (action == A_NONE) return;
+  const double beta = st->pub.beta;
+  const bool to_final = st->pub.mode == M_FINAL && action != A_SWAP_TO_X;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    switch (action) {
+      case A_DIR:
+        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(p[i]));
+        break;
+      case A_RESTART:
+        r[i] = ap[i];
+        p[i] = ztrue[i];
+        break;
+      case A_RESTORE_DIR:
+        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(psave[i]));
+        break;
+      case A_SWAP_TO_X:
+        psave[i] = p[i];
+        p[i] = x[i];
+        break;
+    }
+    if (to_final) p[i] = x[i];
+  }
+}
+
+__host__ BlockSet make_blocks(const tls_pcg_args* a, int64_t* total) {
+  BlockSet bs{};
+  int64_t nb = 0;
+  if (a->pre == nullptr || a->npre == 0) {
+    bs.identity = 1;
+    // one unit block per element
+    bs.ngroups = 1;
+    bs.g[0].count = (int32_t)a->n;
+    bs.g[0].dim = 1;
+    bs.g[0].nmembers = 1;
+    bs.g[0].member_offset[0] = 0;
+    bs.g[0].member_dim[0] = 1;
+    bs.block_begin[0] = 0;
+    bs.block_begin[1] = a->n;
+    *total = a->n;
+    return bs;
+  }
+  bs.ngroups = a->npre;
+  for (int i = 0; i < a->npre; ++i) {
+    bs.g[i] = a->pre[i];
+    bs.block_begin[i] = nb;
+    nb += a->pre[i].count;
+  }
+  bs.block_begin[a->npre] = nb;
+  *total = nb;
+  return bs;
+}
+
+static int grid_of(int64_t n, int block, int cap) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+template <typename TV>
+static int pcg_start_t(const tls_pcg_args* a, double rtol, double atol, int max_it, int interval, int periodic,
+                       double drift, cudaStream_t s) {
+  PcgState* st = reinterpret_cast<PcgState*>(a->control);
+  const int g = grid_of(a->n, kUpdThreads, kMaxUpdBlocks);
+  pcg_init_kernel<TV><<<g, kUpdThreads, 0, s>>>(a->n, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r,
+                                                a->partials + kOpPartials);
+  TLS_CHECK_LAUNCH();
+  pcg_init_finish_kernel<<<1, 32, 0, s>>>(st, a->partials + kOpPartials, g, rtol, atol, max_it, interval, periodic,
+                                          drift);
+  TLS_CHECK_LAUNCH();
+  int64_t nb;
+  BlockSet bs = make_blocks(a, &nb);
+  const int gb = grid_of(nb, kUpdThreads, kMaxUpdBlocks);
+  pcg_precondition_kernel<TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->r, (TV*)a->z, (TV*)a->p,
+                                                         a->partials + kOpPartials);
+  TLS_CHECK_LAUNCH();
+  pcg_rz_finish_kernel<<<1, 32, 0, s>>>(st, a->partials + kOpPartials, gb);
+  TLS_CHECK_LAUNCH();
+  return TLS_OK;
+}
+
+__global__ void set_block_counts_kernel(PcgState* st, int op_blocks, int upd_blocks) {
+  st->op_blocks = op_blocks;
+  st->upd_blocks = upd_blocks;
+}
+
+// Number of dot partials the operator's final kernel writes (one per block).
+static int operator_blocks(const tls_pcg_args* a) {
+  if (a->op_kind == 0) {
+    int blocks = 0;
+    for (int i = 0; i < a->normal->nvar_groups; ++i) {
+      const int64_t threads = (int64_t)a->normal->seg[i].count * a->normal->seg[i].lanes;
+      blocks += (int)((threads + 255) / 256);
+    }
+    return blocks;
+  }
+  return (a->schur->nretained * 32 + 255) / 256;
+}
+
+template <typename TV>
+static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
+  PcgState* st = reinterpret_cast<PcgState*>(a->control);
+  int64_t nb;
+  BlockSet bs = make_blocks(a, &nb);
+  const int gb = grid_of(nb, kUpdThreads, kMaxUpdBlocks);
+  const int gd = grid_of(a->n, 256, 148 * 8);
+  const int op_blocks = operator_blocks(a);
+  if (op_blocks > kOpPartials) return tls_set_error(TLS_ERR_UNSUPPORTED, "operator uses too many blocks");
+  for (int k = 0; k < steps; ++k) {
+    int launched = 0;
+    int rc;
+    if (a->op_kind == 0)
+      rc = tls_normal_apply(a->normal, a->p, a->ap, a->partials, &launched, s);
+    else
+      rc = tls_schur_apply(a->schur, a->p, a->ap, a->partials, &launched, s);
+    if (rc) return rc;
+    if (launched != op_blocks) return tls_set_error(TLS_ERR_INVALID, "operator block count changed");
+    if (k == 0) {
+      set_block_counts_kernel<<<1, 1, 0, s>>>(st, op_blocks, gb);
+      TLS_CHECK_LAUNCH();
+    }
+    pcg_alpha_kernel<<<1, 256, 0, s>>>(st, a->partials);
+    TLS_CHECK_LAUNCH();
+    pcg_update_kernel<TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r, (TV*)a->z,
+                                                     (const TV*)a->p, (TV*)a->ap, (TV*)a->ztrue, a->partials);
+    TLS_CHECK_LAUNCH();
+    pcg_decide_kernel<<<1, 256, 0, s>>>(st, a->partials);
+    TLS_CHECK_LAUNCH();
+    pcg_direction_kernel<TV><<<gd, 256, 0, s>>>(a->n, st, (const TV*)a->x, (TV*)a->r, (const TV*)a->z, (TV*)a->p,
+                                                (TV*)a->psave, (const TV*)a->ap, (const TV*)a->ztrue);
+    TLS_CHECK_LAUNCH();
+  }
+  return TLS_OK;
+}
+
+// ---------------------------------------------------------------- block Jacobi
+__global__ void block_cholesky_kernel(tls_block_group g, double damping, int32_t* bad) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.count) return;
+  const int d = g.dim;
+  double A[kMaxBlock * kMaxBlock], L[kMaxBlock * kMaxBlock], s[kMaxBlock];
+  for (int k = 0; k < d; ++k) s[k] = g.scale ? g.scale[block_column(g, i, k)] : 1.0;
+  for (int a = 0; a < d; ++a)
+    for (int b = 0; b < d; ++b) A[a * d + b] = s[a] * g.blocks[i * d * d + a * d + b] * s[b];
+  const bool ok = cholesky_block(A, L, d, damping);
+  for (int k = 0; k < d * d; ++k) g.factor[i * d * d + k] = L[k];
+  if (!ok) atomicAdd(bad, 1);
+}
+
+template <typename TV>
+__global__ void block_solve_kernel(BlockSet bs, int64_t nblocks, const TV* r, TV* z) {
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (int64_t)gridDim.x * blockDim.x) {
+    const int gi = find_group(bs, b);
+    double rb[kMaxBlock], zb[kMaxBlock];
+    int64_t cols[kMaxBlock];
+    int dim;
+    apply_block(bs, gi, b - bs.block_begin[gi], r, z, rb, zb, dim, cols);
+  }
+}
+
+}  // namespace tls
+
+using namespace tls;
+
+extern "C" int tls_block_cholesky(const tls_block_group* groups, int32_t ngroups, double damping, int32_t* bad,
+                                  tls_stream_t stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
+  for (int i = 0; i < ngroups; ++i) {
+    if (groups[i].dim > kMaxBlock) return tls_set_error(TLS_ERR_UNSUPPORTED, "preconditioner block dim > 16");
+    if (groups[i].count == 0) continue;
+    block_cholesky_kernel<<<(groups[i].count + 127) / 128, 128, 0, s>>>(groups[i], damping, bad);
+    TLS_CHECK_LAUNCH();
+  }
+  return TLS_OK;
+}
+
+extern "C" int tls_block_solve(const tls_block_group* groups, int32_t ngroups, const void* r, void* z,
+                               int32_t vec_dtype, tls_stream_t stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  tls_pcg_args a{};
+  a.pre = groups;
+  a.npre = ngroups;
+  int64_t nb;
+  BlockSet bs = make_blocks(&a, &nb);
+  if (nb == 0) return TLS_OK;
+  const int g = grid_of(nb, 128, 148 * 16);
+  if (vec_dtype == TLS_F64)
+    block_solve_kernel<double><<<g, 128, 0, s>>>(bs, nb, (const double*)r, (double*)z);
+  else
+    block_solve_kernel<float><<<g, 128, 0, s>>>(bs, nb, (const float*)r, (float*)z);
+  TLS_CHECK_LAUNCH();
+  return TLS_OK;
+}
+
+extern "C" int tls_pcg_start(const tls_pcg_args* a, double rtol, double atol, int32_t max_iterations,
+                             int32_t check_interval, int32_t periodic, double drift_tolerance, tls_stream_t stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (a->npre > TLS_MAX_GROUPS) return tls_set_error(TLS_ERR_INVALID, "too many preconditioner groups");
+  if (a->vec_dtype == TLS_F64)
+    return pcg_start_t<double>(a, rtol, atol, max_iterations, check_interval, periodic, drift_tolerance, s);
+  return pcg_start_t<float>(a, rtol, atol, max_iterations, check_interval, periodic, drift_tolerance, s);
+}
+
+extern "C" int tls_pcg_run(const tls_pcg_args* a, int32_t steps, tls_stream_t stream) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (a->vec_dtype == TLS_F64) return pcg_run_t<double>(a, steps, s);
+  return pcg_run_t<float>(a, steps, s);
+}
+
+extern "C" int tls_pcg_state_bytes(void) { return (int)sizeof(PcgState); }

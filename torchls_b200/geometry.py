@@ -205,13 +205,13 @@ def se3_log(pose: Tensor) -> Tensor:
     w = so3_log(pose[..., :3, :3])
     W = skew(w)
     t2 = (w * w).sum(-1, keepdim=True)
-    small = t2 < SMALL_ANGLE2
+    # V^-1 = I - W/2 + k W^2, k = (1 - (t/2) cot(t/2)) / t^2; the closed form
+    # cancels for small t, so a Taylor series is used below t = 0.5.
+    small = t2 < 0.25
     safe_t2 = torch.where(small, torch.ones_like(t2), t2)
-    t = safe_t2.sqrt()
-    # V^-1 = I - W/2 + k W^2, k = (1 - (t/2) cot(t/2)) / t^2
-    half = t / 2
+    half = safe_t2.sqrt() / 2
     k_big = (1 - half * torch.cos(half) / torch.sin(half)) / safe_t2
-    k_small = 1.0 / 12 + t2 / 720 + t2 * t2 / 30240
+    k_small = 1.0 / 12 + t2 * (1.0 / 720 + t2 * (1.0 / 30240 + t2 * (1.0 / 1209600 + t2 / 47900160)))
     k = torch.where(small, k_small, k_big)[..., None]
     eye = torch.eye(3, dtype=pose.dtype, device=pose.device)
     vinv = eye - 0.5 * W + k * (W @ W)

@@ -1,0 +1,299 @@
+"""Schur elimination of one independent variable group on the GPU.
+
+Interface of torchls ``schur.py``: ``SchurPlan`` (symbolic, once per problem),
+``SchurLinearization`` (per linearization: cross blocks), ``DampedSchurSystem``
+(per trial: reduced_rhs, matvec, preconditioner, backsubstitute,
+dense_matrix).
+
+Edges are the unique (retained variable, eliminated variable) pairs sorted by
+key r * E + e, exactly as torchls orders them (schur.py:83-124); ``edges``
+exposes that order. The kernels store edges in a chunked order instead: a
+chunk holds whole eliminated variables (so each eliminated sum stays inside
+one thread block) and within a chunk edges are sorted by retained variable
+(so retained sums are contiguous runs). W is stored structure-of-arrays
+[dr*de][E] in that order.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .kernels import segment_reduce
+
+SMEM_BYTES = 200 * 1024
+
+
+class SchurPlan:
+    def __init__(self, problem, eliminate, device, *, preconditioner_groups=(), chunk_edges: int = 2048):
+        layout = problem.layout
+        matches = [i for i, e in enumerate(layout) if e.key == eliminate]
+        if len(matches) != 1:
+            raise ValueError("eliminate must identify one parameter group by name or Var type")
+        self.eliminated = matches[0]
+        self.e = layout[self.eliminated]
+        self.retained = tuple(i for i in range(len(layout)) if i != self.eliminated)
+        if not self.retained:
+            raise ValueError("Schur elimination needs a retained parameter group")
+        if len(self.retained) != 1:
+            raise NotImplementedError("the CUDA Schur path supports exactly one retained variable group")
+        if preconditioner_groups:
+            raise NotImplementedError("joint preconditioner groups are not supported with the CUDA Schur path")
+        self.device = torch.device(device)
+        self.r = layout[self.retained[0]]
+        self.dim = self.r.size
+        self.original_layout = layout
+        dr, de = self.r.dim, self.e.dim
+        self.dr, self.de = dr, de
+        E_count = self.e.count
+        keys, recs = [], []
+        self.plan_info = []
+        for k, plan in enumerate(problem.plans):
+            eslots = [s for s, t in enumerate(plan.type_indices) if t == self.eliminated]
+            rslots = [s for s, t in enumerate(plan.type_indices) if t != self.eliminated]
+            if eslots and any(not torch.equal(plan.indices[s], plan.indices[eslots[0]]) for s in eslots[1:]):
+                raise ValueError(
+                    "Eliminated variables must be independent: a residual connects distinct eliminated indices")
+            if len(rslots) > 1:
+                raise NotImplementedError(
+                    "the CUDA Schur path does not support residuals coupling several retained variables")
+            info = dict(eslots=eslots, rslots=rslots, width=0, slot_cross=[-1] * L.MAX_SLOTS, base=0)
+            if eslots and rslots:
+                off = 0
+                for s in rslots:
+                    info["slot_cross"][s] = off
+                    off += layout[plan.type_indices[s]].dim * de
+                info["width"] = off
+                for s in rslots:
+                    key = plan.indices[s].numpy() * E_count + plan.indices[eslots[0]].numpy()
+                    keys.append(key)
+                    recs.append((k, s, plan.count))
+            self.plan_info.append(info)
+        base = 0
+        for k, plan in enumerate(problem.plans):
+            self.plan_info[k]["base"] = base
+            base += plan.count * self.plan_info[k]["width"]
+        self.cross_size = base
+        allkeys = np.concatenate(keys) if keys else np.zeros(0, np.int64)
+        uniq, inverse = np.unique(allkeys, return_inverse=True)
+        ri, ei = uniq // E_count, uniq % E_count
+        self.nedges = len(uniq)
+        self.edges = ((torch.from_numpy(ri).to(device), torch.from_numpy(ei).to(device)),)
+        # ---- chunked order
+        deg = np.bincount(ei, minlength=E_count)
+        max_deg = int(deg.max()) if len(deg) else 0
+        cap = SMEM_BYTES // ((dr + de) * 8)
+        if max_deg > cap:
+            raise ValueError(f"an eliminated variable has {max_deg} retained neighbours; the CUDA Schur path "
+                             f"supports at most {cap}")
+        target = max(1, min(chunk_edges, cap - max_deg + 1))
+        start_e = np.cumsum(deg) - deg
+        chunk_of_e = start_e // target
+        order = np.lexsort((ei, ri, chunk_of_e[ei]))
+        pos_of_edge = np.empty(self.nedges, np.int64)
+        pos_of_edge[order] = np.arange(self.nedges)
+        self.order = order  # chunk position -> reference edge index
+        self.pos_of_edge = pos_of_edge
+        c_r, c_e, c_ch = ri[order], ei[order], chunk_of_e[ei[order]]
+        newchunk = np.ones(self.nedges, bool)
+        newchunk[1:] = c_ch[1:] != c_ch[:-1]
+        chunk_ptr = np.concatenate((np.flatnonzero(newchunk), [self.nedges])).astype(np.int32)
+        newrun = newchunk.copy()
+        newrun[1:] |= c_r[1:] != c_r[:-1]
+        run_starts = np.flatnonzero(newrun)
+        run_ptr = np.concatenate((run_starts, [self.nedges])).astype(np.int32)
+        run_chunk = np.cumsum(newchunk)[run_starts] - 1
+        nchunks = len(chunk_ptr) - 1
+        chunk_run_ptr = np.searchsorted(run_chunk, np.arange(nchunks + 1)).astype(np.int32)
+        run_r = c_r[run_starts]
+        rorder = np.argsort(run_r, kind="stable")
+        rrun_ptr = np.concatenate(([0], np.cumsum(np.bincount(run_r, minlength=self.r.count)))).astype(np.int32)
+        eorder = np.lexsort((np.arange(self.nedges), c_e))
+        elim_ptr = np.concatenate(([0], np.cumsum(np.bincount(c_e, minlength=E_count)))).astype(np.int32)
+        self.nchunks = nchunks
+        self.nruns = len(run_starts)
+        self.max_chunk_edges = int(np.diff(chunk_ptr).max()) if nchunks else 1
+        # ---- cross-contribution segments per edge (chunk order)
+        cursor, ids, offs = 0, [], []
+        for k, s, n in recs:
+            info = self.plan_info[k]
+            ids.append(pos_of_edge[inverse[cursor : cursor + n]])
+            offs.append(info["base"] + np.arange(n, dtype=np.int64) * info["width"] + info["slot_cross"][s])
+            cursor += n
+        ids = np.concatenate(ids) if ids else np.zeros(0, np.int64)
+        offs = np.concatenate(offs) if offs else np.zeros(0, np.int64)
+        o = np.argsort(ids, kind="stable")
+        if self.cross_size >= 2**31:
+            raise ValueError("Schur cross buffer exceeds the 32-bit offset range")
+        cptr = np.concatenate(([0], np.cumsum(np.bincount(ids, minlength=self.nedges)))).astype(np.int32)
+        t = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt)
+        self.dev = dict(
+            chunk_ptr=t(chunk_ptr), chunk_run_ptr=t(chunk_run_ptr), edge_r=t(c_r), edge_e=t(c_e),
+            elim_ptr=t(elim_ptr), elim_edges=t(eorder), run_ptr=t(run_ptr), rrun_ptr=t(rrun_ptr),
+            rrun_list=t(rorder), cross_ptr=t(cptr), cross_src=t(offs[o]),
+        )
+        self.cross_seg = L.Segments(self.nedges, dr * de, 1, 0, self.dev["cross_ptr"].data_ptr(),
+                                    self.dev["cross_src"].data_ptr())
+        # reduced-vector indices into the full tangent (schur.py:28-37)
+        self.global_indices = torch.arange(self.r.offset, self.r.offset + self.r.size, device=device)
+        self.layout = (self.r,)
+        self.bad = torch.zeros(1, dtype=torch.int32, device=device)
+
+    # ---------------------------------------------------------------- linearization hooks
+    def cross_buffer(self, device):
+        return torch.empty(self.cross_size, dtype=torch.float64, device=device)
+
+    def fill_cross_args(self, k, la) -> int:
+        info = self.plan_info[k]
+        mask = 0
+        for s in info["eslots"]:
+            mask |= 1 << s
+        la.elim_mask = mask if info["width"] else 0
+        la.elim_dim = self.de
+        for s in range(L.MAX_SLOTS):
+            la.slot_cross[s] = info["slot_cross"][s] if info["width"] else -1
+        la.cross_width = info["width"]
+        return info["base"]
+
+
+class SchurLinearization:
+    """Cross blocks E_e = J_r^T J_e per edge (schur.py:192-257), in chunk order, float64."""
+
+    def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
+        self.plan = plan
+        dev = plan.device
+        self.cross = torch.empty((plan.nedges, plan.dr, plan.de), dtype=torch.float64, device=dev)
+        if plan.nedges:
+            segment_reduce(plan.cross_seg, lin.cross_contrib, self.cross)
+        self.ret_diag = diagonal_raw[plan.retained[0]].contiguous()
+        self.elim_diag = diagonal_raw[plan.eliminated].contiguous()
+        self.scale = None if scale is None else scale.to(torch.float64).contiguous()
+        self.wdtype, self.vec_dtype = wdtype, vec_dtype
+        self.dense = dense
+        n, E = plan.nedges, plan.nedges
+        self.w = torch.empty((plan.dr * plan.de, max(E, 1)), dtype=wdtype, device=dev)
+        self.inv_l = torch.empty((plan.e.count, plan.de, plan.de), dtype=torch.float64, device=dev)
+        self.run_partial = torch.empty((max(plan.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
+        self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
+
+    def damped(self, damping):
+        return DampedSchurSystem(self, damping)
+
+
+class DampedSchurSystem:
+    """schur.py:263-397 on the GPU."""
+
+    def __init__(self, lin: SchurLinearization, damping: float):
+        self.linear, self.plan, self.damping = lin, lin.plan, float(damping)
+        self.args = self._args()
+        L.call("tls_schur_damp", C.byref(self.args), L.stream_handle(self.plan.device))
+        if int(self.plan.bad.item()) > 0:
+            raise torch.linalg.LinAlgError("damped eliminated block is not positive definite")
+        self._rhs_ready = False
+
+    def _args(self) -> L.SchurArgs:
+        p, lin = self.plan, self.linear
+        a = L.SchurArgs()
+        a.nedges, a.nchunks, a.dr, a.de = p.nedges, p.nchunks, p.dr, p.de
+        a.nretained, a.nelim = p.r.count, p.e.count
+        a.wdtype, a.vec_dtype = L.dtype_code(lin.wdtype), L.dtype_code(lin.vec_dtype)
+        a.max_chunk_edges, a.nruns = p.max_chunk_edges, p.nruns
+        a.retained_offset, a.elim_offset = p.r.offset, p.e.offset
+        d = p.dev
+        for name in ("chunk_ptr", "chunk_run_ptr", "edge_r", "edge_e", "elim_ptr", "elim_edges", "run_ptr",
+                     "rrun_ptr", "rrun_list"):
+            setattr(a, name, d[name].data_ptr())
+        a.cross = lin.cross.data_ptr()
+        a.elim_diag = lin.elim_diag.data_ptr()
+        a.ret_diag = lin.ret_diag.data_ptr()
+        a.scale = None if lin.scale is None else lin.scale.data_ptr()
+        a.inv_l = lin.inv_l.data_ptr()
+        a.w = lin.w.data_ptr()
+        a.run_partial = lin.run_partial.data_ptr()
+        a.ybuf = lin.ybuf.data_ptr()
+        a.damping = self.damping
+        a.bad = p.bad.data_ptr()
+        return a
+
+    @property
+    def stream(self):
+        return L.stream_handle(self.plan.device)
+
+    def reduced_rhs(self, rhs: torch.Tensor) -> torch.Tensor:
+        """rhs_c = b_c - W (L^-1 b_e) from the full scaled rhs b (schur.py:285-290)."""
+        b = rhs.to(torch.float64).contiguous()
+        out = torch.empty(self.plan.dim, dtype=self.linear.vec_dtype, device=b.device)
+        L.call("tls_schur_reduced_rhs", C.byref(self.args), b.data_ptr(), out.data_ptr(), self.stream)
+        self._rhs_ready = True
+        return out
+
+    def backsubstitute(self, retained: torch.Tensor) -> torch.Tensor:
+        """Full float64 step: retained part plus L^-T (L^-1 b_e - W^T x_c) (schur.py:292-301)."""
+        if not self._rhs_ready:
+            raise ValueError("backsubstitute requires reduced_rhs first")
+        x = retained.to(self.linear.vec_dtype).contiguous()
+        total = sum(e.size for e in self.plan.original_layout)
+        out = torch.zeros(total, dtype=torch.float64, device=x.device)
+        L.call("tls_schur_backsubstitute", C.byref(self.args), x.data_ptr(), out.data_ptr(), self.stream)
+        return out
+
+    def matvec(self, vector: torch.Tensor) -> torch.Tensor:
+        """(s U s + lambda I) v - W (W^T v) (schur.py:303-328)."""
+        v = vector.to(self.linear.vec_dtype).contiguous()
+        out = torch.empty_like(v)
+        L.call("tls_schur_matvec", C.byref(self.args), v.data_ptr(), out.data_ptr(), self.stream)
+        return out
+
+    def preconditioner_blocks(self) -> torch.Tensor:
+        p = self.plan
+        out = torch.empty((p.r.count, p.dr, p.dr), dtype=torch.float64, device=p.device)
+        L.call("tls_schur_preconditioner_blocks", C.byref(self.args), out.data_ptr(), self.stream)
+        return out
+
+    def preconditioner(self, *, graph_safe: bool = False):
+        """Exact Schur block-diagonal preconditioner (schur.py:353-378)."""
+        from .solvers import BlockJacobiPreconditioner
+
+        p = self.plan
+        blocks = self.preconditioner_blocks()
+        return BlockJacobiPreconditioner.from_blocks([(blocks, [(0, p.dr)], p.r.count, p.dr)], self.damping,
+                                                     None, p.dim)
+
+    def dense_matrix(self) -> torch.Tensor:
+        """Dense reduced matrix (s U s + lambda I) - W W^T, symmetrised (schur.py:380-397)."""
+        p = self.plan
+        E = p.nedges
+        n = p.dim
+        S = torch.zeros((n, n), dtype=torch.float64, device=p.device)
+        # base blocks
+        U = self.linear.ret_diag
+        if self.linear.scale is not None:
+            s = self.linear.scale[p.r.offset : p.r.offset + p.r.size].view(p.r.count, p.dr)
+            U = U * s[:, :, None] * s[:, None, :]
+        idx = torch.arange(p.r.count, device=p.device)[:, None] * p.dr + torch.arange(p.dr, device=p.device)
+        S[idx[:, :, None], idx[:, None, :]] = U
+        S += self.damping * torch.eye(n, dtype=torch.float64, device=p.device)
+        if E:
+            # W rows (retained columns) x eliminated columns, sparse COO -> dense chunks
+            w = self.linear.w[:, :E].to(torch.float64).view(p.dr, p.de, E)
+            er = p.dev["edge_r"].long()
+            ee = p.dev["edge_e"].long()
+            cols_all = ee[:, None] * p.de + torch.arange(p.de, device=p.device)[None, :]
+            rows_all = er[:, None] * p.dr + torch.arange(p.dr, device=p.device)[None, :]
+            step = max(1, (1 << 27) // max(n, 1))
+            ncols = p.e.count * p.de
+            for c0 in range(0, ncols, step):
+                c1 = min(ncols, c0 + step)
+                sel = ((cols_all[:, 0] >= c0) & (cols_all[:, 0] < c1)).nonzero().flatten()
+                if sel.numel() == 0:
+                    continue
+                Wd = torch.zeros((n, c1 - c0), dtype=torch.float64, device=p.device)
+                r_idx = rows_all[sel][:, :, None].expand(-1, p.dr, p.de)
+                c_idx = (cols_all[sel] - c0)[:, None, :].expand(-1, p.dr, p.de)
+                vals = w[:, :, sel].permute(2, 0, 1)
+                Wd[r_idx.reshape(-1), c_idx.reshape(-1)] = vals.reshape(-1)
+                S -= Wd @ Wd.T
+        return 0.5 * (S + S.T)
