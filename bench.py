@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark: mid-size bundle adjustment solve on B200.
+
+Workload (one "step"): a full LM solve of the seeded 1,000,000-observation
+bundle adjustment (256 cameras, 100,000 points, 10 views within +-60 degrees,
+Huber 0.01, Schur-PCG with block-Jacobi on 6x6 camera blocks, <= 20 LM
+iterations, PCG rtol 1e-6), from the same initial values every step, reaching
+the float64 reference cost within 1e-8 relative.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+Prints one JSON line (rank 0). ``value`` is seconds per solve in mixed
+precision (lower is better); ``fp64_s`` the same solve in float64. Several
+GPUs run independent replicas of the same solve ("replicas only": one coupled
+problem does not shard); timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BA solve s to rel-cost 1e-8 (mixed vs FP64 CUDA); normal-matvec HBM GB/s vs peak"
+TARGET_FILE = os.path.join(ROOT, "tests", "golden", "ba_mid_target.json")
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the Schur chunk
+# kernel on this workload (profiles/schur_chunk_kernel_ba_mid.md); None until captured.
+NCU_TRAFFIC_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison solve")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="10-camera / 4,000-observation case (debug)")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="only build the workload and time the matvec kernels (the ncu capture target)")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "cuda" else "gloo"
+        if args.impl == "cuda":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- workload
+def make_data(small: bool):
+    from torchls_b200 import synthetic
+
+    return synthetic.small_bundle_adjustment(0) if small else synthetic.mid_bundle_adjustment(0)
+
+
+def build(data, device, tls):
+    from torchls_b200 import synthetic
+
+    return synthetic.build_bundle_adjustment(data, tls, device=device, loss=tls.HuberLoss(0.01))
+
+
+def solve_opts(tls, precision):
+    return dict(linear_solver="schur_cg", eliminate="points",
+                conjugate_gradient=tls.ConjugateGradientConfig(precision=precision),
+                termination=tls.TerminationConfig(max_iterations=20), return_summary=True)
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def time_solves(problem, init, tls, precision, steps, warmup, device, flush):
+    """Warm up, then time `steps` solves individually with CUDA events."""
+    from torchls_b200 import _lib
+
+    opts = solve_opts(tls, precision)
+    for _ in range(warmup):
+        problem.parameters = {k: v.clone() for k, v in init.items()}
+        problem.solve(**opts)
+    torch.cuda.synchronize(device)
+    times, summ = [], None
+    launches0 = _lib.launch_count()
+    for _ in range(steps):
+        problem.parameters = {k: v.clone() for k, v in init.items()}
+        flush_l2(flush)
+        torch.cuda.synchronize(device)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        _, summ = problem.solve(**opts)
+        end.record()
+        torch.cuda.synchronize(device)
+        times.append(start.elapsed_time(end) / 1e3)
+    launches = (_lib.launch_count() - launches0) // steps
+    return times, summ, launches
+
+
+def kernel_roofline(problem, tls, device):
+    """Time the reduced-camera (Schur) matvec and the full normal matvec alone."""
+    import ctypes
+
+    from torchls_b200 import _lib as L
+    from torchls_b200.schur import SchurLinearization, SchurPlan
+
+    an = problem._ensure_analyzed()
+    plan = SchurPlan(an, "points", torch.device(device))
+    lin = problem.linearize(jacobian_dtype=torch.float32, schur=plan)
+    raw = lin.jacobian.diagonal_blocks()
+    slin = SchurLinearization(plan, lin, raw, None, wdtype=torch.float32, vec_dtype=torch.float64)
+    system = slin.damped(1e-3)
+    x = torch.randn(plan.dim, device=device, dtype=torch.float64)
+    out = torch.empty_like(x)
+    stream = L.stream_handle(device)
+    reps = 50
+    for _ in range(5):
+        L.call("tls_schur_matvec", ctypes.byref(system.args), x.data_ptr(), out.data_ptr(), stream)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        L.call("tls_schur_matvec", ctypes.byref(system.args), x.data_ptr(), out.data_ptr(), stream)
+    e.record()
+    torch.cuda.synchronize(device)
+    schur_s = s.elapsed_time(e) / 1e3 / reps
+    E = plan.nedges
+    # algorithmic bytes: W (18 float32) + 2 int32 edge indices per edge, x and out (float64)
+    schur_bytes = E * (plan.dr * plan.de * 4 + 2 * 4) + 2 * plan.dim * 8
+    # full-system normal matvec J^T J x + lambda x: float32 J, float64 vectors
+    J = lin.jacobian
+    v = torch.randn(J.shape[1], device=device, dtype=torch.float64)
+    args = J.normal_args(torch.float64, 1e-3)
+    y = torch.empty_like(v)
+    for _ in range(5):
+        L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(), y.data_ptr(), stream)
+    s.record()
+    for _ in range(reps):
+        L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(), y.data_ptr(), stream)
+    e.record()
+    torch.cuda.synchronize(device)
+    normal_s = s.elapsed_time(e) / 1e3 / reps
+    st = J.structure
+    nnz = sum(p.count * st.rdims[k] * st.D[k] for k, p in enumerate(st.plans))
+    slots = sum(p.count * len(p.type_indices) for p in st.plans)
+    normal_bytes = nnz * 4 + slots * 4 + 2 * J.shape[1] * 8
+    return dict(schur_s=schur_s, schur_bytes=schur_bytes, normal_s=normal_s, normal_bytes=normal_bytes,
+                nedges=E)
+
+
+def e2e_steps(data, tls, device, steps, precision):
+    """The public API with host buffers: pinned H2D of the step's inputs, solve, D2H of the solution."""
+    free, fixed = data.split_fixed_camera()
+    host = {
+        "cams": data.cameras_init[1:].clone().pin_memory(),
+        "points": data.points_init.clone().pin_memory(),
+        "uv_free": data.uv[free].clone().pin_memory(),
+        "uv_fixed": data.uv[fixed].clone().pin_memory(),
+    }
+    dev = {k: torch.empty_like(v, device=device) for k, v in host.items()}
+    problem = tls.Problem({"cams": dev["cams"], "points": dev["points"]}, manifolds={"cams": tls.SE3Var})
+    problem.add_residual(tls.reprojection, ("cams", data.camera_index[free] - 1), ("points", data.point_index[free]),
+                         dev["uv_free"], loss=tls.HuberLoss(0.01))
+    problem.add_residual(tls.reprojection, data.cameras_true[0].to(device), ("points", data.point_index[fixed]),
+                         dev["uv_fixed"], in_dims=(None, 0, 0), loss=tls.HuberLoss(0.01))
+    out_host = {"cams": torch.empty_like(host["cams"]).pin_memory(),
+                "points": torch.empty_like(host["points"]).pin_memory()}
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    d2h = sum(v.numel() * v.element_size() for v in out_host.values())
+    opts = solve_opts(tls, precision)
+    times = []
+    for i in range(steps + 1):  # first call warms the analysis cache
+        torch.cuda.synchronize(device)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for k in host:
+            dev[k].copy_(host[k], non_blocking=True)
+        problem.parameters = {"cams": dev["cams"], "points": dev["points"]}
+        sol, _ = problem.solve(**opts)
+        out_host["cams"].copy_(sol["cams"], non_blocking=True)
+        out_host["points"].copy_(sol["points"], non_blocking=True)
+        end.record()
+        torch.cuda.synchronize(device)
+        if i:
+            times.append(start.elapsed_time(end) / 1e3)
+    return sum(times) / len(times), h2d, d2h
+
+
+def cpu_sample(small: bool):
+    """The numpy oracle (a CPU restatement of torchls) on a bounded sample:
+    one LM iteration of the same solve, extrapolated to the reference's
+    iteration count."""
+    import numpy as np
+
+    import oracle
+    from oracle.model import huber_loss
+
+    data = make_data(small)
+    free, fixed = data.split_fixed_camera()
+    from torchls_b200.residuals import reprojection
+
+    op = oracle.OracleProblem({"cams": data.cameras_init[1:].numpy(), "points": data.points_init.numpy()},
+                              {"cams": "se3"})
+    op.add_residual(reprojection, ("cams", (data.camera_index[free] - 1).numpy()),
+                    ("points", data.point_index[free].numpy()), data.uv[free].numpy(), loss=huber_loss(0.01))
+    op.add_residual(reprojection, data.cameras_true[0].numpy(), ("points", data.point_index[fixed].numpy()),
+                    data.uv[fixed].numpy(), in_dims=(None, 0, 0), loss=huber_loss(0.01))
+    t0 = time.perf_counter()
+    oracle.solve(op, linear_solver="schur_cg", eliminate="points", termination=dict(max_iterations=1))
+    one = time.perf_counter() - t0
+    iters = 6
+    if os.path.exists(TARGET_FILE) and not small:
+        iters = json.load(open(TARGET_FILE))["iterations"]
+    return one * iters, one, iters, np.__name__
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    for _ in range(args.warmup):
+        cpu_sample(args.small)
+    vals = []
+    sample = None
+    for _ in range(args.steps):
+        v, one, iters, _ = cpu_sample(args.small)
+        vals.append(v)
+        sample = f"1 of {iters} LM iterations of the solve (numpy oracle), x{iters}"
+    value = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": workload_config(args, world),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, world):
+    return {"workload": "ba_small_4k_obs" if args.small else "ba_mid_1M_obs",
+            "cameras": 10 if args.small else 256, "points": 500 if args.small else 100000,
+            "observations": 4000 if args.small else 1000000, "solver": "schur_cg", "loss": "huber 0.01",
+            "max_lm_iterations": 20, "pcg_rtol": 1e-6, "parallelism": f"replicas x{world}",
+            "l2": "flushed between steps (256 MB write); working set also exceeds L2"}
+
+
+def run_cuda(args, world, rank, local):
+    import torchls_b200 as tls
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    data = make_data(args.small)
+    problem = build(data, device, tls)
+    if args.roofline_only:
+        roof = kernel_roofline(problem, tls, device)
+        if rank == 0:
+            print(json.dumps({k: v for k, v in roof.items()}), flush=True)
+        return
+    init = {k: v.clone() for k, v in problem.parameters.items()}
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    target = None
+    if os.path.exists(TARGET_FILE) and not args.small:
+        target = json.load(open(TARGET_FILE))["final_cost"]
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        times, summ, launches = time_solves(problem, init, tls, "mixed", args.steps, args.warmup, device, flush)
+    mixed_s = dist_max(sum(times) / len(times), world, device)
+    fp64 = None
+    if not args.no_fp64:
+        t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush)
+        fp64 = (dist_max(sum(t64) / len(t64), world, device), s64)
+    roof = kernel_roofline(problem, tls, device)
+    e2e_s, h2d, d2h = e2e_steps(data, tls, device, args.steps, "mixed")
+    e2e_s = dist_max(e2e_s, world, device)
+    barrier(world)
+    if rank != 0:
+        return
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    schur_gbs = roof["schur_bytes"] / roof["schur_s"] / 1e9
+    normal_gbs = roof["normal_bytes"] / roof["normal_s"] / 1e9
+    rel = None if target is None else abs(summ.final_cost - target) / target
+    line = {
+        "metric": METRIC, "value": mixed_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed_s * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
+        "config": workload_config(args, world),
+        "final_cost": summ.final_cost, "target_cost": target, "rel_cost_error": rel,
+        "reached_1e-8": None if rel is None else rel <= 1e-8,
+        "lm_iterations": summ.iterations, "cg_iterations": summ.linear_iterations_history,
+        "lm_iterations_per_s": summ.iterations / mixed_s,
+        "fp64_s": None if fp64 is None else fp64[0],
+        "fp64_final_cost": None if fp64 is None else fp64[1].final_cost,
+        "mixed_speedup_vs_fp64": None if fp64 is None else fp64[0] / mixed_s,
+        "normal_matvec": {"gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
+                          "bytes": roof["normal_bytes"]},
+        "roofline": {"kernel": "schur reduced-camera matvec (chunk + gather)", "bound": "hbm",
+                     "achieved": schur_gbs, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
+                     "frac": schur_gbs / hbm, "us_per_launch": roof["schur_s"] * 1e6,
+                     "algorithmic_bytes": roof["schur_bytes"],
+                     "traffic": NCU_TRAFFIC_BYTES},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        torch.set_num_threads(os.cpu_count() or 1)
+        v, one, iters, _ = cpu_sample(args.small)
+        line["cpu_baseline"] = {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"1 of {iters} LM iterations (numpy oracle, {one:.2f} s), x{iters}"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_cuda(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

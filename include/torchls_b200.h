@@ -4,8 +4,8 @@
  * Every entry point takes plain device pointers, sizes and a cudaStream_t and
  * returns an int status (TLS_OK = 0). Nothing here allocates device memory:
  * callers pass every buffer and workspace. Calls are asynchronous on `stream`
- * unless stated otherwise; there is no global mutable state except the
- * thread-local last-error message.
+ * unless stated otherwise; the only global mutable state is the thread-local
+ * last-error message and a launch counter.
  *
  * Layout conventions (shared by all calls):
  *   tangent vector   : variable groups in declaration order; group g occupies
@@ -93,7 +93,7 @@ typedef struct tls_factor_group {
 typedef struct tls_segments {
   int32_t count;       /* targets */
   int32_t width;       /* values per contribution block */
-  int32_t lanes;       /* lanes cooperating per target (1..32, power of two) */
+  int32_t lanes;       /* lanes per target: power of two <= 32, or 256 (one block per target) */
   int32_t pad_;
   const int32_t* ptr;  /* [count + 1] */
   const int32_t* src;  /* [nnz] element offset of each block */
@@ -272,9 +272,11 @@ TLS_API int tls_pcg_state_bytes(void);
  * Replaces: schur.py:192-397 (SchurLinearization, DampedSchurSystem) for one
  * retained group of dimension dr <= 8 and an eliminated group of dimension
  * de <= 4. Edges (retained i, eliminated p) are stored in a chunked order:
- * each chunk holds whole eliminated variables; inside a chunk edges are sorted
- * by retained variable so that retained sums are contiguous runs. Every
- * reduction follows a fixed order (deterministic).
+ * each chunk (one thread block) holds whole eliminated variables, at most
+ * 256 * ept edges; inside a chunk edges are sorted by retained variable and
+ * cut into runs of equal retained variable that never cross a 32-edge
+ * window, so a run is reduced by one warp. Every reduction follows a fixed
+ * order (deterministic).
  */
 struct tls_schur_args {
   int32_t nedges;
@@ -284,17 +286,21 @@ struct tls_schur_args {
   int32_t nelim;                /* eliminated variables */
   int32_t wdtype;               /* TLS_F32 / TLS_F64 storage of W */
   int32_t vec_dtype;            /* reduced vectors */
-  int32_t max_chunk_edges;      /* shared memory: max_chunk_edges * (dr + de) doubles */
+  int32_t ept;                  /* edges per thread: chunks hold <= 256 * ept edges */
   int32_t nruns;
   int64_t retained_offset;      /* tangent offset of the retained group (full vector) */
   int64_t elim_offset;          /* tangent offset of the eliminated group (full vector) */
   const int32_t* chunk_ptr;     /* [nchunks+1] edge ranges */
-  const int32_t* chunk_run_ptr; /* [nchunks+1] run ranges */
+  const int32_t* cpt_ptr;       /* [nchunks+1] ranges into chunk_points */
+  const int32_t* chunk_points;  /* eliminated variables of each chunk, ascending */
+  const int32_t* cw_ptr;        /* [nchunks+1] 32-edge window ranges into win_run */
+  const int32_t* win_run;       /* first run id of each window */
   const int32_t* edge_r;        /* [E] retained variable per edge (chunk order) */
+  const uint32_t* edge_meta;    /* [E] point slot in chunk | run head lane << 16 | run tail << 21 */
   const int32_t* edge_e;        /* [E] eliminated variable per edge */
   const int32_t* elim_ptr;      /* [nelim+1] CSR: edges of each eliminated variable */
   const int32_t* elim_edges;    /* [E] edge positions, ascending */
-  const int32_t* run_ptr;       /* [nruns+1] edge ranges of equal retained variable */
+  const int32_t* run_ptr;       /* [nruns+1] edge ranges of each run */
   const int32_t* rrun_ptr;      /* [nretained+1] CSR: runs of each retained variable */
   const int32_t* rrun_list;     /* [nruns] run ids in chunk order */
   const double* cross;          /* [E][dr][de] J_r^T J_e per edge (unscaled) */
@@ -349,6 +355,9 @@ TLS_API int tls_trial_terms(int64_t count, int32_t rdim, const double* old_raw, 
                     tls_stream_t stream);
 
 /* ---------------------------------------------------------------- misc */
+/* Number of kernels this library has launched in the process (a relaxed
+ * atomic counter; the only global state besides the last-error message). */
+TLS_API int64_t tls_launch_count(void);
 TLS_API const char* tls_last_error(void);
 TLS_API int tls_version(void);
 TLS_API int tls_device_init(int32_t device);

@@ -38,7 +38,14 @@ def close(a, b, rtol, atol=0.0, what=""):
     assert err <= rtol * scale + atol, f"{what}: max err {err:.3e} vs scale {scale:.3e} (rtol {rtol:g})"
 
 
-def check_summary(s, ref, *, histories=True, counts=True, cost_rtol=1e-10):
+def check_summary(s, ref, *, histories=True, counts=True, cost_rtol=1e-10, cg_slack=0):
+    """Compare a SolveSummary with the reference's.
+
+    ``cg_slack`` allows CG iteration counts to differ by that many per linear
+    solve: for CG runs of ~180 iterations the float64 summation order of the
+    dot products (deterministic but not torch's) can move the rtol crossing
+    by one iteration.
+    """
     assert s.termination_reason == ref["termination_reason"], (s.termination_reason, ref["termination_reason"])
     close(s.final_cost, ref["final_cost"], cost_rtol, what="final_cost")
     if not counts:
@@ -48,6 +55,7 @@ def check_summary(s, ref, *, histories=True, counts=True, cost_rtol=1e-10):
     assert s.rejected_steps == ref["rejected_steps"]
     close(s.initial_cost, ref["initial_cost"], 1e-12, what="initial_cost")
     if histories:
-        assert s.linear_iterations_history == ref["linear_iterations_history"]
+        got, want = s.linear_iterations_history, ref["linear_iterations_history"]
+        assert len(got) == len(want) and all(abs(a - b) <= cg_slack for a, b in zip(got, want)), (got, want)
         close(s.lambda_history, ref["lambda_history"], 1e-12, what="lambda_history")
         close(s.cost_history, ref["cost_history"], 1e-8, what="cost_history")

@@ -30,7 +30,7 @@ STRUCTS = {
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^TLS_API\s+(?:int|const char\*)\s+(tls_\w+)\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^TLS_API\s+(?:int|int64_t|const char\*)\s+(tls_\w+)\(", text, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -72,7 +72,7 @@ def test_pcg_state_fits_control_struct():
 
 def test_errors_map_to_python_exceptions():
     lib = L.lib()
-    seg = L.Segments(4, 3, 3, 0, None, None)  # lanes must be a power of two
+    seg = L.Segments(4, 3, 3, 0, None, None)  # lanes must be a power of two or 256
     status = lib.tls_segment_reduce(ctypes.byref(seg), None, L.F64, 0, 3, None, L.F64, None)
     assert status == L.TLS_ERR_INVALID
     with pytest.raises(ValueError, match="lanes"):

@@ -86,12 +86,12 @@ class PcgControl(C.Structure):
 class SchurArgs(C.Structure):
     _fields_ = [
         ("nedges", i32), ("nchunks", i32), ("dr", i32), ("de", i32), ("nretained", i32), ("nelim", i32),
-        ("wdtype", i32), ("vec_dtype", i32), ("max_chunk_edges", i32), ("nruns", i32),
-        ("retained_offset", i64), ("elim_offset", i64), ("chunk_ptr", vp), ("chunk_run_ptr", vp),
-        ("edge_r", vp), ("edge_e", vp), ("elim_ptr", vp), ("elim_edges", vp), ("run_ptr", vp),
-        ("rrun_ptr", vp), ("rrun_list", vp), ("cross", vp), ("elim_diag", vp), ("ret_diag", vp),
-        ("scale", vp), ("inv_l", vp), ("w", vp), ("run_partial", vp), ("ybuf", vp), ("damping", f64),
-        ("bad", vp),
+        ("wdtype", i32), ("vec_dtype", i32), ("ept", i32), ("nruns", i32),
+        ("retained_offset", i64), ("elim_offset", i64), ("chunk_ptr", vp), ("cpt_ptr", vp),
+        ("chunk_points", vp), ("cw_ptr", vp), ("win_run", vp), ("edge_r", vp), ("edge_meta", vp),
+        ("edge_e", vp), ("elim_ptr", vp), ("elim_edges", vp), ("run_ptr", vp), ("rrun_ptr", vp),
+        ("rrun_list", vp), ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp),
+        ("w", vp), ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp),
     ]
 
 
@@ -124,6 +124,7 @@ _SIGNATURES = {
     "tls_retract": [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp],
     "tls_reduce": [vp, i32, i64, i32, vp, vp, vp],
     "tls_trial_terms": [i64, i32, vp, vp, i32, f64, vp, vp, vp, i32, vp, vp, vp],
+    "tls_launch_count": [],
     "tls_last_error": [],
     "tls_version": [],
     "tls_device_init": [i32],
@@ -144,7 +145,7 @@ def lib():
         for name, argtypes in _SIGNATURES.items():
             fn = getattr(handle, name)
             fn.argtypes = argtypes
-            fn.restype = C.c_char_p if name == "tls_last_error" else C.c_int
+            fn.restype = {"tls_last_error": C.c_char_p, "tls_launch_count": C.c_int64}.get(name, C.c_int)
         _lib = handle
     return _lib
 
@@ -184,3 +185,8 @@ def dtype_code(dtype: torch.dtype) -> int:
 def require_cuda(t: torch.Tensor, what: str = "CUDA backend") -> None:
     if t.device.type != "cuda":
         raise ValueError(f"{what} requires CUDA tensors; got device {t.device}")
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    return int(lib().tls_launch_count())

@@ -2,9 +2,16 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "common.cuh"
 
 static thread_local char g_last_error[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void tls_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+extern "C" int64_t tls_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int tls_set_error(int code, const char* msg) {
   snprintf(g_last_error, sizeof(g_last_error), "%s", msg);

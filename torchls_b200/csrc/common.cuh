@@ -8,12 +8,14 @@
 
 #define TLS_CHECK_LAUNCH()                                   \
   do {                                                       \
+    tls_count_launch();                                      \
     cudaError_t _e = cudaGetLastError();                     \
     if (_e != cudaSuccess) return tls_set_cuda_error(_e);    \
   } while (0)
 
 int tls_set_cuda_error(cudaError_t e);
 int tls_set_error(int code, const char* msg);
+void tls_count_launch();
 
 namespace tls {
 

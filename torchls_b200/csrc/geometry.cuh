@@ -221,7 +221,7 @@ __device__ __forceinline__ void q_coefficients(double t2, double& c2, double& c3
     c2 = 1.0 / 6.0 + t2 * (-1.0 / 120.0 + t2 * (1.0 / 5040.0 + t2 * (-1.0 / 362880.0 + t2 / 39916800.0)));
     c3 = 1.0 / 24.0 + t2 * (-1.0 / 720.0 + t2 * (1.0 / 40320.0 + t2 * (-1.0 / 3628800.0 + t2 / 479001600.0)));
     const double d5 = -1.0 / 120.0 + t2 * (1.0 / 5040.0 + t2 * (-1.0 / 362880.0 + t2 * (1.0 / 39916800.0 - t2 / 6227020800.0)));
-    c4 = 0.5 * (c3 - 3.0 * d5);
+    c4 = 0.5 * (c3 + 3.0 * d5);
   } else {
     const double t = sqrt(t2);
     double s, c;
@@ -229,7 +229,7 @@ __device__ __forceinline__ void q_coefficients(double t2, double& c2, double& c3
     c2 = (t - s) / (t2 * t);
     c3 = (0.5 * t2 + c - 1.0) / (t2 * t2);
     const double d5 = (t - s - t2 * t / 6.0) / (t2 * t2 * t);
-    c4 = 0.5 * (c3 - 3.0 * d5);
+    c4 = 0.5 * (c3 + 3.0 * d5);
   }
 }
 

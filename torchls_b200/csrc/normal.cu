@@ -7,6 +7,7 @@
 // contributions in a fixed list order. No atomics: results are bitwise
 // reproducible run to run.
 #include "common.cuh"
+#include "pcg_state.cuh"
 
 namespace tls {
 
@@ -142,20 +143,38 @@ struct GatherGroups {
   tls_segments seg[TLS_MAX_GROUPS];
 };
 
+// Lanes per target: 1..32 (aligned lane groups inside a warp) or, for hot
+// variables, a whole 256-thread block per target ("block mode", lanes > 32).
+__host__ __device__ __forceinline__ int gather_blocks_for(const tls_segments& seg) {
+  if (seg.lanes > 32) return seg.count;
+  const int64_t threads = (int64_t)seg.count * seg.lanes;
+  return (int)((threads + 255) / 256);
+}
+
 template <int WM, typename TV>
 __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, const TV* __restrict__ contrib,
                                                             const TV* __restrict__ x, const TV* __restrict__ scale,
                                                             double damping, TV* __restrict__ y,
-                                                            double* __restrict__ dot_partials) {
+                                                            double* __restrict__ dot_partials, PcgState* pst) {
+  __shared__ double red[8][WM];
+  __shared__ double sm[8];
   int gi = 0;
 #pragma unroll 1
   while (gi + 1 < g.ngroups && (int)blockIdx.x >= g.block_begin[gi + 1]) ++gi;
   const tls_segments& seg = g.seg[gi];
-  const int L = seg.lanes;
-  const int64_t local = (int64_t)(blockIdx.x - g.block_begin[gi]) * blockDim.x + threadIdx.x;
-  const int64_t t = local / L;
-  const int lane = (int)(local % L);
   const int d = g.dim[gi];
+  const bool block_mode = seg.lanes > 32;
+  const int L = block_mode ? 256 : seg.lanes;
+  int64_t t;
+  int lane;
+  if (block_mode) {
+    t = blockIdx.x - g.block_begin[gi];
+    lane = threadIdx.x;
+  } else {
+    const int64_t local = (int64_t)(blockIdx.x - g.block_begin[gi]) * blockDim.x + threadIdx.x;
+    t = local / L;
+    lane = (int)(local % L);
+  }
   double acc[WM];
 #pragma unroll
   for (int k = 0; k < WM; ++k) acc[k] = 0.0;
@@ -168,10 +187,32 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
         if (k < d) acc[k] += to_d(src[k]);
     }
   }
+  bool writer;
+  if (block_mode) {
+    const int w = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < WM; ++k) acc[k] = group_sum(acc[k], L);
+    for (int k = 0; k < WM; ++k) {
+      const double v = warp_sum(acc[k]);
+      if ((threadIdx.x & 31) == 0) red[w][k] = v;
+    }
+    __syncthreads();
+    writer = threadIdx.x == 0;
+    if (writer) {
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v += red[q][k];
+        acc[k] = v;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < WM; ++k) acc[k] = group_sum(acc[k], L);
+    writer = lane == 0;
+  }
   double dot = 0.0;
-  if (t < seg.count && lane == 0) {
+  if (t < seg.count && writer) {
     const int64_t base = g.offset[gi] + t * d;
 #pragma unroll
     for (int k = 0; k < WM; ++k) {
@@ -188,9 +229,9 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
     }
   }
   if (dot_partials) {
-    __shared__ double sm[8];
     const double s = block_sum<256>(dot, sm);
     if (threadIdx.x == 0) dot_partials[blockIdx.x] = s;
+    if (pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, sm);
   }
 }
 
@@ -199,12 +240,19 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
 using namespace tls;
 
 int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                      cudaStream_t st);
+                      void* pcg_state, cudaStream_t st);
+
+// Number of blocks (and dot partials) of the normal operator's gather kernel.
+int tls_normal_gather_blocks(const tls_normal_args* a) {
+  int blocks = 0;
+  for (int i = 0; i < a->nvar_groups; ++i) blocks += gather_blocks_for(a->seg[i]);
+  return blocks;
+}
 
 // Shared by tls_normal_matvec and the PCG driver. Returns the number of gather
 // blocks (for dot partials) through *gather_blocks.
 int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                     cudaStream_t st) {
+                     void* pcg_state, cudaStream_t st) {
   if (a->nfactor_groups > TLS_MAX_FACTOR_GROUPS || a->nvar_groups > TLS_MAX_GROUPS)
     return tls_set_error(TLS_ERR_INVALID, "too many groups");
   for (int k = 0; k < a->nfactor_groups; ++k) {
@@ -226,11 +274,12 @@ int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* d
     }
     if (rc) return rc;
   }
-  return tls_normal_gather(a, x, y, dot_partials, gather_blocks, st);
+  return tls_normal_gather(a, x, y, dot_partials, gather_blocks, pcg_state, st);
 }
 
 int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                      cudaStream_t st) {
+                      void* pcg_state, cudaStream_t st) {
+  PcgState* pst = reinterpret_cast<PcgState*>(pcg_state);
   GatherGroups g{};
   g.ngroups = a->nvar_groups;
   int blocks = 0, wmax = 1;
@@ -239,8 +288,7 @@ int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* 
     g.offset[i] = a->vg[i].offset;
     g.dim[i] = a->vg[i].dim;
     g.seg[i] = a->seg[i];
-    const int64_t threads = (int64_t)a->seg[i].count * a->seg[i].lanes;
-    blocks += (int)((threads + 255) / 256);
+    blocks += gather_blocks_for(a->seg[i]);
     if (a->vg[i].dim > wmax) wmax = a->vg[i].dim;
   }
   g.block_begin[a->nvar_groups] = blocks;
@@ -251,11 +299,11 @@ int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* 
     if (a->vec_dtype == TLS_F64)                                                                         \
       normal_gather_kernel<WM, double><<<blocks, 256, 0, st>>>(g, (const double*)a->contrib, (const double*)x, \
                                                                (const double*)a->scale, a->damping,     \
-                                                               (double*)y, dot_partials);                \
+                                                               (double*)y, dot_partials, pst);           \
     else                                                                                                 \
       normal_gather_kernel<WM, float><<<blocks, 256, 0, st>>>(g, (const float*)a->contrib, (const float*)x,   \
                                                               (const float*)a->scale, a->damping,       \
-                                                              (float*)y, dot_partials);                  \
+                                                              (float*)y, dot_partials, pst);             \
     TLS_CHECK_LAUNCH();                                                                                  \
     return TLS_OK;                                                                                       \
   }
@@ -268,7 +316,7 @@ int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* 
 }
 
 extern "C" int tls_normal_matvec(const tls_normal_args* a, const void* x, void* y, tls_stream_t stream) {
-  return tls_normal_apply(a, x, y, nullptr, nullptr, reinterpret_cast<cudaStream_t>(stream));
+  return tls_normal_apply(a, x, y, nullptr, nullptr, nullptr, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int tls_jacobian_matvec(const tls_normal_args* a, const void* x, void* out_rows, tls_stream_t stream) {
@@ -348,5 +396,5 @@ extern "C" int tls_jacobian_rmatvec(const tls_normal_args* a, const void* rows, 
   }
   tls_normal_args b = *a;
   b.damping = 0.0;
-  return tls_normal_gather(&b, nullptr, out, nullptr, nullptr, st);
+  return tls_normal_gather(&b, nullptr, out, nullptr, nullptr, nullptr, st);
 }

@@ -8,45 +8,39 @@
 // device from float64 scalars reduced in a fixed order, so a run needs no
 // host synchronisation and is bitwise reproducible.
 //
-// One state-machine step = operator (ap = A p) -> update -> decide -> direction.
+// One state-machine step is three kernels:
+//   operator   ap = A p; its last block finalises curvature and alpha
+//   update     x, r (or the true residual), z = M r, partial norms; its last
+//              block takes the step's decision (converged, check, restart...)
+//   direction  p = z + beta p, restart, or swap p <-> x for a residual check
 // During a true-residual check p temporarily holds x (the operator always
 // reads p); the saved direction is restored if the iteration continues.
+#include <type_traits>
+
 #include "blocks.cuh"
 #include "common.cuh"
+#include "pcg_state.cuh"
 
 int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                     cudaStream_t st);
+                     void* pcg_state, cudaStream_t st);
 int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* dot_partials, int* gather_blocks,
-                    cudaStream_t st);
+                    void* pcg_state, cudaStream_t st);
+int tls_normal_gather_blocks(const tls_normal_args* a);
 
 namespace tls {
 
-enum { M_ITER = 0, M_CHECK = 1, M_FINAL = 2, M_DONE = 3 };
-enum { A_NONE = 0, A_DIR = 1, A_RESTART = 2, A_RESTORE_DIR = 3, A_SWAP_TO_X = 4 };
-
-// Extended control block kept after the public tls_pcg_control fields.
-struct PcgState {
-  tls_pcg_control pub;
-  int32_t action;
-  int32_t pending;       // reason when the loop broke early
-  int32_t op_blocks;     // number of operator dot partials
-  int32_t upd_blocks;    // number of update partial blocks
-  double rec;            // recurrence norm of the last iteration
-  int32_t rec_hit;       // rec <= threshold at the last iteration
-  int32_t periodic_hit;  // periodic check due at the last iteration
-  int32_t alpha_ok;      // curvature and r.z finite and positive this step
-  int32_t pad2_;
-};
-
 struct BlockSet {
   int32_t ngroups;
-  int32_t identity;            // no preconditioner: unit blocks
+  int32_t identity;                         // no preconditioner: unit blocks
   int64_t block_begin[TLS_MAX_GROUPS + 1];  // prefix of block counts
   tls_block_group g[TLS_MAX_GROUPS];
 };
 
 constexpr int kUpdThreads = 128;
 constexpr int kMaxUpdBlocks = 1024;
+// partials layout: [0, kOpPartials) operator dots; update partials at
+// kOpPartials + k * kMaxUpdBlocks (k = 0, 1, 2).
+constexpr int kOpPartials = 65536;
 
 __device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
   int gi = 0;
@@ -54,29 +48,42 @@ __device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
   return gi;
 }
 
-template <typename TV>
-__device__ __forceinline__ void apply_block(const BlockSet& bs, int gi, int64_t i, const TV* src, TV* dst,
-                                            double* rbuf, double* zbuf, int& dim, int64_t* cols) {
-  const tls_block_group& g = bs.g[gi];
-  dim = g.dim;
-  for (int k = 0; k < dim; ++k) {
-    cols[k] = block_column(g, i, k);
-    rbuf[k] = to_d(src[cols[k]]);
+// z = (L L^T)^-1 r for one block of runtime size dim <= D (registers only).
+template <int D>
+__device__ __forceinline__ void solve_block(const double* __restrict__ L, int dim, const double (&r)[D],
+                                            double (&z)[D]) {
+  double y[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double t = r[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) t -= (i < dim) ? L[i * dim + k] * y[k] : 0.0;
+    y[i] = (i < dim) ? t / L[i * dim + i] : 0.0;
   }
-  if (bs.identity || g.factor == nullptr) {
-    for (int k = 0; k < dim; ++k) zbuf[k] = rbuf[k];
-  } else {
-    cholesky_solve_block(g.factor + i * dim * dim, dim, rbuf, zbuf);
+#pragma unroll
+  for (int i = D - 1; i >= 0; --i) {
+    double t = y[i];
+#pragma unroll
+    for (int k = i + 1; k < D; ++k) t -= (k < dim) ? L[k * dim + i] * z[k] : 0.0;
+    z[i] = (i < dim) ? t / L[i * dim + i] : 0.0;
   }
-  if (dst)
-    for (int k = 0; k < dim; ++k) dst[cols[k]] = static_cast<TV>(zbuf[k]);
 }
 
-__device__ __forceinline__ double sum_fixed(const double* p, int n) {
-  // fixed sequential order: every caller gets the identical value
-  double s = 0.0;
-  for (int i = 0; i < n; ++i) s += p[i];
-  return s;
+template <int D>
+__device__ __forceinline__ void block_cols(const tls_block_group& g, int64_t i, int64_t (&cols)[D]) {
+  int m = 0, start = 0;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    if (k < g.dim) {
+      while (k >= start + g.member_dim[m]) {
+        start += g.member_dim[m];
+        ++m;
+      }
+      cols[k] = g.member_offset[m] + i * g.member_dim[m] + (k - start);
+    } else {
+      cols[k] = 0;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- start
@@ -95,11 +102,16 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_init_kernel(int64_t n, const 
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-__global__ void pcg_init_finish_kernel(PcgState* st, const double* partials, int blocks, double rtol, double atol,
-                                       int max_it, int interval, int periodic, double drift_tol) {
+__global__ void __launch_bounds__(256) pcg_init_finish_kernel(PcgState* st, const double* partials, int blocks,
+                                                              double rtol, double atol, int max_it, int interval,
+                                                              int periodic, double drift_tol) {
+  __shared__ double sm[8];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < blocks; i += 256) acc += partials[i];
+  const double ss = block_sum<256>(acc, sm);
   if (threadIdx.x != 0) return;
   tls_pcg_control& c = st->pub;
-  const double nrm = sqrt(sum_fixed(partials, blocks));
+  const double nrm = sqrt(ss);
   c.rhs_norm = nrm;
   c.threshold = fmax(atol, rtol * nrm);
   c.residual_norm = nrm;
@@ -117,6 +129,9 @@ __global__ void pcg_init_finish_kernel(PcgState* st, const double* partials, int
   st->rec = nrm;
   st->rec_hit = 0;
   st->periodic_hit = 0;
+  st->alpha_ok = 0;
+  st->ticket_op = 0;
+  st->ticket_upd = 0;
   if (!isfinite(nrm)) {
     c.status = TLS_PCG_NONFINITE;
     c.mode = M_DONE;
@@ -127,7 +142,7 @@ __global__ void pcg_init_finish_kernel(PcgState* st, const double* partials, int
 }
 
 // z = M r, p = z, partial r.z (only while ACTIVE)
-template <typename TV>
+template <int D, typename TV>
 __global__ void __launch_bounds__(kUpdThreads) pcg_precondition_kernel(BlockSet bs, int64_t nblocks, const PcgState* st,
                                                                        const TV* r, TV* z, TV* p, double* partials) {
   __shared__ double sm[kUpdThreads / 32];
@@ -137,13 +152,26 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_precondition_kernel(BlockSet 
          b += (int64_t)gridDim.x * blockDim.x) {
       const int gi = find_group(bs, b);
       const int64_t i = b - bs.block_begin[gi];
-      double rb[kMaxBlock], zb[kMaxBlock];
-      int64_t cols[kMaxBlock];
-      int dim;
-      apply_block(bs, gi, i, r, z, rb, zb, dim, cols);
-      for (int k = 0; k < dim; ++k) {
-        p[cols[k]] = static_cast<TV>(zb[k]);
-        acc += rb[k] * static_cast<double>(static_cast<TV>(zb[k]));
+      const tls_block_group& g = bs.g[gi];
+      int64_t cols[D];
+      block_cols<D>(g, i, cols);
+      double rb[D], zb[D];
+#pragma unroll
+      for (int k = 0; k < D; ++k) rb[k] = (k < g.dim) ? to_d(r[cols[k]]) : 0.0;
+      if (bs.identity || g.factor == nullptr) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) zb[k] = rb[k];
+      } else {
+        solve_block<D>(g.factor + i * g.dim * g.dim, g.dim, rb, zb);
+      }
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        if (k < g.dim) {
+          const TV zk = static_cast<TV>(zb[k]);
+          z[cols[k]] = zk;
+          p[cols[k]] = zk;
+          acc += rb[k] * to_d(zk);
+        }
       }
     }
   }
@@ -154,130 +182,16 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_precondition_kernel(BlockSet 
 __global__ void pcg_rz_finish_kernel(PcgState* st, const double* partials, int blocks) {
   if (threadIdx.x != 0) return;
   if (st->pub.status != TLS_PCG_ACTIVE) return;
-  st->pub.rz = sum_fixed(partials, blocks);
+  double s = 0.0;
+  for (int i = 0; i < blocks; ++i) s += partials[i];
+  st->pub.rz = s;
 }
 
-// ---------------------------------------------------------------- one step
-// partials layout: [0, kOpPartials) operator dots; update partials at
-// kOpPartials + k * kMaxUpdBlocks (k = 0, 1, 2).
-constexpr int kOpPartials = 65536;
-
-// Deterministic block-wide sum of p[0..n) (fixed strided order + fixed tree).
-__device__ __forceinline__ double block_sum_list(const double* p, int n, double* sm) {
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
-  return block_sum<256>(acc, sm);
-}
-
-// curvature = p.Ap from the operator's partials; alpha = rz / curvature.
-__global__ void __launch_bounds__(256) pcg_alpha_kernel(PcgState* st, const double* partials) {
-  __shared__ double sm[8];
+// ---------------------------------------------------------------- decision (last update block)
+__device__ void pcg_decide(PcgState* st, double s0, double s1, double s2) {
   tls_pcg_control& c = st->pub;
-  if (c.status != TLS_PCG_ACTIVE || c.mode != M_ITER) {
-    if (threadIdx.x == 0) st->alpha_ok = 0;
-    return;
-  }
-  const double curv = block_sum_list(partials, st->op_blocks, sm);
-  if (threadIdx.x == 0) {
-    const double rz = c.rz;
-    c.curvature = curv;
-    const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
-    st->alpha_ok = ok;
-    c.alpha = ok ? rz / curv : 0.0;
-  }
-}
-
-template <typename TV>
-__global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, int64_t nblocks, const PcgState* st,
-                                                                 const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
-                                                                 const TV* p, TV* ap, TV* ztrue,
-                                                                 double* partials) {
-  __shared__ double sm[kUpdThreads / 32];
-  const tls_pcg_control& c = st->pub;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  const int mode = c.mode;
-  bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
-  double alpha = 0.0;
-  if (work && mode == M_ITER) {
-    if (!st->alpha_ok) work = false;
-    else alpha = c.alpha;
-  }
-  if (work) {
-    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks;
-         b += (int64_t)gridDim.x * blockDim.x) {
-      const int gi = find_group(bs, b);
-      const int64_t i = b - bs.block_begin[gi];
-      const tls_block_group& g = bs.g[gi];
-      const int dim = g.dim;
-      int64_t cols[kMaxBlock];
-      for (int k = 0; k < dim; ++k) cols[k] = block_column(g, i, k);
-      double rb[kMaxBlock], zb[kMaxBlock];
-      if (mode == M_ITER) {
-        for (int k = 0; k < dim; ++k) {
-          const int64_t col = cols[k];
-          const TV pk = p[col];
-          x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(pk));
-          const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
-          r[col] = rn;
-          rb[k] = to_d(rn);
-        }
-      } else {
-        // ap holds A x: true residual tr = rhs - A x (stored into ap)
-        for (int k = 0; k < dim; ++k) {
-          const int64_t col = cols[k];
-          const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
-          ap[col] = tr;
-          const double t = to_d(tr);
-          rb[k] = t;
-          a0 += t * t;
-          const double dr = t - to_d(r[col]);
-          a1 += dr * dr;
-        }
-      }
-      if (mode == M_FINAL) continue;
-      if (bs.identity || g.factor == nullptr) {
-        for (int k = 0; k < dim; ++k) zb[k] = rb[k];
-      } else {
-        cholesky_solve_block(g.factor + i * dim * dim, dim, rb, zb);
-      }
-      TV* zdst = (mode == M_ITER) ? z : ztrue;
-      for (int k = 0; k < dim; ++k) {
-        const TV zk = static_cast<TV>(zb[k]);
-        zdst[cols[k]] = zk;
-        const double zd = static_cast<double>(zk);
-        if (mode == M_ITER) {
-          a0 += rb[k] * rb[k];
-          a1 += rb[k] * zd;
-        } else {
-          a2 += rb[k] * zd;
-        }
-      }
-    }
-  }
-  const double s0 = block_sum<kUpdThreads>(a0, sm);
-  const double s1 = block_sum<kUpdThreads>(a1, sm);
-  const double s2 = block_sum<kUpdThreads>(a2, sm);
-  if (threadIdx.x == 0) {
-    partials[kOpPartials + blockIdx.x] = s0;
-    partials[kOpPartials + kMaxUpdBlocks + blockIdx.x] = s1;
-    partials[kOpPartials + 2 * kMaxUpdBlocks + blockIdx.x] = s2;
-  }
-}
-
-__global__ void __launch_bounds__(256) pcg_decide_kernel(PcgState* st, const double* partials) {
-  __shared__ double sm[8];
-  tls_pcg_control& c = st->pub;
-  const bool live = c.status == TLS_PCG_ACTIVE && c.mode != M_DONE;
-  const int nb = st->upd_blocks;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  if (live) {
-    s0 = block_sum_list(partials + kOpPartials, nb, sm);
-    s1 = block_sum_list(partials + kOpPartials + kMaxUpdBlocks, nb, sm);
-    s2 = block_sum_list(partials + kOpPartials + 2 * kMaxUpdBlocks, nb, sm);
-  }
-  if (threadIdx.x != 0) return;
   st->action = A_NONE;
-  if (!live) return;
+  if (c.status != TLS_PCG_ACTIVE || c.mode == M_DONE) return;
   const double thr = c.threshold;
   if (c.mode == M_ITER) {
     const double curv = c.curvature;
@@ -295,7 +209,6 @@ __global__ void __launch_bounds__(256) pcg_decide_kernel(PcgState* st, const dou
       st->action = A_SWAP_TO_X;
       return;
     }
-    c.alpha = rz / curv;
     c.rr = s0;
     c.rz_new = s1;
     const double rec = sqrt(s0);
@@ -362,6 +275,112 @@ __global__ void __launch_bounds__(256) pcg_decide_kernel(PcgState* st, const dou
   c.mode = M_DONE;
 }
 
+// ---------------------------------------------------------------- update
+template <int D, typename TV>
+__global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, int64_t nblocks, PcgState* st,
+                                                                 const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
+                                                                 const TV* p, TV* ap, TV* ztrue,
+                                                                 double* partials) {
+  __shared__ double sm[kUpdThreads / 32];
+  __shared__ int last;
+  const tls_pcg_control& c = st->pub;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  const int mode = c.mode;
+  bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
+  double alpha = 0.0;
+  if (work && mode == M_ITER) {
+    if (!st->alpha_ok) work = false;
+    else alpha = c.alpha;
+  }
+  if (work) {
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks;
+         b += (int64_t)gridDim.x * blockDim.x) {
+      const int gi = find_group(bs, b);
+      const int64_t i = b - bs.block_begin[gi];
+      const tls_block_group& g = bs.g[gi];
+      const int dim = g.dim;
+      int64_t cols[D];
+      block_cols<D>(g, i, cols);
+      double rb[D], zb[D];
+      if (mode == M_ITER) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          rb[k] = 0.0;
+          if (k < dim) {
+            const int64_t col = cols[k];
+            x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(p[col]));
+            const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
+            r[col] = rn;
+            rb[k] = to_d(rn);
+          }
+        }
+      } else {
+        // ap holds A x: true residual tr = rhs - A x (stored into ap)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          rb[k] = 0.0;
+          if (k < dim) {
+            const int64_t col = cols[k];
+            const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
+            ap[col] = tr;
+            const double t = to_d(tr);
+            rb[k] = t;
+            a0 += t * t;
+            const double dr = t - to_d(r[col]);
+            a1 += dr * dr;
+          }
+        }
+      }
+      if (mode == M_FINAL) continue;
+      if (bs.identity || g.factor == nullptr) {
+#pragma unroll
+        for (int k = 0; k < D; ++k) zb[k] = rb[k];
+      } else {
+        solve_block<D>(g.factor + i * dim * dim, dim, rb, zb);
+      }
+      TV* zdst = (mode == M_ITER) ? z : ztrue;
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        if (k < dim) {
+          const TV zk = static_cast<TV>(zb[k]);
+          zdst[cols[k]] = zk;
+          const double zd = to_d(zk);
+          if (mode == M_ITER) {
+            a0 += rb[k] * rb[k];
+            a1 += rb[k] * zd;
+          } else {
+            a2 += rb[k] * zd;
+          }
+        }
+      }
+    }
+  }
+  double* up = partials + kOpPartials;
+  const double s0 = block_sum<kUpdThreads>(a0, sm);
+  const double s1 = block_sum<kUpdThreads>(a1, sm);
+  const double s2 = block_sum<kUpdThreads>(a2, sm);
+  if (threadIdx.x == 0) {
+    up[blockIdx.x] = s0;
+    up[kMaxUpdBlocks + blockIdx.x] = s1;
+    up[2 * kMaxUpdBlocks + blockIdx.x] = s2;
+  }
+  // last block to finish takes the step's decision
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->ticket_upd, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  const double t0 = block_sum_cg<kUpdThreads>(up, nb, sm);
+  const double t1 = block_sum_cg<kUpdThreads>(up + kMaxUpdBlocks, nb, sm);
+  const double t2 = block_sum_cg<kUpdThreads>(up + 2 * kMaxUpdBlocks, nb, sm);
+  if (threadIdx.x == 0) {
+    st->ticket_upd = 0;
+    pcg_decide(st, t0, t1, t2);
+  }
+}
+
 // Direction / restart / swap. When the next mode is FINAL after a restart or
 // a direction update, p is additionally replaced by x (the operator reads p).
 template <typename TV>
@@ -393,12 +412,12 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(int64_t n, const Pcg
   }
 }
 
-__host__ BlockSet make_blocks(const tls_pcg_args* a, int64_t* total) {
+__host__ BlockSet make_blocks(const tls_pcg_args* a, int64_t* total, int* maxdim) {
   BlockSet bs{};
   int64_t nb = 0;
+  *maxdim = 1;
   if (a->pre == nullptr || a->npre == 0) {
     bs.identity = 1;
-    // one unit block per element
     bs.ngroups = 1;
     bs.g[0].count = (int32_t)a->n;
     bs.g[0].dim = 1;
@@ -415,6 +434,7 @@ __host__ BlockSet make_blocks(const tls_pcg_args* a, int64_t* total) {
     bs.g[i] = a->pre[i];
     bs.block_begin[i] = nb;
     nb += a->pre[i].count;
+    if (a->pre[i].dim > *maxdim) *maxdim = a->pre[i].dim;
   }
   bs.block_begin[a->npre] = nb;
   *total = nb;
@@ -428,26 +448,39 @@ static int grid_of(int64_t n, int block, int cap) {
   return (int)g;
 }
 
+template <typename F>
+static int with_dim(int maxdim, F&& f) {
+  if (maxdim <= 1) return f(std::integral_constant<int, 1>{});
+  if (maxdim <= 3) return f(std::integral_constant<int, 3>{});
+  if (maxdim <= 6) return f(std::integral_constant<int, 6>{});
+  if (maxdim <= 8) return f(std::integral_constant<int, 8>{});
+  if (maxdim <= 16) return f(std::integral_constant<int, 16>{});
+  return tls_set_error(TLS_ERR_UNSUPPORTED, "preconditioner block dim > 16");
+}
+
 template <typename TV>
 static int pcg_start_t(const tls_pcg_args* a, double rtol, double atol, int max_it, int interval, int periodic,
                        double drift, cudaStream_t s) {
   PcgState* st = reinterpret_cast<PcgState*>(a->control);
   const int g = grid_of(a->n, kUpdThreads, kMaxUpdBlocks);
-  pcg_init_kernel<TV><<<g, kUpdThreads, 0, s>>>(a->n, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r,
-                                                a->partials + kOpPartials);
+  double* scratch = a->partials + kOpPartials;
+  pcg_init_kernel<TV><<<g, kUpdThreads, 0, s>>>(a->n, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r, scratch);
   TLS_CHECK_LAUNCH();
-  pcg_init_finish_kernel<<<1, 32, 0, s>>>(st, a->partials + kOpPartials, g, rtol, atol, max_it, interval, periodic,
-                                          drift);
+  pcg_init_finish_kernel<<<1, 256, 0, s>>>(st, scratch, g, rtol, atol, max_it, interval, periodic, drift);
   TLS_CHECK_LAUNCH();
   int64_t nb;
-  BlockSet bs = make_blocks(a, &nb);
+  int maxdim;
+  BlockSet bs = make_blocks(a, &nb, &maxdim);
   const int gb = grid_of(nb, kUpdThreads, kMaxUpdBlocks);
-  pcg_precondition_kernel<TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->r, (TV*)a->z, (TV*)a->p,
-                                                         a->partials + kOpPartials);
-  TLS_CHECK_LAUNCH();
-  pcg_rz_finish_kernel<<<1, 32, 0, s>>>(st, a->partials + kOpPartials, gb);
-  TLS_CHECK_LAUNCH();
-  return TLS_OK;
+  return with_dim(maxdim, [&](auto dim) -> int {
+    constexpr int D = decltype(dim)::value;
+    pcg_precondition_kernel<D, TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->r, (TV*)a->z, (TV*)a->p,
+                                                              scratch);
+    TLS_CHECK_LAUNCH();
+    pcg_rz_finish_kernel<<<1, 32, 0, s>>>(st, scratch, gb);
+    TLS_CHECK_LAUNCH();
+    return TLS_OK;
+  });
 }
 
 __global__ void set_block_counts_kernel(PcgState* st, int op_blocks, int upd_blocks) {
@@ -457,51 +490,43 @@ __global__ void set_block_counts_kernel(PcgState* st, int op_blocks, int upd_blo
 
 // Number of dot partials the operator's final kernel writes (one per block).
 static int operator_blocks(const tls_pcg_args* a) {
-  if (a->op_kind == 0) {
-    int blocks = 0;
-    for (int i = 0; i < a->normal->nvar_groups; ++i) {
-      const int64_t threads = (int64_t)a->normal->seg[i].count * a->normal->seg[i].lanes;
-      blocks += (int)((threads + 255) / 256);
-    }
-    return blocks;
-  }
-  return (a->schur->nretained * 32 + 255) / 256;
+  if (a->op_kind == 0) return tls_normal_gather_blocks(a->normal);
+  return a->schur->nretained;  // one gather block per retained variable
 }
 
 template <typename TV>
 static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
   PcgState* st = reinterpret_cast<PcgState*>(a->control);
   int64_t nb;
-  BlockSet bs = make_blocks(a, &nb);
+  int maxdim;
+  BlockSet bs = make_blocks(a, &nb, &maxdim);
   const int gb = grid_of(nb, kUpdThreads, kMaxUpdBlocks);
   const int gd = grid_of(a->n, 256, 148 * 8);
   const int op_blocks = operator_blocks(a);
   if (op_blocks > kOpPartials) return tls_set_error(TLS_ERR_UNSUPPORTED, "operator uses too many blocks");
-  for (int k = 0; k < steps; ++k) {
-    int launched = 0;
-    int rc;
-    if (a->op_kind == 0)
-      rc = tls_normal_apply(a->normal, a->p, a->ap, a->partials, &launched, s);
-    else
-      rc = tls_schur_apply(a->schur, a->p, a->ap, a->partials, &launched, s);
-    if (rc) return rc;
-    if (launched != op_blocks) return tls_set_error(TLS_ERR_INVALID, "operator block count changed");
-    if (k == 0) {
-      set_block_counts_kernel<<<1, 1, 0, s>>>(st, op_blocks, gb);
+  set_block_counts_kernel<<<1, 1, 0, s>>>(st, op_blocks, gb);
+  TLS_CHECK_LAUNCH();
+  return with_dim(maxdim, [&](auto dim) -> int {
+    constexpr int D = decltype(dim)::value;
+    for (int k = 0; k < steps; ++k) {
+      int launched = 0;
+      int rc;
+      if (a->op_kind == 0)
+        rc = tls_normal_apply(a->normal, a->p, a->ap, a->partials, &launched, st, s);
+      else
+        rc = tls_schur_apply(a->schur, a->p, a->ap, a->partials, &launched, st, s);
+      if (rc) return rc;
+      if (launched != op_blocks) return tls_set_error(TLS_ERR_INVALID, "operator block count changed");
+      pcg_update_kernel<D, TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r,
+                                                          (TV*)a->z, (const TV*)a->p, (TV*)a->ap, (TV*)a->ztrue,
+                                                          a->partials);
+      TLS_CHECK_LAUNCH();
+      pcg_direction_kernel<TV><<<gd, 256, 0, s>>>(a->n, st, (const TV*)a->x, (TV*)a->r, (const TV*)a->z, (TV*)a->p,
+                                                  (TV*)a->psave, (const TV*)a->ap, (const TV*)a->ztrue);
       TLS_CHECK_LAUNCH();
     }
-    pcg_alpha_kernel<<<1, 256, 0, s>>>(st, a->partials);
-    TLS_CHECK_LAUNCH();
-    pcg_update_kernel<TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r, (TV*)a->z,
-                                                     (const TV*)a->p, (TV*)a->ap, (TV*)a->ztrue, a->partials);
-    TLS_CHECK_LAUNCH();
-    pcg_decide_kernel<<<1, 256, 0, s>>>(st, a->partials);
-    TLS_CHECK_LAUNCH();
-    pcg_direction_kernel<TV><<<gd, 256, 0, s>>>(a->n, st, (const TV*)a->x, (TV*)a->r, (const TV*)a->z, (TV*)a->p,
-                                                (TV*)a->psave, (const TV*)a->ap, (const TV*)a->ztrue);
-    TLS_CHECK_LAUNCH();
-  }
-  return TLS_OK;
+    return TLS_OK;
+  });
 }
 
 // ---------------------------------------------------------------- block Jacobi
@@ -518,14 +543,26 @@ __global__ void block_cholesky_kernel(tls_block_group g, double damping, int32_t
   if (!ok) atomicAdd(bad, 1);
 }
 
-template <typename TV>
+template <int D, typename TV>
 __global__ void block_solve_kernel(BlockSet bs, int64_t nblocks, const TV* r, TV* z) {
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (int64_t)gridDim.x * blockDim.x) {
     const int gi = find_group(bs, b);
-    double rb[kMaxBlock], zb[kMaxBlock];
-    int64_t cols[kMaxBlock];
-    int dim;
-    apply_block(bs, gi, b - bs.block_begin[gi], r, z, rb, zb, dim, cols);
+    const int64_t i = b - bs.block_begin[gi];
+    const tls_block_group& g = bs.g[gi];
+    int64_t cols[D];
+    block_cols<D>(g, i, cols);
+    double rb[D], zb[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) rb[k] = (k < g.dim) ? to_d(r[cols[k]]) : 0.0;
+    if (bs.identity || g.factor == nullptr) {
+#pragma unroll
+      for (int k = 0; k < D; ++k) zb[k] = rb[k];
+    } else {
+      solve_block<D>(g.factor + i * g.dim * g.dim, g.dim, rb, zb);
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (k < g.dim) z[cols[k]] = static_cast<TV>(zb[k]);
   }
 }
 
@@ -553,15 +590,19 @@ extern "C" int tls_block_solve(const tls_block_group* groups, int32_t ngroups, c
   a.pre = groups;
   a.npre = ngroups;
   int64_t nb;
-  BlockSet bs = make_blocks(&a, &nb);
+  int maxdim;
+  BlockSet bs = make_blocks(&a, &nb, &maxdim);
   if (nb == 0) return TLS_OK;
   const int g = grid_of(nb, 128, 148 * 16);
-  if (vec_dtype == TLS_F64)
-    block_solve_kernel<double><<<g, 128, 0, s>>>(bs, nb, (const double*)r, (double*)z);
-  else
-    block_solve_kernel<float><<<g, 128, 0, s>>>(bs, nb, (const float*)r, (float*)z);
-  TLS_CHECK_LAUNCH();
-  return TLS_OK;
+  return with_dim(maxdim, [&](auto dim) -> int {
+    constexpr int D = decltype(dim)::value;
+    if (vec_dtype == TLS_F64)
+      block_solve_kernel<D, double><<<g, 128, 0, s>>>(bs, nb, (const double*)r, (double*)z);
+    else
+      block_solve_kernel<D, float><<<g, 128, 0, s>>>(bs, nb, (const float*)r, (float*)z);
+    TLS_CHECK_LAUNCH();
+    return TLS_OK;
+  });
 }
 
 extern "C" int tls_pcg_start(const tls_pcg_args* a, double rtol, double atol, int32_t max_iterations,

@@ -1,0 +1,65 @@
+// Device-side PCG state shared by the PCG driver and the operators' final
+// kernels (which finalise the curvature p.Ap in their last block).
+#pragma once
+#include "common.cuh"
+
+namespace tls {
+
+enum { M_ITER = 0, M_CHECK = 1, M_FINAL = 2, M_DONE = 3 };
+enum { A_NONE = 0, A_DIR = 1, A_RESTART = 2, A_RESTORE_DIR = 3, A_SWAP_TO_X = 4 };
+
+// tls_pcg_control first (read by the host), then private fields.
+struct PcgState {
+  tls_pcg_control pub;
+  int32_t action;        // direction-kernel action decided by the update kernel
+  int32_t pending;       // reason when the loop broke early
+  int32_t op_blocks;     // number of operator dot partials
+  int32_t upd_blocks;    // number of update partial blocks
+  double rec;            // recurrence norm of the last iteration
+  int32_t rec_hit;       // rec <= threshold at the last iteration
+  int32_t periodic_hit;  // periodic check due at the last iteration
+  int32_t alpha_ok;      // curvature and r.z finite and positive this step
+  uint32_t ticket_op;    // last-block-done counters (reset by the last block)
+  uint32_t ticket_upd;
+  int32_t pad_;
+};
+
+// Deterministic sum of p[0..n) by one block (fixed strided order, fixed tree).
+// Loads bypass L1: the values were written by other blocks of this kernel.
+template <int BLOCK>
+__device__ __forceinline__ double block_sum_cg(const double* p, int n, double* sm) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += BLOCK) acc += __ldcg(p + i);
+  return block_sum<BLOCK>(acc, sm);
+}
+
+// Called by every block of an operator's final kernel after thread 0 stored
+// the block's dot partial. The last block to finish computes the curvature
+// p.Ap and alpha = r.z / p.Ap for the PCG update (threadfence reduction).
+template <int BLOCK>
+__device__ __forceinline__ void pcg_operator_epilogue(PcgState* st, const double* partials, int nblocks,
+                                                      double* sm) {
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->ticket_op, 1u) == (unsigned)(nblocks - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double curv = block_sum_cg<BLOCK>(partials, nblocks, sm);
+  if (threadIdx.x == 0) {
+    st->ticket_op = 0;
+    tls_pcg_control& c = st->pub;
+    if (c.status == TLS_PCG_ACTIVE && c.mode == M_ITER) {
+      const double rz = c.rz;
+      c.curvature = curv;
+      const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
+      st->alpha_ok = ok;
+      c.alpha = ok ? rz / curv : 0.0;
+    } else {
+      st->alpha_ok = 0;
+    }
+  }
+}
+
+}  // namespace tls

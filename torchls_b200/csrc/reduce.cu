@@ -10,10 +10,19 @@ namespace tls {
 template <int WM, typename TC, typename TO>
 __global__ void __launch_bounds__(256) segment_reduce_kernel(tls_segments seg, const TC* __restrict__ contrib,
                                                              int mode, int dim, TO* __restrict__ out) {
-  const int L = seg.lanes;
-  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t t = gt / L;
-  const int lane = (int)(gt % L);
+  __shared__ double red[8][WM];
+  const bool block_mode = seg.lanes > 32;
+  const int L = block_mode ? 256 : seg.lanes;
+  int64_t t;
+  int lane;
+  if (block_mode) {
+    t = blockIdx.x;
+    lane = threadIdx.x;
+  } else {
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    t = gt / L;
+    lane = (int)(gt % L);
+  }
   const int W = seg.width;
   double acc[WM];
 #pragma unroll
@@ -27,9 +36,31 @@ __global__ void __launch_bounds__(256) segment_reduce_kernel(tls_segments seg, c
         if (k < W) acc[k] += to_d(src[k]);
     }
   }
+  bool writer;
+  if (block_mode) {
+    const int w = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < WM; ++k) acc[k] = group_sum(acc[k], L);
-  if (t >= seg.count || lane != 0) return;
+    for (int k = 0; k < WM; ++k) {
+      const double v = warp_sum(acc[k]);
+      if ((threadIdx.x & 31) == 0) red[w][k] = v;
+    }
+    __syncthreads();
+    writer = threadIdx.x == 0;
+    if (writer) {
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v += red[q][k];
+        acc[k] = v;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < WM; ++k) acc[k] = group_sum(acc[k], L);
+    writer = lane == 0;
+  }
+  if (t >= seg.count || !writer) return;
   if (mode == 0) {
 #pragma unroll
     for (int k = 0; k < WM; ++k)
@@ -55,10 +86,10 @@ template <typename TC, typename TO>
 static int launch_segments(const tls_segments* seg, const TC* c, int mode, int dim, TO* out, cudaStream_t st) {
   if (seg->count == 0) return TLS_OK;
   const int L = seg->lanes;
-  if (L < 1 || L > 32 || (L & (L - 1))) return tls_set_error(TLS_ERR_INVALID, "lanes must be a power of two <= 32");
-  const int64_t threads = (int64_t)seg->count * L;
+  if (L < 1 || (L <= 32 && (L & (L - 1))) || (L > 32 && L != 256))
+    return tls_set_error(TLS_ERR_INVALID, "lanes must be a power of two <= 32, or 256 (block per target)");
   const int block = 256;
-  const int64_t grid = (threads + block - 1) / block;
+  const int64_t grid = L > 32 ? seg->count : ((int64_t)seg->count * L + block - 1) / block;
   const int W = seg->width;
   if (W <= 4)
     segment_reduce_kernel<4, TC, TO><<<grid, block, 0, st>>>(*seg, c, mode, dim, out);

@@ -5,15 +5,16 @@
 // retained variable, so equal-retained edges form contiguous runs.
 //
 // Reduced matvec S x = (s U s + lambda I) x - W (W^T x), without forming S:
-//   chunk kernel   t_e = W_e^T x_i          (edge-local, into shared memory)
+//   chunk kernel   t_e = W_e^T x_i          (W_e loaded once, kept in registers)
 //                  y_p = sum_{e in p} t_e   (fixed order, shared memory)
-//                  u_e = W_e y_p            (edge-local)
-//                  partial[run] = sum_{e in run} u_e
+//                  u_e = W_e y_p
+//                  partial[run] = warp-segmented sum of u_e over the run
 //   gather kernel  out_i = base_i - sum_{runs of i} partial[run]
-// W is read once from HBM per matvec (the second, phase-2 read of a chunk's
-// W hits L1/L2). Every sum follows a fixed order: deterministic.
+// W is read from HBM exactly once per matvec; 8 bytes of edge metadata ride
+// along. Every sum follows a fixed order: deterministic.
 #include "blocks.cuh"
 #include "common.cuh"
+#include "pcg_state.cuh"
 
 namespace tls {
 
@@ -22,131 +23,177 @@ __device__ __forceinline__ TW ldw(const void* w, int64_t idx) {
   return __ldg(reinterpret_cast<const TW*>(w) + idx);
 }
 
-// MODE 0: matvec phase 1 from x; MODE 1: y_p taken from a->ybuf (reduced rhs)
-template <int DR, int DE, int MODE, typename TW, typename TV, typename TA>
-__global__ void __launch_bounds__(256) schur_chunk_kernel(tls_schur_args a, const TV* __restrict__ x) {
+constexpr int kChunkThreads = 256;
+
+// One thread block per chunk. MODE 0: S x (y_p = sum_{e in p} W_e^T x_i);
+// MODE 1: reduced rhs (y_p = L_p^-1 b_p taken from a.ybuf).
+//   phase 1   (MODE 0) t_e = W_e^T x_i for each edge; W_e stays in registers
+//   phase 1.5 y_p = sum of the t_e of p's edges, once per eliminated variable
+//   phase 2   u_e = W_e y_p; warp-segmented inclusive scan over runs (a run
+//             never crosses a 32-edge window); the run's last lane stores it.
+template <int DR, int DE, int EPT, int MODE, typename TW>
+__global__ void __launch_bounds__(kChunkThreads, 2)
+schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
+  constexpr int CAP = kChunkThreads * EPT;
   extern __shared__ double smem[];
+  double* t_s = smem;             // [CAP][DE] per-edge W^T x
+  double* y_s = smem + CAP * DE;  // [CAP][DE] per-variable sums
   const int c = blockIdx.x;
-  const int e0 = a.chunk_ptr[c], e1 = a.chunk_ptr[c + 1];
-  const int ne = e1 - e0;
-  double* t_s = smem;                          // [ne][DE]
-  double* u_s = smem + (size_t)a.max_chunk_edges * DE;  // [ne][DR]
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int e0 = __ldg(a.chunk_ptr + c), ne = __ldg(a.chunk_ptr + c + 1) - e0;
+  const int p0 = __ldg(a.cpt_ptr + c), np = __ldg(a.cpt_ptr + c + 1) - p0;
   const int64_t E = a.nedges;
+  const TW* __restrict__ W = reinterpret_cast<const TW*>(a.w);
+  TW w[EPT][DR * DE];
+  uint32_t meta[EPT];
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    const int le = j * kChunkThreads + tid;
+    meta[j] = 0;
+    if (le < ne) {
+      const int64_t e = e0 + le;
+#pragma unroll
+      for (int k = 0; k < DR * DE; ++k) w[j][k] = __ldg(W + k * E + e);
+      meta[j] = __ldg(a.edge_meta + e);
+    } else {
+#pragma unroll
+      for (int k = 0; k < DR * DE; ++k) w[j][k] = TW(0);
+    }
+  }
   if constexpr (MODE == 0) {
-    for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-      const int e = e0 + le;
-      const int i = __ldg(a.edge_r + e);
-      TA xr[DR];
 #pragma unroll
-      for (int k = 0; k < DR; ++k) xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
+    for (int j = 0; j < EPT; ++j) {
+      const int le = j * kChunkThreads + tid;
+      if (le < ne) {
+        const int64_t i = __ldg(a.edge_r + e0 + le);
+        double xr[DR];
 #pragma unroll
-      for (int b = 0; b < DE; ++b) {
-        TA acc = TA(0);
+        for (int k = 0; k < DR; ++k) xr[k] = __ldg(x + i * DR + k);
 #pragma unroll
-        for (int k = 0; k < DR; ++k) acc += static_cast<TA>(ldw<TW>(a.w, (int64_t)(k * DE + b) * E + e)) * xr[k];
-        t_s[le * DE + b] = static_cast<double>(acc);
+        for (int b = 0; b < DE; ++b) {
+          double acc = 0.0;
+#pragma unroll
+          for (int k = 0; k < DR; ++k) acc += static_cast<double>(w[j][k * DE + b]) * xr[k];
+          t_s[le * DE + b] = acc;
+        }
       }
     }
     __syncthreads();
-  }
-  for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-    const int e = e0 + le;
-    const int p = __ldg(a.edge_e + e);
-    double y[DE];
-    if constexpr (MODE == 0) {
+    for (int pl = tid; pl < np; pl += kChunkThreads) {
+      const int p = __ldg(a.chunk_points + p0 + pl);
+      const int jb = __ldg(a.elim_ptr + p), je = __ldg(a.elim_ptr + p + 1);
+      double y[DE];
 #pragma unroll
       for (int b = 0; b < DE; ++b) y[b] = 0.0;
-      const int pb = __ldg(a.elim_ptr + p), pe = __ldg(a.elim_ptr + p + 1);
-      for (int j = pb; j < pe; ++j) {
-        const int lj = __ldg(a.elim_edges + j) - e0;
+      for (int jj = jb; jj < je; ++jj) {
+        const int lj = __ldg(a.elim_edges + jj) - e0;
 #pragma unroll
         for (int b = 0; b < DE; ++b) y[b] += t_s[lj * DE + b];
       }
-    } else {
 #pragma unroll
-      for (int b = 0; b < DE; ++b) y[b] = a.ybuf[(int64_t)p * DE + b];
+      for (int b = 0; b < DE; ++b) y_s[pl * DE + b] = y[b];
     }
-    TA yv[DE];
+  } else {
+    for (int pl = tid; pl < np; pl += kChunkThreads) {
+      const int64_t p = __ldg(a.chunk_points + p0 + pl);
 #pragma unroll
-    for (int b = 0; b < DE; ++b) yv[b] = static_cast<TA>(y[b]);
-#pragma unroll
-    for (int k = 0; k < DR; ++k) {
-      TA acc = TA(0);
-#pragma unroll
-      for (int b = 0; b < DE; ++b) acc += static_cast<TA>(ldw<TW>(a.w, (int64_t)(k * DE + b) * E + e)) * yv[b];
-      u_s[le * DR + k] = static_cast<double>(acc);
+      for (int b = 0; b < DE; ++b) y_s[pl * DE + b] = a.ybuf[p * DE + b];
     }
   }
   __syncthreads();
-  const int r0 = a.chunk_run_ptr[c], r1 = a.chunk_run_ptr[c + 1];
-  for (int run = r0 + threadIdx.x; run < r1; run += blockDim.x) {
-    const int b = a.run_ptr[run] - e0, e = a.run_ptr[run + 1] - e0;
-    double acc[DR];
+  const int wbase = __ldg(a.cw_ptr + c);
 #pragma unroll
-    for (int k = 0; k < DR; ++k) acc[k] = 0.0;
-    for (int le = b; le < e; ++le)
+  for (int j = 0; j < EPT; ++j) {
+    const int le = j * kChunkThreads + tid;
+    if (j * kChunkThreads >= ne) break;  // uniform across the block
+    const bool valid = le < ne;
+    const uint32_t m = valid ? meta[j] : 0u;
+    const int pl = m & 0xFFFFu;
+    const int head = (m >> 16) & 31;
+    const bool tail = valid && ((m >> 21) & 1u);
+    double y[DE];
 #pragma unroll
-      for (int k = 0; k < DR; ++k) acc[k] += u_s[le * DR + k];
+    for (int b = 0; b < DE; ++b) y[b] = valid ? y_s[pl * DE + b] : 0.0;
+    const unsigned tails = __ballot_sync(0xffffffffu, tail);
+    const int run = tail ? __ldg(a.win_run + wbase + (le >> 5)) + __popc(tails & ((1u << lane) - 1u)) : 0;
+    // one output component at a time keeps few doubles live
 #pragma unroll
-    for (int k = 0; k < DR; ++k) a.run_partial[(int64_t)run * DR + k] = acc[k];
+    for (int k = 0; k < DR; ++k) {
+      double u = 0.0;
+#pragma unroll
+      for (int b = 0; b < DE; ++b) u += static_cast<double>(w[j][k * DE + b]) * y[b];
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, u, off);
+        if (lane - off >= head) u += v;
+      }
+      if (tail) a.run_partial[(int64_t)run * DR + k] = u;
+    }
   }
 }
 
-// MODE 0: out = s U s x + lambda x - sum   (matvec, optional dot partials)
-// MODE 1: out = b_retained - sum            (reduced rhs, b float64 full vector)
+// One block per retained variable: sum its runs in a fixed order, then
+// MODE 0: out = s U s x + lambda x - sum  (matvec, optional dot partial per block)
+// MODE 1: out = b_retained - sum          (reduced rhs, b float64 full vector)
 template <int DR, int MODE, typename TV>
 __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, const TV* __restrict__ x,
                                                            const double* __restrict__ b, TV* __restrict__ out,
-                                                           double* __restrict__ dot_partials) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+                                                           double* __restrict__ dot_partials, PcgState* pst) {
+  __shared__ double sm[8][DR];
+  __shared__ double smd[8];
+  const int64_t i = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double acc[DR];
 #pragma unroll
   for (int k = 0; k < DR; ++k) acc[k] = 0.0;
-  const bool live = warp < a.nretained;
-  if (live) {
-    const int rb = a.rrun_ptr[warp], re = a.rrun_ptr[warp + 1];
-    for (int j = rb + lane; j < re; j += 32) {
-      const int run = a.rrun_list[j];
+  const int rb = __ldg(a.rrun_ptr + i), re = __ldg(a.rrun_ptr + i + 1);
+  for (int j = rb + tid; j < re; j += 256) {
+    const int64_t run = __ldg(a.rrun_list + j);
 #pragma unroll
-      for (int k = 0; k < DR; ++k) acc[k] += a.run_partial[(int64_t)run * DR + k];
-    }
+    for (int k = 0; k < DR; ++k) acc[k] += a.run_partial[run * DR + k];
   }
 #pragma unroll
-  for (int k = 0; k < DR; ++k) acc[k] = warp_sum(acc[k]);
-  double dot = 0.0;
-  if (live && lane == 0) {
-    const int64_t i = warp;
+  for (int k = 0; k < DR; ++k) {
+    const double v = warp_sum(acc[k]);
+    if (lane == 0) sm[warp][k] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double tot[DR];
+#pragma unroll
+    for (int k = 0; k < DR; ++k) {
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v += sm[q][k];
+      tot[k] = v;
+    }
     if constexpr (MODE == 0) {
-      double xs[DR], xv[DR];
+      double xs[DR], xv[DR], s[DR];
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
         xv[k] = to_d(x[i * DR + k]);
-        const double s = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
-        xs[k] = s * xv[k];
+        s[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+        xs[k] = s[k] * xv[k];
       }
       const double* U = a.ret_diag + i * DR * DR;
+      double dot = 0.0;
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
         double v = 0.0;
 #pragma unroll
         for (int l = 0; l < DR; ++l) v += U[k * DR + l] * xs[l];
-        const double s = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
-        v = s * v + a.damping * xv[k] - acc[k];
+        v = s[k] * v + a.damping * xv[k] - tot[k];
         const TV o = static_cast<TV>(v);
         out[i * DR + k] = o;
         dot += xv[k] * to_d(o);
       }
+      if (dot_partials) dot_partials[i] = dot;
     } else {
 #pragma unroll
-      for (int k = 0; k < DR; ++k) out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - acc[k]);
+      for (int k = 0; k < DR; ++k) out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - tot[k]);
     }
   }
-  if (dot_partials) {
-    __shared__ double sm[8];
-    const double s = block_sum<256>(dot, sm);
-    if (threadIdx.x == 0) dot_partials[blockIdx.x] = s;
-  }
+  if (MODE == 0 && pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
 }
 
 // Per eliminated variable: L = chol(s C s + lambda I), store L^-1; y = L^-1 b_e optional.
@@ -308,16 +355,35 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
 
 template <int DR, int DE>
 struct SchurOps {
-  template <typename TW, typename TV, typename TA>
-  static int matvec(const tls_schur_args& a, const TV* x, TV* out, double* dots, int* gblocks, cudaStream_t s) {
-    const size_t smem = (size_t)a.max_chunk_edges * (DE + DR) * sizeof(double);
-    auto k = schur_chunk_kernel<DR, DE, 0, TW, TV, TA>;
+  template <int MODE, typename TW, int EPT>
+  static int chunks_ept(const tls_schur_args& a, const double* x, cudaStream_t s) {
+    constexpr size_t smem = 2 * sizeof(double) * kChunkThreads * EPT * DE;
+    auto k = schur_chunk_kernel<DR, DE, EPT, MODE, TW>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (a.nchunks > 0) k<<<a.nchunks, 256, smem, s>>>(a, x);
+    k<<<a.nchunks, kChunkThreads, smem, s>>>(a, x);
     TLS_CHECK_LAUNCH();
-    const int blocks = (a.nretained * 32 + 255) / 256;
-    if (gblocks) *gblocks = blocks;
-    if (blocks > 0) schur_gather_kernel<DR, 0, TV><<<blocks, 256, 0, s>>>(a, x, nullptr, out, dots);
+    return TLS_OK;
+  }
+  template <int MODE, typename TW>
+  static int chunks(const tls_schur_args& a, const double* x, cudaStream_t s) {
+    if (a.nchunks == 0) return TLS_OK;
+    // 2 edges per thread: W stays in registers between the phases
+    if constexpr (sizeof(TW) == 4) {
+      if (a.ept != 2) return tls_set_error(TLS_ERR_INVALID, "Schur layouts use 2 edges per thread");
+      return chunks_ept<MODE, TW, 2>(a, x, s);
+    } else {
+      if (a.ept != 2) return tls_set_error(TLS_ERR_INVALID, "float64 W needs a 2-edge-per-thread layout");
+      return chunks_ept<MODE, TW, 2>(a, x, s);
+    }
+  }
+  template <typename TW, typename TV, typename TA>
+  static int matvec(const tls_schur_args& a, const TV* x, TV* out, double* dots, int* gblocks, PcgState* pst,
+                    cudaStream_t s) {
+    static_assert(sizeof(TV) == 8, "reduced vectors are float64");
+    int rc = chunks<0, TW>(a, reinterpret_cast<const double*>(x), s);
+    if (rc) return rc;
+    if (gblocks) *gblocks = a.nretained;
+    if (a.nretained > 0) schur_gather_kernel<DR, 0, TV><<<a.nretained, 256, 0, s>>>(a, x, nullptr, out, dots, pst);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
@@ -325,13 +391,10 @@ struct SchurOps {
   static int rhs(const tls_schur_args& a, const double* b, TV* out, cudaStream_t s) {
     if (a.nelim > 0) schur_elim_rhs_kernel<DE><<<(a.nelim + 127) / 128, 128, 0, s>>>(a, b);
     TLS_CHECK_LAUNCH();
-    const size_t smem = (size_t)a.max_chunk_edges * (DE + DR) * sizeof(double);
-    auto k = schur_chunk_kernel<DR, DE, 1, TW, TV, TA>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (a.nchunks > 0) k<<<a.nchunks, 256, smem, s>>>(a, nullptr);
-    TLS_CHECK_LAUNCH();
-    const int blocks = (a.nretained * 32 + 255) / 256;
-    if (blocks > 0) schur_gather_kernel<DR, 1, TV><<<blocks, 256, 0, s>>>(a, nullptr, b, out, nullptr);
+    int rc = chunks<1, TW>(a, nullptr, s);
+    if (rc) return rc;
+    if (a.nretained > 0)
+      schur_gather_kernel<DR, 1, TV><<<a.nretained, 256, 0, s>>>(a, nullptr, b, out, nullptr, nullptr);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
@@ -386,16 +449,15 @@ static int dispatch_dims(int dr, int de, F&& f) {
 
 using namespace tls;
 
-int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* dots, int* gblocks, cudaStream_t s) {
+int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* dots, int* gblocks, void* pcg_state,
+                    cudaStream_t s) {
+  if (a->vec_dtype != TLS_F64) return tls_set_error(TLS_ERR_UNSUPPORTED, "reduced Schur vectors are float64");
+  PcgState* pst = reinterpret_cast<PcgState*>(pcg_state);
   return dispatch_dims(a->dr, a->de, [&](auto ops) -> int {
     using O = decltype(ops);
-    if (a->vec_dtype == TLS_F64) {
-      if (a->wdtype == TLS_F64)
-        return O::template matvec<double, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, s);
-      return O::template matvec<float, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, s);
-    }
-    if (a->wdtype != TLS_F32) return tls_set_error(TLS_ERR_UNSUPPORTED, "float64 W with float32 vectors");
-    return O::template matvec<float, float, float>(*a, (const float*)x, (float*)out, dots, gblocks, s);
+    if (a->wdtype == TLS_F64)
+      return O::template matvec<double, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, pst, s);
+    return O::template matvec<float, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, pst, s);
   });
 }
 
@@ -408,29 +470,27 @@ extern "C" int tls_schur_damp(const tls_schur_args* a, tls_stream_t stream) {
 }
 
 extern "C" int tls_schur_matvec(const tls_schur_args* a, const void* x, void* out, tls_stream_t stream) {
-  return tls_schur_apply(a, x, out, nullptr, nullptr, reinterpret_cast<cudaStream_t>(stream));
+  return tls_schur_apply(a, x, out, nullptr, nullptr, nullptr, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int tls_schur_reduced_rhs(const tls_schur_args* a, const double* b, void* rhs_c, tls_stream_t stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (a->vec_dtype != TLS_F64) return tls_set_error(TLS_ERR_UNSUPPORTED, "reduced Schur vectors are float64");
   return dispatch_dims(a->dr, a->de, [&](auto ops) -> int {
     using O = decltype(ops);
-    if (a->vec_dtype == TLS_F64)
-      return a->wdtype == TLS_F64 ? O::template rhs<double, double, double>(*a, b, (double*)rhs_c, s)
-                                  : O::template rhs<float, double, double>(*a, b, (double*)rhs_c, s);
-    return O::template rhs<float, float, float>(*a, b, (float*)rhs_c, s);
+    return a->wdtype == TLS_F64 ? O::template rhs<double, double, double>(*a, b, (double*)rhs_c, s)
+                                : O::template rhs<float, double, double>(*a, b, (double*)rhs_c, s);
   });
 }
 
 extern "C" int tls_schur_backsubstitute(const tls_schur_args* a, const void* x_c, double* delta_full,
                                         tls_stream_t stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (a->vec_dtype != TLS_F64) return tls_set_error(TLS_ERR_UNSUPPORTED, "reduced Schur vectors are float64");
   return dispatch_dims(a->dr, a->de, [&](auto ops) -> int {
     using O = decltype(ops);
-    if (a->vec_dtype == TLS_F64)
-      return a->wdtype == TLS_F64 ? O::template backsub<double, double>(*a, (const double*)x_c, delta_full, s)
-                                  : O::template backsub<float, double>(*a, (const double*)x_c, delta_full, s);
-    return O::template backsub<float, float>(*a, (const float*)x_c, delta_full, s);
+    return a->wdtype == TLS_F64 ? O::template backsub<double, double>(*a, (const double*)x_c, delta_full, s)
+                                : O::template backsub<float, double>(*a, (const double*)x_c, delta_full, s);
   });
 }
 

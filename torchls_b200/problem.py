@@ -37,6 +37,10 @@ def _is_ref(arg) -> bool:
 
 
 def _lanes(degree_mean: float) -> int:
+    """Lanes per reduction target: a power of two <= 32 for cold variables, a
+    whole 256-thread block per target for hot ones (mean degree > 64)."""
+    if degree_mean > 64:
+        return 256
     lanes = 1
     while lanes < degree_mean and lanes < 32:
         lanes *= 2

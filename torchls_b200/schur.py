@@ -24,11 +24,9 @@ import torch
 from . import _lib as L
 from .kernels import segment_reduce
 
-SMEM_BYTES = 200 * 1024
-
 
 class SchurPlan:
-    def __init__(self, problem, eliminate, device, *, preconditioner_groups=(), chunk_edges: int = 2048):
+    def __init__(self, problem, eliminate, device, *, preconditioner_groups=()):
         layout = problem.layout
         matches = [i for i, e in enumerate(layout) if e.key == eliminate]
         if len(matches) != 1:
@@ -82,65 +80,16 @@ class SchurPlan:
         ri, ei = uniq // E_count, uniq % E_count
         self.nedges = len(uniq)
         self.edges = ((torch.from_numpy(ri).to(device), torch.from_numpy(ei).to(device)),)
-        # ---- chunked order
-        deg = np.bincount(ei, minlength=E_count)
-        max_deg = int(deg.max()) if len(deg) else 0
-        cap = SMEM_BYTES // ((dr + de) * 8)
-        if max_deg > cap:
-            raise ValueError(f"an eliminated variable has {max_deg} retained neighbours; the CUDA Schur path "
-                             f"supports at most {cap}")
-        target = max(1, min(chunk_edges, cap - max_deg + 1))
-        start_e = np.cumsum(deg) - deg
-        chunk_of_e = start_e // target
-        order = np.lexsort((ei, ri, chunk_of_e[ei]))
-        pos_of_edge = np.empty(self.nedges, np.int64)
-        pos_of_edge[order] = np.arange(self.nedges)
-        self.order = order  # chunk position -> reference edge index
-        self.pos_of_edge = pos_of_edge
-        c_r, c_e, c_ch = ri[order], ei[order], chunk_of_e[ei[order]]
-        newchunk = np.ones(self.nedges, bool)
-        newchunk[1:] = c_ch[1:] != c_ch[:-1]
-        chunk_ptr = np.concatenate((np.flatnonzero(newchunk), [self.nedges])).astype(np.int32)
-        newrun = newchunk.copy()
-        newrun[1:] |= c_r[1:] != c_r[:-1]
-        run_starts = np.flatnonzero(newrun)
-        run_ptr = np.concatenate((run_starts, [self.nedges])).astype(np.int32)
-        run_chunk = np.cumsum(newchunk)[run_starts] - 1
-        nchunks = len(chunk_ptr) - 1
-        chunk_run_ptr = np.searchsorted(run_chunk, np.arange(nchunks + 1)).astype(np.int32)
-        run_r = c_r[run_starts]
-        rorder = np.argsort(run_r, kind="stable")
-        rrun_ptr = np.concatenate(([0], np.cumsum(np.bincount(run_r, minlength=self.r.count)))).astype(np.int32)
-        eorder = np.lexsort((np.arange(self.nedges), c_e))
-        elim_ptr = np.concatenate(([0], np.cumsum(np.bincount(c_e, minlength=E_count)))).astype(np.int32)
-        self.nchunks = nchunks
-        self.nruns = len(run_starts)
-        self.max_chunk_edges = int(np.diff(chunk_ptr).max()) if nchunks else 1
-        # ---- cross-contribution segments per edge (chunk order)
-        cursor, ids, offs = 0, [], []
-        for k, s, n in recs:
-            info = self.plan_info[k]
-            ids.append(pos_of_edge[inverse[cursor : cursor + n]])
-            offs.append(info["base"] + np.arange(n, dtype=np.int64) * info["width"] + info["slot_cross"][s])
-            cursor += n
-        ids = np.concatenate(ids) if ids else np.zeros(0, np.int64)
-        offs = np.concatenate(offs) if offs else np.zeros(0, np.int64)
-        o = np.argsort(ids, kind="stable")
-        if self.cross_size >= 2**31:
-            raise ValueError("Schur cross buffer exceeds the 32-bit offset range")
-        cptr = np.concatenate(([0], np.cumsum(np.bincount(ids, minlength=self.nedges)))).astype(np.int32)
-        t = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt)
-        self.dev = dict(
-            chunk_ptr=t(chunk_ptr), chunk_run_ptr=t(chunk_run_ptr), edge_r=t(c_r), edge_e=t(c_e),
-            elim_ptr=t(elim_ptr), elim_edges=t(eorder), run_ptr=t(run_ptr), rrun_ptr=t(rrun_ptr),
-            rrun_list=t(rorder), cross_ptr=t(cptr), cross_src=t(offs[o]),
-        )
-        self.cross_seg = L.Segments(self.nedges, dr * de, 1, 0, self.dev["cross_ptr"].data_ptr(),
-                                    self.dev["cross_src"].data_ptr())
+        self.E_count = E_count
+        self._ri, self._ei = ri, ei
+        self._records = recs
+        self._inverse = inverse
+        self.reduced_dim = self.dim
         # reduced-vector indices into the full tangent (schur.py:28-37)
         self.global_indices = torch.arange(self.r.offset, self.r.offset + self.r.size, device=device)
         self.layout = (self.r,)
         self.bad = torch.zeros(1, dtype=torch.int32, device=device)
+        self.chunks = ChunkLayout(self)
 
     # ---------------------------------------------------------------- linearization hooks
     def cross_buffer(self, device):
@@ -159,15 +108,115 @@ class SchurPlan:
         return info["base"]
 
 
+class ChunkLayout:
+    """Chunked edge order used by the kernels (one thread block per chunk).
+
+    Eliminated variables are ordered by their smallest retained neighbour, so
+    a chunk's edges touch few retained variables and runs are long. Chunks
+    hold whole eliminated variables and at most ``CHUNK_EDGES`` edges; inside
+    a chunk edges are sorted by retained variable and cut into runs that
+    never cross a 32-edge window.
+    """
+
+    THREADS, EPT = 256, 2
+    CHUNK_EDGES = THREADS * EPT
+
+    def __init__(self, plan: SchurPlan):
+        ri, ei, E, P = plan._ri, plan._ei, plan.nedges, plan.E_count
+        device = plan.device
+        deg = np.bincount(ei, minlength=P)
+        max_deg = int(deg.max()) if E else 0
+        cap = self.CHUNK_EDGES
+        if max_deg > cap:
+            raise ValueError(f"an eliminated variable has {max_deg} retained neighbours; the CUDA Schur path "
+                             f"supports at most {cap}")
+        first = np.full(P, np.iinfo(np.int64).max)
+        if E:
+            np.minimum.at(first, ei, ri)
+        point_order = np.lexsort((np.arange(P), first))
+        rank = np.empty(P, np.int64)
+        rank[point_order] = np.arange(P)
+        deg_o = deg[point_order]
+        start = np.cumsum(deg_o) - deg_o
+        chunk_of_rank = start // max(1, cap - max_deg + 1)
+        ch = chunk_of_rank[rank[ei]]
+        order = np.lexsort((ei, ri, ch))
+        # chunk ids renumbered densely in order of appearance
+        c_r, c_e, c_raw = ri[order], ei[order], ch[order]
+        newchunk = np.ones(E, bool)
+        newchunk[1:] = c_raw[1:] != c_raw[:-1]
+        cid = np.cumsum(newchunk) - 1
+        nchunks = int(cid[-1]) + 1 if E else 0
+        chunk_ptr = np.concatenate((np.flatnonzero(newchunk), [E])).astype(np.int64)
+        local = np.arange(E) - chunk_ptr[cid] if E else np.zeros(0, np.int64)
+        newrun = newchunk.copy()
+        newrun[1:] |= c_r[1:] != c_r[:-1]
+        newrun |= (local % 32) == 0
+        run_starts = np.flatnonzero(newrun)
+        nruns = len(run_starts)
+        run_id = np.cumsum(newrun) - 1
+        run_ptr = np.concatenate((run_starts, [E]))
+        head = local[run_starts][run_id] % 32 if E else np.zeros(0, np.int64)
+        tail = np.zeros(E, bool)
+        if E:
+            tail[run_ptr[1:] - 1] = True
+        # chunk points: distinct eliminated variables per chunk, ascending
+        ckey = cid * P + c_e
+        uniq_cp, cp_inv = np.unique(ckey, return_inverse=True)
+        cpt_chunk = uniq_cp // P
+        cpt_ptr = np.searchsorted(cpt_chunk, np.arange(nchunks + 1))
+        chunk_points = uniq_cp % P
+        pl = cp_inv - cpt_ptr[cid] if E else np.zeros(0, np.int64)
+        if E and pl.max() >= 1 << 16:
+            raise ValueError("too many eliminated variables in one chunk")
+        meta = (pl | (head << 16) | (tail.astype(np.int64) << 21)).astype(np.uint32)
+        # windows: first run id of each 32-edge window of each chunk
+        nwin = (np.diff(chunk_ptr) + 31) // 32
+        cw_ptr = np.concatenate(([0], np.cumsum(nwin)))
+        win_start_edge = (np.repeat(chunk_ptr[:-1], nwin)
+                          + 32 * (np.arange(int(cw_ptr[-1])) - np.repeat(cw_ptr[:-1], nwin)))
+        win_run = run_id[win_start_edge] if E else np.zeros(0, np.int64)
+        run_r = c_r[run_starts]
+        rorder = np.argsort(run_r, kind="stable")
+        rrun_ptr = np.concatenate(([0], np.cumsum(np.bincount(run_r, minlength=plan.r.count))))
+        eorder = np.lexsort((np.arange(E), c_e))
+        elim_ptr = np.concatenate(([0], np.cumsum(np.bincount(c_e, minlength=P))))
+        pos_of_edge = np.empty(E, np.int64)
+        pos_of_edge[order] = np.arange(E)
+        self.order, self.pos_of_edge = order, pos_of_edge
+        self.nchunks, self.nruns = nchunks, nruns
+        # cross-contribution segments per edge (chunk order)
+        cursor, ids, offs = 0, [], []
+        for k, s_, n in plan._records:
+            info = plan.plan_info[k]
+            ids.append(pos_of_edge[plan._inverse[cursor : cursor + n]])
+            offs.append(info["base"] + np.arange(n, dtype=np.int64) * info["width"] + info["slot_cross"][s_])
+            cursor += n
+        ids = np.concatenate(ids) if ids else np.zeros(0, np.int64)
+        offs = np.concatenate(offs) if offs else np.zeros(0, np.int64)
+        o = np.argsort(ids, kind="stable")
+        cptr = np.concatenate(([0], np.cumsum(np.bincount(ids, minlength=E))))
+        t = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt)
+        self.dev = dict(
+            chunk_ptr=t(chunk_ptr), cpt_ptr=t(cpt_ptr), chunk_points=t(chunk_points), cw_ptr=t(cw_ptr),
+            win_run=t(win_run), edge_r=t(c_r), edge_meta=t(meta.view(np.int32)), edge_e=t(c_e),
+            elim_ptr=t(elim_ptr), elim_edges=t(eorder), run_ptr=t(run_ptr), rrun_ptr=t(rrun_ptr),
+            rrun_list=t(rorder), cross_ptr=t(cptr), cross_src=t(offs[o]),
+        )
+        self.cross_seg = L.Segments(E, plan.dr * plan.de, 1, 0, self.dev["cross_ptr"].data_ptr(),
+                                    self.dev["cross_src"].data_ptr())
+
+
 class SchurLinearization:
     """Cross blocks E_e = J_r^T J_e per edge (schur.py:192-257), in chunk order, float64."""
 
     def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
         self.plan = plan
         dev = plan.device
+        self.layout = plan.chunks
         self.cross = torch.empty((plan.nedges, plan.dr, plan.de), dtype=torch.float64, device=dev)
         if plan.nedges:
-            segment_reduce(plan.cross_seg, lin.cross_contrib, self.cross)
+            segment_reduce(self.layout.cross_seg, lin.cross_contrib, self.cross)
         self.ret_diag = diagonal_raw[plan.retained[0]].contiguous()
         self.elim_diag = diagonal_raw[plan.eliminated].contiguous()
         self.scale = None if scale is None else scale.to(torch.float64).contiguous()
@@ -176,7 +225,7 @@ class SchurLinearization:
         n, E = plan.nedges, plan.nedges
         self.w = torch.empty((plan.dr * plan.de, max(E, 1)), dtype=wdtype, device=dev)
         self.inv_l = torch.empty((plan.e.count, plan.de, plan.de), dtype=torch.float64, device=dev)
-        self.run_partial = torch.empty((max(plan.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
+        self.run_partial = torch.empty((max(self.layout.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
         self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
 
     def damped(self, damping):
@@ -197,14 +246,15 @@ class DampedSchurSystem:
     def _args(self) -> L.SchurArgs:
         p, lin = self.plan, self.linear
         a = L.SchurArgs()
-        a.nedges, a.nchunks, a.dr, a.de = p.nedges, p.nchunks, p.dr, p.de
+        a.nedges, a.dr, a.de = p.nedges, p.dr, p.de
         a.nretained, a.nelim = p.r.count, p.e.count
         a.wdtype, a.vec_dtype = L.dtype_code(lin.wdtype), L.dtype_code(lin.vec_dtype)
-        a.max_chunk_edges, a.nruns = p.max_chunk_edges, p.nruns
+        lay = lin.layout
+        a.nchunks, a.ept, a.nruns = lay.nchunks, lay.EPT, lay.nruns
         a.retained_offset, a.elim_offset = p.r.offset, p.e.offset
-        d = p.dev
-        for name in ("chunk_ptr", "chunk_run_ptr", "edge_r", "edge_e", "elim_ptr", "elim_edges", "run_ptr",
-                     "rrun_ptr", "rrun_list"):
+        d = lay.dev
+        for name in ("chunk_ptr", "cpt_ptr", "chunk_points", "cw_ptr", "win_run", "edge_r", "edge_meta", "edge_e",
+                     "elim_ptr", "elim_edges", "run_ptr", "rrun_ptr", "rrun_list"):
             setattr(a, name, d[name].data_ptr())
         a.cross = lin.cross.data_ptr()
         a.elim_diag = lin.elim_diag.data_ptr()
@@ -279,8 +329,8 @@ class DampedSchurSystem:
         if E:
             # W rows (retained columns) x eliminated columns, sparse COO -> dense chunks
             w = self.linear.w[:, :E].to(torch.float64).view(p.dr, p.de, E)
-            er = p.dev["edge_r"].long()
-            ee = p.dev["edge_e"].long()
+            er = self.linear.layout.dev["edge_r"].long()
+            ee = self.linear.layout.dev["edge_e"].long()
             cols_all = ee[:, None] * p.de + torch.arange(p.de, device=p.device)[None, :]
             rows_all = er[:, None] * p.dr + torch.arange(p.dr, device=p.device)[None, :]
             step = max(1, (1 << 27) // max(n, 1))

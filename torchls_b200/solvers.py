@@ -5,10 +5,10 @@ Interface of torchls ``solvers.py``: ``ConjugateGradientConfig``,
 ``pcg``, ``block_jacobi`` and ``solve`` keep their fields, defaults, reason
 strings and validation (solvers.py:19-164). The backend is ``"cuda"``: every
 linear-algebra step runs in this package's kernels; there is no CPU path.
-``precision="mixed"`` stores Jacobians, Schur blocks and PCG vectors in
-float32 while gradients, costs, dot products, gain ratios and small-block
-factorizations stay float64; the outer LM iterations refine the float32
-inner solves.
+``precision="mixed"`` stores Jacobians and Schur W blocks in float32 (half
+the bytes of every matvec) while PCG vectors, gradients, costs, dot
+products, gain ratios and small-block factorizations stay float64; the outer
+LM iterations refine the float32-operator inner solves.
 """
 
 from __future__ import annotations
@@ -69,8 +69,8 @@ class ConjugateGradientConfig:
     # Operator applications between host status reads of the device PCG.
     graph_batch_iterations: int = 16
     cache_retained_matrix: bool = False
-    # "native": Jacobian and PCG vectors in the parameter dtype;
-    # "mixed": float32 Jacobian / Schur W / PCG vectors, float64 reductions.
+    # "native": Jacobian and Schur W stored in the parameter dtype;
+    # "mixed": float32 Jacobian / Schur W storage, float64 vectors and reductions.
     precision: str = "native"
 
     def __post_init__(self):
@@ -517,7 +517,10 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
     if device.type != "cuda":
         raise ValueError("the CUDA backend requires parameters on a CUDA device")
     mixed = cg.precision == "mixed" or vals.dtype == torch.float32
+    # Storage precision of J and Schur W; PCG vectors and every reduction stay
+    # float64 so the inner solve converges to the same tolerance either way.
     jdt = torch.float32 if mixed else torch.float64
+    vdt = torch.float64
     bplan = BoundsPlan(bounds, problem.layout, vals) if bounds is not None else None
     if bplan is not None and bplan.groups and trust_region is None:
         raise ValueError("Bounds require a trust-region LM solve")
@@ -529,13 +532,19 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
     damping = trust_region.lambda_initial if trust_region else 0.0
     rejection_factor = 2.0
     with _region("analyze_schur", profile):
-        schur_plan = SchurPlan(problem, eliminate, device, preconditioner_groups=cg.preconditioner_groups) \
-            if is_schur else None
+        schur_plan = None
+        if is_schur:
+            # symbolic Schur structure is cached on the analysed problem
+            cache = problem.__dict__.setdefault("_schur_plans", {})
+            key = (eliminate, device, tuple(cg.preconditioner_groups))
+            if key not in cache:
+                cache[key] = SchurPlan(problem, eliminate, device, preconditioner_groups=cg.preconditioner_groups)
+            schur_plan = cache[key]
     if linear_solver == "schur_dense" and schur_plan.dim > 8192:
         raise ValueError("Dense Schur is limited to 8192 retained dimensions; use schur_cg")
     summary.reduced_dim = schur_plan.dim if is_schur else None
     n = problem.tangent_dim
-    pcg_ws = DevicePCG(schur_plan.dim if is_schur else n, jdt, device)
+    pcg_ws = DevicePCG(schur_plan.dim if is_schur else n, vdt, device)
     column_scale = None
     layout = problem.layout
     with _region("linearize", profile):
@@ -583,7 +592,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             combined = solve_scale if mask is None else (mask if solve_scale is None else mask * solve_scale)
             linear_gradient = gradient if solve_scale is None else gradient * solve_scale
             scaled = lin.jacobian if combined is None else lin.jacobian.scale_columns(combined)
-            schur_lin = SchurLinearization(schur_plan, lin, raw_diag, combined, wdtype=jdt, vec_dtype=jdt,
+            schur_lin = SchurLinearization(schur_plan, lin, raw_diag, combined, wdtype=jdt, vec_dtype=vdt,
                                            dense=linear_solver == "schur_dense") if is_schur else None
             joint_specs = None
             if not is_schur and cg.preconditioner is not None:
@@ -632,8 +641,8 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                         scale_for_pre = None if cg.preconditioner_groups else combined
                         pre = BlockJacobiPreconditioner.from_blocks(joint_specs, damping, scale_for_pre, n)
                     with _region("linear_solve", profile):
-                        res = pcg_ws.run((-linear_gradient).to(jdt), cg,
-                                         normal_args=scaled.normal_args(jdt, damping), preconditioner=pre)
+                        res = pcg_ws.run((-linear_gradient).to(vdt), cg,
+                                         normal_args=scaled.normal_args(vdt, damping), preconditioner=pre)
                     summary.linear_iterations += res.iterations
                     summary.linear_iterations_history.append(res.iterations)
                     summary.linear_converged_history.append(res.converged)
