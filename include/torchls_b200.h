@@ -271,12 +271,13 @@ TLS_API int tls_pcg_state_bytes(void);
 /* ---------------------------------------------------------------- Schur complement
  * Replaces: schur.py:192-397 (SchurLinearization, DampedSchurSystem) for one
  * retained group of dimension dr <= 8 and an eliminated group of dimension
- * de <= 4. Edges (retained i, eliminated p) are stored in a chunked order:
- * each chunk (one thread block) holds whole eliminated variables, at most
- * 256 * ept edges; inside a chunk edges are sorted by retained variable and
- * cut into runs of equal retained variable that never cross a 32-edge
- * window, so a run is reduced by one warp. Every reduction follows a fixed
- * order (deterministic).
+ * de <= 4. Edges (retained i, eliminated p) are stored in chunks of whole
+ * eliminated variables; each chunk owns a fixed-size slab (W and int32
+ * metadata) that the matvec kernel streams into shared memory with 1-D bulk
+ * copies (TMA), double-buffered, in a persistent grid. Inside a chunk edges
+ * are sorted by retained variable and cut into runs that never cross a
+ * 32-edge window, so a run is reduced by one warp. Every reduction follows a
+ * fixed order (deterministic).
  */
 struct tls_schur_args {
   int32_t nedges;
@@ -285,34 +286,32 @@ struct tls_schur_args {
   int32_t nretained;            /* retained variables */
   int32_t nelim;                /* eliminated variables */
   int32_t wdtype;               /* TLS_F32 / TLS_F64 storage of W */
-  int32_t vec_dtype;            /* reduced vectors */
-  int32_t ept;                  /* edges per thread: chunks hold <= 256 * ept edges */
+  int32_t vec_dtype;            /* reduced vectors (float64) */
+  int32_t cap;                  /* edges per chunk slab: 512 (float32 W) or 256 (float64 W) */
+  int32_t meta_ints;            /* int32 words per chunk metadata slab: 5 * cap + 8 */
   int32_t nruns;
+  int32_t pad_;
   int64_t retained_offset;      /* tangent offset of the retained group (full vector) */
   int64_t elim_offset;          /* tangent offset of the eliminated group (full vector) */
-  const int32_t* chunk_ptr;     /* [nchunks+1] edge ranges */
-  const int32_t* cpt_ptr;       /* [nchunks+1] ranges into chunk_points */
-  const int32_t* chunk_points;  /* eliminated variables of each chunk, ascending */
-  const int32_t* cw_ptr;        /* [nchunks+1] 32-edge window ranges into win_run */
-  const int32_t* win_run;       /* first run id of each window */
-  const int32_t* edge_r;        /* [E] retained variable per edge (chunk order) */
-  const uint32_t* edge_meta;    /* [E] point slot in chunk | run head lane << 16 | run tail << 21 */
-  const int32_t* edge_e;        /* [E] eliminated variable per edge */
-  const int32_t* elim_ptr;      /* [nelim+1] CSR: edges of each eliminated variable */
-  const int32_t* elim_edges;    /* [E] edge positions, ascending */
-  const int32_t* run_ptr;       /* [nruns+1] edge ranges of each run */
-  const int32_t* rrun_ptr;      /* [nretained+1] CSR: runs of each retained variable */
-  const int32_t* rrun_list;     /* [nruns] run ids in chunk order */
-  const double* cross;          /* [E][dr][de] J_r^T J_e per edge (unscaled) */
+  const int32_t* meta;          /* [nchunks][meta_ints]: [ne, np, 0, 0][edge_r][meta][tail pos][pt ptr][pt edges] */
+  const int32_t* slab_r;        /* [nchunks*cap] retained variable per slab entry (-1: padding) */
+  const int32_t* slab_e;        /* [nchunks*cap] eliminated variable per slab entry */
+  const int32_t* elim_ptr;      /* [nelim+1] CSR: slab entries of each eliminated variable */
+  const int32_t* elim_slab;     /* [E] slab indices, ascending */
+  const int32_t* rrun_ptr;      /* [nretained+1] CSR over retained-major run positions */
+  const int32_t* crun_start;    /* [nruns] first slab index of each run (retained-major) */
+  const int32_t* crun_len;      /* [nruns] edges in each run */
+  const double* cross;          /* [nchunks*cap][dr][de] J_r^T J_e per slab entry (unscaled) */
   const double* elim_diag;      /* [nelim][de][de] eliminated diagonal blocks (unscaled) */
   const double* ret_diag;       /* [nretained][dr][dr] retained diagonal blocks (unscaled) */
   const double* scale;          /* [n_full] column scale or NULL */
   double* inv_l;                /* [nelim][de][de] L^-1, L = chol(s C s + lambda I) */
-  void* w;                      /* [dr*de][E] whitened W (SoA, wdtype) */
-  double* run_partial;          /* [nruns][dr] workspace */
+  void* w;                      /* [nchunks][dr*de][cap] whitened W slabs (wdtype), 16-byte aligned */
+  double* run_partial;          /* [nruns][dr] workspace, retained-major */
   double* ybuf;                 /* [nelim][de] workspace: L^-1 b_e */
   double damping;
   int32_t* bad;                 /* device: number of non-PD eliminated blocks */
+  int32_t* err;                 /* device: set to 1 if a bounded wait gave up (never expected) */
 };
 
 /* Factor eliminated blocks and whiten every edge (schur.py:263-283). */

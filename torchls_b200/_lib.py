@@ -86,12 +86,11 @@ class PcgControl(C.Structure):
 class SchurArgs(C.Structure):
     _fields_ = [
         ("nedges", i32), ("nchunks", i32), ("dr", i32), ("de", i32), ("nretained", i32), ("nelim", i32),
-        ("wdtype", i32), ("vec_dtype", i32), ("ept", i32), ("nruns", i32),
-        ("retained_offset", i64), ("elim_offset", i64), ("chunk_ptr", vp), ("cpt_ptr", vp),
-        ("chunk_points", vp), ("cw_ptr", vp), ("win_run", vp), ("edge_r", vp), ("edge_meta", vp),
-        ("edge_e", vp), ("elim_ptr", vp), ("elim_edges", vp), ("run_ptr", vp), ("rrun_ptr", vp),
-        ("rrun_list", vp), ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp),
-        ("w", vp), ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp),
+        ("wdtype", i32), ("vec_dtype", i32), ("cap", i32), ("meta_ints", i32), ("nruns", i32), ("pad_", i32),
+        ("retained_offset", i64), ("elim_offset", i64), ("meta", vp), ("slab_r", vp), ("slab_e", vp),
+        ("elim_ptr", vp), ("elim_slab", vp), ("rrun_ptr", vp), ("crun_start", vp), ("crun_len", vp),
+        ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp), ("w", vp),
+        ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp), ("err", vp),
     ]
 
 

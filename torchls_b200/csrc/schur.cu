@@ -1,71 +1,140 @@
 // Schur complement of one eliminated group (torchls schur.py:192-397).
 //
-// Edges (retained i, eliminated p) live in a chunked order: a chunk holds
-// whole eliminated variables, and inside a chunk the edges are sorted by
-// retained variable, so equal-retained edges form contiguous runs.
+// Edges (retained i, eliminated p) live in chunks of whole eliminated
+// variables. Each chunk owns a fixed-size, 16-byte aligned slab: W as
+// [dr*de][cap] plus an int32 metadata block. The reduced matvec
+// S x = (s U s + lambda I) x - W (W^T x) never forms S:
 //
-// Reduced matvec S x = (s U s + lambda I) x - W (W^T x), without forming S:
-//   chunk kernel   t_e = W_e^T x_i          (W_e loaded once, kept in registers)
-//                  y_p = sum_{e in p} t_e   (fixed order, shared memory)
-//                  u_e = W_e y_p
-//                  partial[run] = warp-segmented sum of u_e over the run
-//   gather kernel  out_i = base_i - sum_{runs of i} partial[run]
-// W is read from HBM exactly once per matvec; 8 bytes of edge metadata ride
-// along. Every sum follows a fixed order: deterministic.
+//   chunk kernel (persistent grid, 2 CTAs/SM). Thread 0 streams chunk slabs
+//   into shared memory with 1-D bulk copies (cp.async.bulk, TMA) completing
+//   on an mbarrier; two stages, so chunk c+grid loads while chunk c computes.
+//     phase 1   t_e = W_e^T x_i                 (per edge, into shared memory)
+//     phase 1.5 y_p = sum_{e in p} t_e          (per eliminated variable, fixed order)
+//     phase 2   u_e = W_e y_p; warp-segmented inclusive scan over runs of
+//               equal retained variable (runs never cross a 32-edge window);
+//               the run's last lane stores the run partial, retained-major.
+//   gather kernel (one block per retained variable) sums its contiguous run
+//   partials in a fixed order and adds the diagonal term; its last block
+//   finalises the PCG curvature.
+//
+// W is read from HBM exactly once per matvec. Every sum follows a fixed order:
+// results are bitwise reproducible. Every mbarrier wait is bounded: on
+// timeout the kernel raises a.err and keeps going (it never hangs).
+#include <stdint.h>
+
 #include "blocks.cuh"
 #include "common.cuh"
 #include "pcg_state.cuh"
 
 namespace tls {
 
-template <typename TW>
-__device__ __forceinline__ TW ldw(const void* w, int64_t idx) {
-  return __ldg(reinterpret_cast<const TW*>(w) + idx);
+constexpr int kChunkThreads = 256;
+constexpr int kMetaHead = 4;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-constexpr int kChunkThreads = 256;
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
 
-// One thread block per chunk. MODE 0: S x (y_p = sum_{e in p} W_e^T x_i);
-// MODE 1: reduced rhs (y_p = L_p^-1 b_p taken from a.ybuf).
-//   phase 1   (MODE 0) t_e = W_e^T x_i for each edge; W_e stays in registers
-//   phase 1.5 y_p = sum of the t_e of p's edges, once per eliminated variable
-//   phase 2   u_e = W_e y_p; warp-segmented inclusive scan over runs (a run
-//             never crosses a 32-edge window); the run's last lane stores it.
-template <int DR, int DE, int EPT, int MODE, typename TW>
-__global__ void __launch_bounds__(kChunkThreads, 2)
-schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
-  constexpr int CAP = kChunkThreads * EPT;
-  extern __shared__ double smem[];
-  double* t_s = smem;             // [CAP][DE] per-edge W^T x
-  double* y_s = smem + CAP * DE;  // [CAP][DE] per-variable sums
-  const int c = blockIdx.x;
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int e0 = __ldg(a.chunk_ptr + c), ne = __ldg(a.chunk_ptr + c + 1) - e0;
-  const int p0 = __ldg(a.cpt_ptr + c), np = __ldg(a.cpt_ptr + c + 1) - p0;
-  const int64_t E = a.nedges;
-  const TW* __restrict__ W = reinterpret_cast<const TW*>(a.w);
-  TW w[EPT][DR * DE];
-  uint32_t meta[EPT];
-#pragma unroll
-  for (int j = 0; j < EPT; ++j) {
-    const int le = j * kChunkThreads + tid;
-    meta[j] = 0;
-    if (le < ne) {
-      const int64_t e = e0 + le;
-#pragma unroll
-      for (int k = 0; k < DR * DE; ++k) w[j][k] = __ldg(W + k * E + e);
-      meta[j] = __ldg(a.edge_meta + e);
-    } else {
-#pragma unroll
-      for (int k = 0; k < DR * DE; ++k) w[j][k] = TW(0);
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
+// Both addresses are 16-byte aligned and `bytes` is a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Bounded wait on a bulk-copy barrier: gives up after ~2^31 SM cycles (about
+// one second) and flags the error instead of hanging.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1LL << 31)) {
+      if (err) atomicExch(err, 1);
+      return;
     }
   }
-  if constexpr (MODE == 0) {
-#pragma unroll
-    for (int j = 0; j < EPT; ++j) {
-      const int le = j * kChunkThreads + tid;
-      if (le < ne) {
-        const int64_t i = __ldg(a.edge_r + e0 + le);
+}
+
+template <int DR, int DE, int CAP, typename TW>
+struct SlabShape {
+  static constexpr int kWBytes = DR * DE * CAP * (int)sizeof(TW);
+  static constexpr int kMetaInts = 5 * CAP + 8;
+  static constexpr int kMetaBytes = kMetaInts * 4;
+  static constexpr int kStageBytes = kWBytes + kMetaBytes;
+  static constexpr int kTBytes = CAP * DE * (int)sizeof(double);
+  static constexpr int kSmemBytes = 2 * kStageBytes + kTBytes;
+  static_assert(kWBytes % 16 == 0 && kMetaBytes % 16 == 0, "slabs must be 16-byte multiples");
+};
+
+// MODE 0: S x partials (phase 1 from x); MODE 1: reduced rhs (y_p = a.ybuf[p]).
+template <int DR, int DE, int CAP, int MODE, typename TW>
+__global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
+  using S = SlabShape<DR, DE, CAP, TW>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  double* t_s = reinterpret_cast<double*>(smem + 2 * S::kStageBytes);  // [CAP][DE], reused for y
+  const int tid = threadIdx.x, lane = tid & 31;
+  const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
+  const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int c, int stg) {
+    unsigned char* base = smem + stg * S::kStageBytes;
+    fence_proxy_async();
+    mbar_expect_tx(&bar[stg], S::kStageBytes);
+    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &bar[stg]);
+    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &bar[stg]);
+  };
+  if (tid == 0 && (int)blockIdx.x < a.nchunks) issue(blockIdx.x, 0);
+  int it = 0;
+  for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x, ++it) {
+    const int stg = it & 1;
+    if (tid == 0 && c + (int)gridDim.x < a.nchunks) issue(c + gridDim.x, stg ^ 1);
+    mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+    const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
+    const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
+    const int ne = Ms[0], np = Ms[1];
+    const int32_t* er = Ms + kMetaHead;
+    const uint32_t* meta = reinterpret_cast<const uint32_t*>(Ms + kMetaHead + CAP);
+    const int32_t* tpos = Ms + kMetaHead + 2 * CAP;
+    const int32_t* pp = Ms + kMetaHead + 3 * CAP;
+    const int32_t* pe = Ms + 2 * kMetaHead + 4 * CAP;
+    // ---- phase 1: t_e = W_e^T x_i
+    if constexpr (MODE == 0) {
+      for (int le = tid; le < ne; le += kChunkThreads) {
+        const int64_t i = er[le];
         double xr[DR];
 #pragma unroll
         for (int k = 0; k < DR; ++k) xr[k] = __ldg(x + i * DR + k);
@@ -73,67 +142,78 @@ schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
         for (int b = 0; b < DE; ++b) {
           double acc = 0.0;
 #pragma unroll
-          for (int k = 0; k < DR; ++k) acc += static_cast<double>(w[j][k * DE + b]) * xr[k];
+          for (int k = 0; k < DR; ++k) acc += static_cast<double>(Ws[(k * DE + b) * CAP + le]) * xr[k];
           t_s[le * DE + b] = acc;
+        }
+      }
+      __syncthreads();
+    }
+    // ---- phase 1.5: y_p per eliminated variable (<= CAP / 256 per thread), then overwrite t_s
+    constexpr int PPT = CAP / kChunkThreads;
+    double yreg[PPT][DE];
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int pl = tid + q * kChunkThreads;
+#pragma unroll
+      for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
+      if (pl < np) {
+        if constexpr (MODE == 0) {
+          for (int j = pp[pl]; j < pp[pl + 1]; ++j) {
+            const int lj = pe[j];
+#pragma unroll
+            for (int b = 0; b < DE; ++b) yreg[q][b] += t_s[lj * DE + b];
+          }
+        } else {
+          const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + pe[pp[pl]]);
+#pragma unroll
+          for (int b = 0; b < DE; ++b) yreg[q][b] = a.ybuf[p * DE + b];
         }
       }
     }
     __syncthreads();
-    for (int pl = tid; pl < np; pl += kChunkThreads) {
-      const int p = __ldg(a.chunk_points + p0 + pl);
-      const int jb = __ldg(a.elim_ptr + p), je = __ldg(a.elim_ptr + p + 1);
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int pl = tid + q * kChunkThreads;
+      if (pl < np) {
+#pragma unroll
+        for (int b = 0; b < DE; ++b) t_s[pl * DE + b] = yreg[q][b];
+      }
+    }
+    __syncthreads();
+    // ---- phase 2: u_e = W_e y_p, warp-segmented run sums
+    for (int base = 0; base < ne; base += kChunkThreads) {
+      const int le = base + tid;
+      const bool valid = le < ne;
+      const uint32_t m = valid ? meta[le] : 0u;
+      const int pl = m & 0xFFFFu;
+      const int head = (m >> 16) & 31;
+      const bool tail = valid && ((m >> 21) & 1u);
       double y[DE];
 #pragma unroll
-      for (int b = 0; b < DE; ++b) y[b] = 0.0;
-      for (int jj = jb; jj < je; ++jj) {
-        const int lj = __ldg(a.elim_edges + jj) - e0;
+      for (int b = 0; b < DE; ++b) y[b] = valid ? t_s[pl * DE + b] : 0.0;
+      const int64_t pos = tail ? (int64_t)tpos[le] : 0;
 #pragma unroll
-        for (int b = 0; b < DE; ++b) y[b] += t_s[lj * DE + b];
+      for (int k = 0; k < DR; ++k) {
+        double u = 0.0;
+        if (valid) {
+#pragma unroll
+          for (int b = 0; b < DE; ++b) u += static_cast<double>(Ws[(k * DE + b) * CAP + le]) * y[b];
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const double v = __shfl_up_sync(0xffffffffu, u, off);
+          if (lane - off >= head) u += v;
+        }
+        if (tail) a.run_partial[pos * DR + k] = u;
       }
-#pragma unroll
-      for (int b = 0; b < DE; ++b) y_s[pl * DE + b] = y[b];
     }
-  } else {
-    for (int pl = tid; pl < np; pl += kChunkThreads) {
-      const int64_t p = __ldg(a.chunk_points + p0 + pl);
-#pragma unroll
-      for (int b = 0; b < DE; ++b) y_s[pl * DE + b] = a.ybuf[p * DE + b];
-    }
-  }
-  __syncthreads();
-  const int wbase = __ldg(a.cw_ptr + c);
-#pragma unroll
-  for (int j = 0; j < EPT; ++j) {
-    const int le = j * kChunkThreads + tid;
-    if (j * kChunkThreads >= ne) break;  // uniform across the block
-    const bool valid = le < ne;
-    const uint32_t m = valid ? meta[j] : 0u;
-    const int pl = m & 0xFFFFu;
-    const int head = (m >> 16) & 31;
-    const bool tail = valid && ((m >> 21) & 1u);
-    double y[DE];
-#pragma unroll
-    for (int b = 0; b < DE; ++b) y[b] = valid ? y_s[pl * DE + b] : 0.0;
-    const unsigned tails = __ballot_sync(0xffffffffu, tail);
-    const int run = tail ? __ldg(a.win_run + wbase + (le >> 5)) + __popc(tails & ((1u << lane) - 1u)) : 0;
-    // one output component at a time keeps few doubles live
-#pragma unroll
-    for (int k = 0; k < DR; ++k) {
-      double u = 0.0;
-#pragma unroll
-      for (int b = 0; b < DE; ++b) u += static_cast<double>(w[j][k * DE + b]) * y[b];
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const double v = __shfl_up_sync(0xffffffffu, u, off);
-        if (lane - off >= head) u += v;
-      }
-      if (tail) a.run_partial[(int64_t)run * DR + k] = u;
-    }
+    __syncthreads();
   }
 }
 
-// One block per retained variable: sum its runs in a fixed order, then
-// MODE 0: out = s U s x + lambda x - sum  (matvec, optional dot partial per block)
+// One block per retained variable: sum its contiguous run partials in a fixed
+// order, then
+// MODE 0: out = s U s x + lambda x - sum  (matvec; dot partial + PCG epilogue)
 // MODE 1: out = b_retained - sum          (reduced rhs, b float64 full vector)
 template <int DR, int MODE, typename TV>
 __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, const TV* __restrict__ x,
@@ -148,9 +228,8 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
   for (int k = 0; k < DR; ++k) acc[k] = 0.0;
   const int rb = __ldg(a.rrun_ptr + i), re = __ldg(a.rrun_ptr + i + 1);
   for (int j = rb + tid; j < re; j += 256) {
-    const int64_t run = __ldg(a.rrun_list + j);
 #pragma unroll
-    for (int k = 0; k < DR; ++k) acc[k] += a.run_partial[run * DR + k];
+    for (int k = 0; k < DR; ++k) acc[k] += a.run_partial[(int64_t)j * DR + k];
   }
 #pragma unroll
   for (int k = 0; k < DR; ++k) {
@@ -196,9 +275,15 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
   if (MODE == 0 && pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
 }
 
-// Per eliminated variable: L = chol(s C s + lambda I), store L^-1; y = L^-1 b_e optional.
+// W slab index of component k of slab entry s.
+template <int DR, int DE>
+__device__ __forceinline__ int64_t w_index(int64_t s, int k, int cap) {
+  return ((s / cap) * (DR * DE) + k) * cap + (s % cap);
+}
+
+// Per eliminated variable: L = chol(s C s + lambda I), store L^-1.
 template <int DE>
-__global__ void schur_factor_kernel(tls_schur_args a, const double* __restrict__ b) {
+__global__ void schur_factor_kernel(tls_schur_args a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.nelim) return;
   double C[DE * DE], L[DE * DE], s[DE];
@@ -227,20 +312,26 @@ __global__ void schur_factor_kernel(tls_schur_args a, const double* __restrict__
   for (int k = 0; k < DE * DE; ++k) a.inv_l[p * DE * DE + k] = Li[k];
 }
 
-// W_e = diag(s_i) E_e diag(s_p) L_p^-T, stored SoA [dr*de][E]
+// W_e = diag(s_i) E_e diag(s_p) L_p^-T into the slabs; padding entries get 0.
 template <int DR, int DE, typename TW>
 __global__ void schur_whiten_kernel(tls_schur_args a) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.nedges) return;
-  const int64_t i = a.edge_r[e], p = a.edge_e[e];
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= (int64_t)a.nchunks * a.cap) return;
+  TW* w = reinterpret_cast<TW*>(a.w);
+  const int64_t i = a.slab_r[s];
+  if (i < 0) {
+#pragma unroll
+    for (int k = 0; k < DR * DE; ++k) w[w_index<DR, DE>(s, k, a.cap)] = TW(0);
+    return;
+  }
+  const int64_t p = a.slab_e[s];
   double sr[DR], se[DE];
 #pragma unroll
   for (int k = 0; k < DR; ++k) sr[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
 #pragma unroll
   for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
   const double* Li = a.inv_l + p * DE * DE;
-  const double* E = a.cross + e * DR * DE;
-  TW* w = reinterpret_cast<TW*>(a.w);
+  const double* E = a.cross + s * DR * DE;
 #pragma unroll
   for (int r = 0; r < DR; ++r) {
 #pragma unroll
@@ -248,7 +339,7 @@ __global__ void schur_whiten_kernel(tls_schur_args a) {
       double v = 0.0;
 #pragma unroll
       for (int k = 0; k < DE; ++k) v += sr[r] * E[r * DE + k] * se[k] * Li[c * DE + k];
-      w[(int64_t)(r * DE + c) * a.nedges + e] = static_cast<TW>(v);
+      w[w_index<DR, DE>(s, r * DE + c, a.cap)] = static_cast<TW>(v);
     }
   }
 }
@@ -268,7 +359,7 @@ __global__ void schur_elim_rhs_kernel(tls_schur_args a, const double* __restrict
   }
 }
 
-// delta_p = L_p^-T (y_p - sum_{e in p} W_e^T x_i); delta_full retained part = x
+// delta_p = L_p^-T (y_p - sum_{e in p} W_e^T x_i); the retained part of delta is x
 template <int DR, int DE, typename TW, typename TV>
 __global__ void schur_backsub_kernel(tls_schur_args a, const TV* __restrict__ xc, double* __restrict__ delta) {
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -276,18 +367,19 @@ __global__ void schur_backsub_kernel(tls_schur_args a, const TV* __restrict__ xc
   if (tid < nret) delta[a.retained_offset + tid] = to_d(xc[tid]);
   if (tid >= a.nelim) return;
   const int64_t p = tid;
+  const TW* w = reinterpret_cast<const TW*>(a.w);
   double t[DE];
 #pragma unroll
   for (int b = 0; b < DE; ++b) t[b] = a.ybuf[p * DE + b];
   const int pb = a.elim_ptr[p], pe = a.elim_ptr[p + 1];
   for (int j = pb; j < pe; ++j) {
-    const int e = a.elim_edges[j];
-    const int64_t i = a.edge_r[e];
+    const int64_t s = a.elim_slab[j];
+    const int64_t i = a.slab_r[s];
 #pragma unroll
     for (int b = 0; b < DE; ++b) {
       double acc = 0.0;
 #pragma unroll
-      for (int k = 0; k < DR; ++k) acc += to_d(ldw<TW>(a.w, (int64_t)(k * DE + b) * a.nedges + e)) * to_d(xc[i * DR + k]);
+      for (int k = 0; k < DR; ++k) acc += to_d(w[w_index<DR, DE>(s, k * DE + b, a.cap)]) * to_d(xc[i * DR + k]);
       t[b] -= acc;
     }
   }
@@ -306,6 +398,7 @@ template <int DR, int DE, typename TW>
 __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, double* __restrict__ out) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  const TW* w = reinterpret_cast<const TW*>(a.w);
   double acc[DR * (DR + 1) / 2];
 #pragma unroll
   for (int k = 0; k < DR * (DR + 1) / 2; ++k) acc[k] = 0.0;
@@ -313,13 +406,14 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
   if (live) {
     const int rb = a.rrun_ptr[warp], re = a.rrun_ptr[warp + 1];
     for (int j = rb + lane; j < re; j += 32) {
-      const int run = a.rrun_list[j];
-      for (int e = a.run_ptr[run]; e < a.run_ptr[run + 1]; ++e) {
+      const int64_t s0 = a.crun_start[j];
+      const int len = a.crun_len[j];
+      for (int64_t s = s0; s < s0 + len; ++s) {
         double wv[DR][DE];
 #pragma unroll
         for (int r = 0; r < DR; ++r)
 #pragma unroll
-          for (int c = 0; c < DE; ++c) wv[r][c] = to_d(ldw<TW>(a.w, (int64_t)(r * DE + c) * a.nedges + e));
+          for (int c = 0; c < DE; ++c) wv[r][c] = to_d(w[w_index<DR, DE>(s, r * DE + c, a.cap)]);
         int idx = 0;
 #pragma unroll
         for (int r = 0; r < DR; ++r)
@@ -355,25 +449,36 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
 
 template <int DR, int DE>
 struct SchurOps {
-  template <int MODE, typename TW, int EPT>
-  static int chunks_ept(const tls_schur_args& a, const double* x, cudaStream_t s) {
-    constexpr size_t smem = 2 * sizeof(double) * kChunkThreads * EPT * DE;
-    auto k = schur_chunk_kernel<DR, DE, EPT, MODE, TW>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k<<<a.nchunks, kChunkThreads, smem, s>>>(a, x);
+  template <int MODE, typename TW, int CAP>
+  static int chunks_cap(const tls_schur_args& a, const double* x, cudaStream_t s) {
+    using S = SlabShape<DR, DE, CAP, TW>;
+    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
+    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
+      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
+    auto k = schur_chunk_kernel<DR, DE, CAP, MODE, TW>;
+    static int grid_cap = 0;  // resident CTAs per SM x SMs, computed once per instantiation
+    if (grid_cap == 0) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes);
+      int per_sm = 0, dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, S::kSmemBytes);
+      grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    }
+    const int grid = a.nchunks < grid_cap ? a.nchunks : grid_cap;
+    k<<<grid, kChunkThreads, S::kSmemBytes, s>>>(a, x);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
   template <int MODE, typename TW>
   static int chunks(const tls_schur_args& a, const double* x, cudaStream_t s) {
     if (a.nchunks == 0) return TLS_OK;
-    // 2 edges per thread: W stays in registers between the phases
     if constexpr (sizeof(TW) == 4) {
-      if (a.ept != 2) return tls_set_error(TLS_ERR_INVALID, "Schur layouts use 2 edges per thread");
-      return chunks_ept<MODE, TW, 2>(a, x, s);
+      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs");
+      return chunks_cap<MODE, TW, 512>(a, x, s);
     } else {
-      if (a.ept != 2) return tls_set_error(TLS_ERR_INVALID, "float64 W needs a 2-edge-per-thread layout");
-      return chunks_ept<MODE, TW, 2>(a, x, s);
+      if (a.cap != 256) return tls_set_error(TLS_ERR_INVALID, "float64 W uses 256-edge chunk slabs");
+      return chunks_cap<MODE, TW, 256>(a, x, s);
     }
   }
   template <typename TW, typename TV, typename TA>
@@ -401,16 +506,17 @@ struct SchurOps {
   template <typename TW>
   static int damp(const tls_schur_args& a, cudaStream_t s) {
     cudaMemsetAsync(a.bad, 0, sizeof(int32_t), s);
-    if (a.nelim > 0) schur_factor_kernel<DE><<<(a.nelim + 127) / 128, 128, 0, s>>>(a, nullptr);
+    if (a.nelim > 0) schur_factor_kernel<DE><<<(a.nelim + 127) / 128, 128, 0, s>>>(a);
     TLS_CHECK_LAUNCH();
-    if (a.nedges > 0) schur_whiten_kernel<DR, DE, TW><<<(a.nedges + 127) / 128, 128, 0, s>>>(a);
+    const int64_t nslab = (int64_t)a.nchunks * a.cap;
+    if (nslab > 0) schur_whiten_kernel<DR, DE, TW><<<(unsigned)((nslab + 127) / 128), 128, 0, s>>>(a);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
   template <typename TW, typename TV>
   static int backsub(const tls_schur_args& a, const TV* xc, double* delta, cudaStream_t s) {
     const int64_t n = a.nelim > (int64_t)a.nretained * DR ? a.nelim : (int64_t)a.nretained * DR;
-    if (n > 0) schur_backsub_kernel<DR, DE, TW, TV><<<(n + 127) / 128, 128, 0, s>>>(a, xc, delta);
+    if (n > 0) schur_backsub_kernel<DR, DE, TW, TV><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, xc, delta);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
@@ -435,12 +541,8 @@ static int dispatch_dims(int dr, int de, F&& f) {
   TLS_D(1, 1)
   TLS_D(2, 2)
   TLS_D(3, 2)
-  TLS_D(6, 6)
   TLS_D(2, 1)
   TLS_D(1, 3)
-  TLS_D(8, 3)
-  TLS_D(6, 4)
-  TLS_D(4, 3)
 #undef TLS_D
   return tls_set_error(TLS_ERR_UNSUPPORTED, "Schur block dims not instantiated");
 }

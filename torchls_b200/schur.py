@@ -89,7 +89,20 @@ class SchurPlan:
         self.global_indices = torch.arange(self.r.offset, self.r.offset + self.r.size, device=device)
         self.layout = (self.r,)
         self.bad = torch.zeros(1, dtype=torch.int32, device=device)
-        self.chunks = ChunkLayout(self)
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        self._layouts = {}
+
+    def chunks_for(self, wdtype) -> ChunkLayout:
+        """Slab layout for W stored as ``wdtype`` (512 edges per chunk for
+        float32, 256 for float64: 36 KB of W per chunk either way)."""
+        cap = 512 if wdtype == torch.float32 else 256
+        if cap not in self._layouts:
+            self._layouts[cap] = ChunkLayout(self, cap)
+        return self._layouts[cap]
+
+    @property
+    def chunks(self) -> ChunkLayout:
+        return self.chunks_for(torch.float64)
 
     # ---------------------------------------------------------------- linearization hooks
     def cross_buffer(self, device):
@@ -109,24 +122,29 @@ class SchurPlan:
 
 
 class ChunkLayout:
-    """Chunked edge order used by the kernels (one thread block per chunk).
+    """Chunked, slab-padded edge layout used by the kernels.
 
-    Eliminated variables are ordered by their smallest retained neighbour, so
-    a chunk's edges touch few retained variables and runs are long. Chunks
-    hold whole eliminated variables and at most ``CHUNK_EDGES`` edges; inside
-    a chunk edges are sorted by retained variable and cut into runs that
-    never cross a 32-edge window.
+    Eliminated variables are ordered by their smallest retained neighbour (so
+    a chunk's edges touch few retained variables) and packed into chunks of
+    whole variables with at most ``cap`` edges. Inside a chunk edges are
+    sorted by retained variable and cut into runs that never cross a 32-edge
+    window. Each chunk owns a fixed-size, 16-byte aligned slab: W as
+    [dr*de][cap] and an int32 metadata block
+        [ne, np, 0, 0][edge_r: cap][meta: cap][tail run position: cap]
+        [point edge ptr: cap + 4][point edge list: cap]
+    so one bulk copy brings a chunk into shared memory. Edge ``slab index``
+    = chunk * cap + position. Run partials are stored retained-major
+    (``rrun_ptr``), so each retained variable sums a contiguous range.
     """
 
-    THREADS, EPT = 256, 2
-    CHUNK_EDGES = THREADS * EPT
+    THREADS = 256
 
-    def __init__(self, plan: SchurPlan):
+    def __init__(self, plan: SchurPlan, cap: int):
         ri, ei, E, P = plan._ri, plan._ei, plan.nedges, plan.E_count
         device = plan.device
+        self.cap = cap
         deg = np.bincount(ei, minlength=P)
         max_deg = int(deg.max()) if E else 0
-        cap = self.CHUNK_EDGES
         if max_deg > cap:
             raise ValueError(f"an eliminated variable has {max_deg} retained neighbours; the CUDA Schur path "
                              f"supports at most {cap}")
@@ -141,69 +159,92 @@ class ChunkLayout:
         chunk_of_rank = start // max(1, cap - max_deg + 1)
         ch = chunk_of_rank[rank[ei]]
         order = np.lexsort((ei, ri, ch))
-        # chunk ids renumbered densely in order of appearance
         c_r, c_e, c_raw = ri[order], ei[order], ch[order]
         newchunk = np.ones(E, bool)
         newchunk[1:] = c_raw[1:] != c_raw[:-1]
         cid = np.cumsum(newchunk) - 1
         nchunks = int(cid[-1]) + 1 if E else 0
         chunk_ptr = np.concatenate((np.flatnonzero(newchunk), [E])).astype(np.int64)
+        ne = np.diff(chunk_ptr)
         local = np.arange(E) - chunk_ptr[cid] if E else np.zeros(0, np.int64)
+        sidx = cid * cap + local
+        # runs: equal retained variable, split at 32-edge windows
         newrun = newchunk.copy()
         newrun[1:] |= c_r[1:] != c_r[:-1]
         newrun |= (local % 32) == 0
         run_starts = np.flatnonzero(newrun)
         nruns = len(run_starts)
         run_id = np.cumsum(newrun) - 1
-        run_ptr = np.concatenate((run_starts, [E]))
-        head = local[run_starts][run_id] % 32 if E else np.zeros(0, np.int64)
+        run_end = np.concatenate((run_starts[1:], [E]))
+        head = (local[run_starts] % 32)[run_id] if E else np.zeros(0, np.int64)
+        run_r = c_r[run_starts]
+        cm = np.argsort(run_r, kind="stable")  # retained-major position -> run id
+        run_pos = np.empty(nruns, np.int64)
+        run_pos[cm] = np.arange(nruns)
+        rrun_ptr = np.concatenate(([0], np.cumsum(np.bincount(run_r, minlength=plan.r.count))))
+        crun_start = sidx[run_starts][cm] if E else np.zeros(0, np.int64)
+        crun_len = (run_end - run_starts)[cm]
         tail = np.zeros(E, bool)
         if E:
-            tail[run_ptr[1:] - 1] = True
-        # chunk points: distinct eliminated variables per chunk, ascending
+            tail[run_end - 1] = True
+        tailpos = np.where(tail, run_pos[run_id], -1) if E else np.zeros(0, np.int64)
+        # chunk points and their local edge lists
         ckey = cid * P + c_e
         uniq_cp, cp_inv = np.unique(ckey, return_inverse=True)
         cpt_chunk = uniq_cp // P
         cpt_ptr = np.searchsorted(cpt_chunk, np.arange(nchunks + 1))
-        chunk_points = uniq_cp % P
+        npts = np.diff(cpt_ptr)
         pl = cp_inv - cpt_ptr[cid] if E else np.zeros(0, np.int64)
-        if E and pl.max() >= 1 << 16:
-            raise ValueError("too many eliminated variables in one chunk")
-        meta = (pl | (head << 16) | (tail.astype(np.int64) << 21)).astype(np.uint32)
-        # windows: first run id of each 32-edge window of each chunk
-        nwin = (np.diff(chunk_ptr) + 31) // 32
-        cw_ptr = np.concatenate(([0], np.cumsum(nwin)))
-        win_start_edge = (np.repeat(chunk_ptr[:-1], nwin)
-                          + 32 * (np.arange(int(cw_ptr[-1])) - np.repeat(cw_ptr[:-1], nwin)))
-        win_run = run_id[win_start_edge] if E else np.zeros(0, np.int64)
-        run_r = c_r[run_starts]
-        rorder = np.argsort(run_r, kind="stable")
-        rrun_ptr = np.concatenate(([0], np.cumsum(np.bincount(run_r, minlength=plan.r.count))))
-        eorder = np.lexsort((np.arange(E), c_e))
+        meta = pl | (head << 16) | (tail.astype(np.int64) << 21)
+        # ---- metadata slab
+        self.meta_ints = 5 * cap + 8
+        M = np.zeros((max(nchunks, 1), self.meta_ints), np.int64)
+        off_r, off_m, off_t, off_pp, off_pe = 4, 4 + cap, 4 + 2 * cap, 4 + 3 * cap, 8 + 4 * cap
+        if nchunks:
+            M[:nchunks, 0] = ne
+            M[:nchunks, 1] = npts
+            M[cid, off_r + local] = c_r
+            M[cid, off_m + local] = meta
+            M[cid, off_t + local] = tailpos
+            # point-local CSR: edges of each chunk point in ascending local position
+            po = np.lexsort((local, pl, cid))
+            pcount = np.bincount(cp_inv, minlength=len(uniq_cp))
+            pstart = np.cumsum(pcount) - pcount  # global start per (chunk, point)
+            local_start = pstart - pstart[cpt_ptr[cpt_chunk]]
+            M[cpt_chunk, off_pp + (np.arange(len(uniq_cp)) - cpt_ptr[cpt_chunk])] = local_start
+            M[np.arange(nchunks), off_pp + npts] = ne
+            rank_in_chunk = np.arange(E) - chunk_ptr[cid[po]]
+            M[cid[po], off_pe + rank_in_chunk] = local[po]
+        self.nchunks, self.nruns, self.nedges = nchunks, nruns, E
+        self.order, self.pos_of_edge = order, np.empty(E, np.int64)
+        self.pos_of_edge[order] = np.arange(E)
+        self.slab_of_edge = np.empty(E, np.int64)
+        self.slab_of_edge[order] = sidx  # reference edge -> slab index
+        nslab = max(nchunks, 1) * cap
+        slab_r = np.full(nslab, -1, np.int64)
+        slab_e = np.full(nslab, -1, np.int64)
+        slab_r[sidx], slab_e[sidx] = c_r, c_e
+        eorder = np.lexsort((sidx, c_e))
         elim_ptr = np.concatenate(([0], np.cumsum(np.bincount(c_e, minlength=P))))
-        pos_of_edge = np.empty(E, np.int64)
-        pos_of_edge[order] = np.arange(E)
-        self.order, self.pos_of_edge = order, pos_of_edge
-        self.nchunks, self.nruns = nchunks, nruns
-        # cross-contribution segments per edge (chunk order)
+        # cross-contribution segments per slab entry
         cursor, ids, offs = 0, [], []
         for k, s_, n in plan._records:
             info = plan.plan_info[k]
-            ids.append(pos_of_edge[plan._inverse[cursor : cursor + n]])
+            ids.append(self.slab_of_edge[plan._inverse[cursor : cursor + n]])
             offs.append(info["base"] + np.arange(n, dtype=np.int64) * info["width"] + info["slot_cross"][s_])
             cursor += n
         ids = np.concatenate(ids) if ids else np.zeros(0, np.int64)
         offs = np.concatenate(offs) if offs else np.zeros(0, np.int64)
         o = np.argsort(ids, kind="stable")
-        cptr = np.concatenate(([0], np.cumsum(np.bincount(ids, minlength=E))))
+        cptr = np.concatenate(([0], np.cumsum(np.bincount(ids, minlength=nslab))))
         t = lambda a, dt=torch.int32: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt)
+        self.nslab = nslab
         self.dev = dict(
-            chunk_ptr=t(chunk_ptr), cpt_ptr=t(cpt_ptr), chunk_points=t(chunk_points), cw_ptr=t(cw_ptr),
-            win_run=t(win_run), edge_r=t(c_r), edge_meta=t(meta.view(np.int32)), edge_e=t(c_e),
-            elim_ptr=t(elim_ptr), elim_edges=t(eorder), run_ptr=t(run_ptr), rrun_ptr=t(rrun_ptr),
-            rrun_list=t(rorder), cross_ptr=t(cptr), cross_src=t(offs[o]),
+            meta=t(M.reshape(-1)), slab_r=t(slab_r), slab_e=t(slab_e), elim_ptr=t(elim_ptr),
+            elim_slab=t(sidx[eorder]), rrun_ptr=t(rrun_ptr), crun_start=t(crun_start), crun_len=t(crun_len),
+            cross_ptr=t(cptr), cross_src=t(offs[o]),
         )
-        self.cross_seg = L.Segments(E, plan.dr * plan.de, 1, 0, self.dev["cross_ptr"].data_ptr(),
+        self.cross_seg = L.Segments(nslab, plan.dr * plan.de, 1, 0, self.dev["cross_ptr"].data_ptr(),
                                     self.dev["cross_src"].data_ptr())
 
 
@@ -213,19 +254,19 @@ class SchurLinearization:
     def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
         self.plan = plan
         dev = plan.device
-        self.layout = plan.chunks
-        self.cross = torch.empty((plan.nedges, plan.dr, plan.de), dtype=torch.float64, device=dev)
+        self.layout = plan.chunks_for(wdtype)
+        lay = self.layout
+        self.cross = torch.empty((lay.nslab, plan.dr, plan.de), dtype=torch.float64, device=dev)
         if plan.nedges:
-            segment_reduce(self.layout.cross_seg, lin.cross_contrib, self.cross)
+            segment_reduce(lay.cross_seg, lin.cross_contrib, self.cross)
         self.ret_diag = diagonal_raw[plan.retained[0]].contiguous()
         self.elim_diag = diagonal_raw[plan.eliminated].contiguous()
         self.scale = None if scale is None else scale.to(torch.float64).contiguous()
         self.wdtype, self.vec_dtype = wdtype, vec_dtype
         self.dense = dense
-        n, E = plan.nedges, plan.nedges
-        self.w = torch.empty((plan.dr * plan.de, max(E, 1)), dtype=wdtype, device=dev)
+        self.w = torch.empty((lay.nslab * plan.dr * plan.de,), dtype=wdtype, device=dev)
         self.inv_l = torch.empty((plan.e.count, plan.de, plan.de), dtype=torch.float64, device=dev)
-        self.run_partial = torch.empty((max(self.layout.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
+        self.run_partial = torch.empty((max(lay.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
         self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
 
     def damped(self, damping):
@@ -250,11 +291,10 @@ class DampedSchurSystem:
         a.nretained, a.nelim = p.r.count, p.e.count
         a.wdtype, a.vec_dtype = L.dtype_code(lin.wdtype), L.dtype_code(lin.vec_dtype)
         lay = lin.layout
-        a.nchunks, a.ept, a.nruns = lay.nchunks, lay.EPT, lay.nruns
+        a.nchunks, a.cap, a.nruns, a.meta_ints = lay.nchunks, lay.cap, lay.nruns, lay.meta_ints
         a.retained_offset, a.elim_offset = p.r.offset, p.e.offset
         d = lay.dev
-        for name in ("chunk_ptr", "cpt_ptr", "chunk_points", "cw_ptr", "win_run", "edge_r", "edge_meta", "edge_e",
-                     "elim_ptr", "elim_edges", "run_ptr", "rrun_ptr", "rrun_list"):
+        for name in ("meta", "slab_r", "slab_e", "elim_ptr", "elim_slab", "rrun_ptr", "crun_start", "crun_len"):
             setattr(a, name, d[name].data_ptr())
         a.cross = lin.cross.data_ptr()
         a.elim_diag = lin.elim_diag.data_ptr()
@@ -266,6 +306,7 @@ class DampedSchurSystem:
         a.ybuf = lin.ybuf.data_ptr()
         a.damping = self.damping
         a.bad = p.bad.data_ptr()
+        a.err = p.err.data_ptr()
         return a
 
     @property
@@ -328,9 +369,13 @@ class DampedSchurSystem:
         S += self.damping * torch.eye(n, dtype=torch.float64, device=p.device)
         if E:
             # W rows (retained columns) x eliminated columns, sparse COO -> dense chunks
-            w = self.linear.w[:, :E].to(torch.float64).view(p.dr, p.de, E)
-            er = self.linear.layout.dev["edge_r"].long()
-            ee = self.linear.layout.dev["edge_e"].long()
+            lay = self.linear.layout
+            valid = (lay.dev["slab_r"] >= 0).nonzero().flatten()
+            slab = self.linear.w.view(lay.nslab // lay.cap, p.dr * p.de, lay.cap).permute(1, 0, 2).reshape(
+                p.dr, p.de, lay.nslab).to(torch.float64)
+            w = slab[:, :, valid]
+            er = lay.dev["slab_r"][valid].long()
+            ee = lay.dev["slab_e"][valid].long()
             cols_all = ee[:, None] * p.de + torch.arange(p.de, device=p.device)[None, :]
             rows_all = er[:, None] * p.dr + torch.arange(p.dr, device=p.device)[None, :]
             step = max(1, (1 << 27) // max(n, 1))
