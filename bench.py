@@ -183,10 +183,12 @@ def time_solves(problem, init, tls, precision, steps, warmup, device, flush):
         flush_l2(flush)
         torch.cuda.synchronize(device)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed_solve")
         start.record()
         _, summ = problem.solve(**opts)
         end.record()
         torch.cuda.synchronize(device)
+        torch.cuda.nvtx.range_pop()
         times.append(start.elapsed_time(end) / 1e3)
     launches = (_lib.launch_count() - launches0) // steps
     return times, summ, launches
