@@ -323,7 +323,10 @@ class DevicePCG:
         self.host = torch.empty(C.sizeof(L.PcgControl), dtype=torch.uint8, pin_memory=True)
 
     def run(self, rhs: Tensor, config: ConjugateGradientConfig, *, normal_args=None, schur_args=None,
-            preconditioner: BlockJacobiPreconditioner | None = None) -> PCGResult:
+            preconditioner: BlockJacobiPreconditioner | None = None, error_word: Tensor | None = None) -> PCGResult:
+        """``error_word``: the operator's device error flag (the Schur chunk
+        kernel's bounded bulk-copy waits set it instead of hanging); read once
+        after the loop."""
         a = L.PcgArgs()
         a.n = self.n
         a.vec_dtype = L.dtype_code(self.dtype)
@@ -355,6 +358,8 @@ class DevicePCG:
             if ctrl.status != L.PCG_ACTIVE:
                 break
             L.call("tls_pcg_run", C.byref(a), batch, stream)
+        if error_word is not None and int(error_word.item()) != 0:
+            raise RuntimeError("Schur matvec: a device wait for a bulk copy timed out")
         return PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
                          ctrl.status == L.PCG_CONVERGED, _REASONS[ctrl.status], int(ctrl.restarts),
                          int(ctrl.checks), float(ctrl.rhs_norm))
@@ -450,7 +455,7 @@ def pcg(matvec: Callable[[Tensor], Tensor], rhs: Tensor, *, preconditioner=None,
             return ws.run(rhs, config, normal_args=obj.normal_args(rhs.dtype, damping), preconditioner=preconditioner)
         if kind == "schur" and rhs.dtype == obj.linear.vec_dtype:
             ws = DevicePCG(rhs.numel(), rhs.dtype, rhs.device)
-            return ws.run(rhs, config, schur_args=obj.args, preconditioner=preconditioner)
+            return ws.run(rhs, config, schur_args=obj.args, preconditioner=preconditioner, error_word=obj.plan.err)
     return _generic_pcg(matvec, rhs, preconditioner, config)
 
 
@@ -624,7 +629,8 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                             summary.linear_relative_residual_history.append(None)
                         else:
                             pre = system.preconditioner() if cg.preconditioner else None
-                            res = pcg_ws.run(rhs, cg, schur_args=system.args, preconditioner=pre)
+                            res = pcg_ws.run(rhs, cg, schur_args=system.args, preconditioner=pre,
+                                             error_word=schur_plan.err)
                             retained, its, conv = res.solution, res.iterations, res.converged
                             usable = res.reason in ("residual_tolerance", "max_iterations") and _finite(retained)
                             summary.linear_restarts += res.restarts
