@@ -187,6 +187,19 @@ TLS_API int tls_jacobian_matvec(const tls_normal_args* args, const void* x, void
 TLS_API int tls_squared_matvec_norm(const tls_normal_args* args, const double* x, double* partials,
                             double* out, tls_stream_t stream);
 
+/* The same |J diag(s) x|^2 for callers that cannot allocate device memory
+ * where they need it (inside another framework's memory pool, a binding with
+ * no device allocator, a loop where an allocation may block): the block
+ * partials live in a 512 KB array inside this library, held on every GPU
+ * that loads it until the process exits. No counterpart in the reference.
+ * Limit: at most 8,388,608 factors per factor group (65,536 blocks of 128);
+ * larger inputs return TLS_ERR_INVALID before any work. The first call on a
+ * device looks up the array's device address (make that device current and
+ * make the first call before any stream capture). Calls share the array:
+ * calls that overlap on the GPU race. Allocates nothing. */
+TLS_API int tls_squared_matvec_norm_static(const tls_normal_args* args, const double* x, double* out,
+                                   tls_stream_t stream);
+
 /* J^T u (times diag(s) when scale is set) for u in factor-major row layout,
  * through the contribution workspace; replaces sparse.py:43-55 rmatvec. */
 TLS_API int tls_jacobian_rmatvec(const tls_normal_args* args, const void* rows, void* out, tls_stream_t stream);

@@ -109,6 +109,7 @@ _SIGNATURES = {
     "tls_normal_matvec": [C.POINTER(NormalArgs), vp, vp, vp],
     "tls_jacobian_matvec": [C.POINTER(NormalArgs), vp, vp, vp],
     "tls_squared_matvec_norm": [C.POINTER(NormalArgs), vp, vp, vp, vp],
+    "tls_squared_matvec_norm_static": [C.POINTER(NormalArgs), vp, vp, vp],
     "tls_jacobian_rmatvec": [C.POINTER(NormalArgs), vp, vp, vp],
     "tls_block_cholesky": [C.POINTER(BlockGroup), i32, f64, vp, vp],
     "tls_block_solve": [C.POINTER(BlockGroup), i32, vp, vp, i32, vp],

@@ -6,6 +6,8 @@
 // J, coalesced contribution stores); a second pass sums each variable's
 // contributions in a fixed list order. No atomics: results are bitwise
 // reproducible run to run.
+#include <mutex>
+
 #include "common.cuh"
 #include "pcg_state.cuh"
 
@@ -397,4 +399,71 @@ extern "C" int tls_jacobian_rmatvec(const tls_normal_args* a, const void* rows, 
   tls_normal_args b = *a;
   b.damping = 0.0;
   return tls_normal_gather(&b, nullptr, out, nullptr, nullptr, nullptr, st);
+}
+
+// ---------------------------------------------------------------- |J x|^2 without caller scratch
+// Some callers cannot allocate device memory at the point where they need
+// this norm: code running inside another framework's allocator or memory
+// pool, a host language binding with no device allocator of its own, or a
+// real-time loop where an allocation may block. For them the block partials
+// live in one file-scope array instead of a caller-supplied buffer. Every GPU
+// that loads this library holds the array (512 KB) until the process exits.
+// Each call rewrites exactly the partials it then sums, so nothing has to be
+// cleared between calls; but every call on a device shares the one array, so
+// calls whose kernels overlap on the GPU (different streams without ordering)
+// race and may return wrong sums.
+constexpr int kStaticSqnormPartials = 65536;  // one double per 128-factor block
+static __device__ __align__(256) double g_sqnorm_scratch[kStaticSqnormPartials];
+
+namespace {
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_addr[kMaxScratchDevices] = {};
+
+// Device address of g_sqnorm_scratch on the current device. The symbol name
+// in host code is only a host-side stand-in; kernels must get this address.
+int static_scratch(double** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return tls_set_error(TLS_ERR_CUDA, "cudaGetDevice failed");
+  if (dev < 0 || dev >= kMaxScratchDevices) return tls_set_error(TLS_ERR_UNSUPPORTED, "device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sqnorm_scratch);
+    if (e != cudaSuccess || !p) return tls_set_error(TLS_ERR_CUDA, cudaGetErrorString(e));
+    g_scratch_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_addr[dev];
+  return TLS_OK;
+}
+}  // namespace
+
+extern "C" int tls_squared_matvec_norm_static(const tls_normal_args* a, const double* x, double* out,
+                                              tls_stream_t stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    if ((a->fg[k].count + 127) / 128 > kStaticSqnormPartials)
+      return tls_set_error(TLS_ERR_INVALID,
+                           "tls_squared_matvec_norm_static: a factor group has more than 8,388,608 factors "
+                           "(65,536 blocks of 128); use tls_squared_matvec_norm with a caller buffer");
+  }
+  double* partials = nullptr;
+  int rc = static_scratch(&partials);
+  if (rc) return rc;
+  bool first = true;
+  for (int k = 0; k < a->nfactor_groups; ++k) {
+    const tls_factor_group& fg = a->fg[k];
+    if (fg.count == 0) continue;
+    FactorPass p = make_pass(fg, a->vg);
+    const int blocks = (int)((fg.count + 127) / 128);
+    rc = fg.jac_dtype == TLS_F64
+             ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, nullptr, partials, st)
+             : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, nullptr, partials, st);
+    if (rc) return rc;
+    sum_partials_kernel<<<1, 256, 0, st>>>(partials, blocks, out, first ? 0 : 1);
+    TLS_CHECK_LAUNCH();
+    first = false;
+  }
+  if (first) cudaMemsetAsync(out, 0, sizeof(double), st);
+  return TLS_OK;
 }
