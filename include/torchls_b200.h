@@ -300,7 +300,8 @@ struct tls_schur_args {
   int32_t nelim;                /* eliminated variables */
   int32_t wdtype;               /* TLS_F32 / TLS_F64 storage of W */
   int32_t vec_dtype;            /* reduced vectors (float64) */
-  int32_t cap;                  /* edges per chunk slab: 512 (float32 W) or 256 (float64 W) */
+  int32_t cap;                  /* edges per chunk slab: 512 (float32 W) or 256 (float64 W); runs of
+                                   equal retained variable never cross a 32 * cap / 256 edge window */
   int32_t meta_ints;            /* int32 words per chunk metadata slab: 5 * cap + 8 */
   int32_t nruns;
   int32_t pad_;

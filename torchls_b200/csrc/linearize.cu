@@ -23,6 +23,7 @@ struct LinParams {
   int32_t elim_mask;                  // bitmask of eliminated slots
   int32_t elim_dim;
   int32_t cross_width;
+  int32_t stage_w;                    // doubles per lane in the shared-memory output stage
   int8_t col_slot[32];                // slot of each column, -1 past D
   const int32_t* index[TLS_MAX_SLOTS];
   const double* packed_residual;
@@ -171,13 +172,41 @@ __device__ __forceinline__ void evaluate(const LinParams& p, int64_t f, double (
   }
 }
 
+// The warp's factors are consecutive, so its rows of a factor-major [N][width]
+// output form one contiguous range: each lane writes its row into the warp's
+// shared-memory buffer, then the warp stores the range with coalesced stores.
+__device__ __forceinline__ void warp_flush(const double* buf, int width, double* dst, int64_t f0, int nvalid) {
+  __syncwarp();
+  const int total = nvalid * width;
+  double* d = dst + f0 * width;
+  for (int i = threadIdx.x & 31; i < total; i += 32) d[i] = buf[i];
+  __syncwarp();
+}
+
 template <int RM, int DM, int KIND, bool CAM, bool PT, bool ALIAS, typename TJ>
 __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
-  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= p.n) return;
+  extern __shared__ double lin_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t f0 = (int64_t)blockIdx.x * blockDim.x + warp * 32;
+  if (f0 >= p.n) return;  // whole warp past the end
+  const int nvalid = (int)((p.n - f0) < 32 ? (p.n - f0) : 32);
+  const int64_t f = f0 + lane;
+  const bool live = lane < nvalid;
+  // per-warp stage: lane rows of the width being flushed, contiguous
+  double* buf = lin_smem + (size_t)warp * 32 * p.stage_w;
+  double* row = buf + lane * p.rdim;
   double r[RM];
   double J[RM][DM];
-  evaluate<RM, DM, KIND, CAM, PT>(p, f, r, J);
+  if (live) {
+    evaluate<RM, DM, KIND, CAM, PT>(p, f, r, J);
+  } else {
+#pragma unroll
+    for (int i = 0; i < RM; ++i) {
+      r[i] = 0.0;
+#pragma unroll
+      for (int c = 0; c < DM; ++c) J[i][c] = 0.0;
+    }
+  }
   const int R = p.rdim;
 
   double s = 0.0;
@@ -187,13 +216,14 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
   if (p.raw_residual) {
 #pragma unroll
     for (int i = 0; i < RM; ++i)
-      if (i < R) p.raw_residual[f * R + i] = r[i];
+      if (i < R) row[i] = r[i];
+    warp_flush(buf, R, p.raw_residual, f0, nvalid);
   }
-  if (p.squared_norm) p.squared_norm[f] = s;
+  if (p.squared_norm && live) p.squared_norm[f] = s;
 
   // --- robust loss / weights (problem-level has_loss, problem.py:264-270)
   double wscale = 1.0, rscale = 1.0, corr = 0.0, obj = s;
-  if (p.has_loss) {
+  if (p.has_loss && live) {
     if (p.loss_kind == TLS_LOSS_HUBER) {
       const double dl = p.delta;
       const double tiny = 2.2250738585072014e-308;
@@ -223,7 +253,7 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
       obj *= w;
     }
     if (p.objective && p.loss_kind != TLS_LOSS_GENERIC) p.objective[f] = obj;
-  } else if (p.objective) {
+  } else if (p.objective && live && !p.has_loss) {
     p.objective[f] = s;
   }
 
@@ -231,7 +261,8 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
     if (p.residual) {
 #pragma unroll
       for (int i = 0; i < RM; ++i)
-        if (i < R) p.residual[f * R + i] = r[i] * rscale;
+        if (i < R) row[i] = r[i] * rscale;
+      warp_flush(buf, R, p.residual, f0, nvalid);
     }
     return;
   }
@@ -258,12 +289,13 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
   if (p.residual) {
 #pragma unroll
     for (int i = 0; i < RM; ++i)
-      if (i < R) p.residual[f * R + i] = r[i];
+      if (i < R) row[i] = r[i];
+    warp_flush(buf, R, p.residual, f0, nvalid);
   }
 
-  // --- Jacobian store, SoA [r*D][N]
+  // --- Jacobian store, SoA [r*D][N] (already coalesced: factor index fastest)
   TJ* jac = reinterpret_cast<TJ*>(p.jac);
-  if (jac) {
+  if (jac && live) {
 #pragma unroll
     for (int i = 0; i < RM; ++i)
 #pragma unroll
@@ -272,17 +304,19 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
   }
   // --- gradient contributions J^T r (float64)
   if (p.grad) {
+    row = buf + lane * p.D;
 #pragma unroll
     for (int c = 0; c < DM; ++c) {
       double g = 0.0;
 #pragma unroll
       for (int i = 0; i < RM; ++i) g += J[i][c] * r[i];
-      if (c < p.D) p.grad[f * p.D + c] = g;
+      if (c < p.D) row[c] = g;
     }
+    warp_flush(buf, p.D, p.grad, f0, nvalid);
   }
   // --- Gram contributions per slot (packed upper), with aliased-slot cross terms
   if (p.gram) {
-    double* out = p.gram + f * p.W;
+    row = buf + lane * p.W;
 #pragma unroll
     for (int c1 = 0; c1 < DM; ++c1) {
 #pragma unroll
@@ -293,39 +327,42 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
 #pragma unroll
           for (int i = 0; i < RM; ++i) g += J[i][c1] * J[i][c2];
           const int a = c1 - p.slot_col[s1], b = c2 - p.slot_col[s1];
-          out[p.slot_gram[s1] + packed_index(a, b, p.slot_dim[s1])] = g;
+          row[p.slot_gram[s1] + packed_index(a, b, p.slot_dim[s1])] = g;
         }
       }
     }
     if constexpr (ALIAS) {
       // slot s1 > s2 of the same group and same variable: add J_s1^T J_s2 + J_s2^T J_s1
+      if (live) {
 #pragma unroll
-      for (int c1 = 0; c1 < DM; ++c1) {
+        for (int c1 = 0; c1 < DM; ++c1) {
 #pragma unroll
-        for (int c2 = 0; c2 < DM; ++c2) {
-          const int s1 = p.col_slot[c1], s2 = p.col_slot[c2];
-          if (s1 >= 0 && s2 >= 0 && s2 < s1 && p.slot_group[s1] == p.slot_group[s2] &&
-              p.index[s1][f] == p.index[s2][f]) {
-            double g = 0.0;
+          for (int c2 = 0; c2 < DM; ++c2) {
+            const int s1 = p.col_slot[c1], s2 = p.col_slot[c2];
+            if (s1 >= 0 && s2 >= 0 && s2 < s1 && p.slot_group[s1] == p.slot_group[s2] &&
+                p.index[s1][f] == p.index[s2][f]) {
+              double g = 0.0;
 #pragma unroll
-            for (int i = 0; i < RM; ++i) g += J[i][c1] * J[i][c2];
-            const int a = c1 - p.slot_col[s1], b = c2 - p.slot_col[s2];
-            const int lo = a < b ? a : b, hi = a < b ? b : a;
-            out[p.slot_gram[s1] + packed_index(lo, hi, p.slot_dim[s1])] += (a == b) ? 2.0 * g : g;
+              for (int i = 0; i < RM; ++i) g += J[i][c1] * J[i][c2];
+              const int a = c1 - p.slot_col[s1], b = c2 - p.slot_col[s2];
+              const int lo = a < b ? a : b, hi = a < b ? b : a;
+              row[p.slot_gram[s1] + packed_index(lo, hi, p.slot_dim[s1])] += (a == b) ? 2.0 * g : g;
+            }
           }
         }
       }
     }
+    warp_flush(buf, p.W, p.gram, f0, nvalid);
   }
   // --- Schur cross contributions: retained slot s -> J_s^T (sum of eliminated slots)
   if (p.cross) {
-    double* out = p.cross + f * p.cross_width;
+    row = buf + lane * p.cross_width;
+    for (int k = 0; k < p.cross_width; ++k) row[k] = 0.0;
 #pragma unroll
     for (int c1 = 0; c1 < DM; ++c1) {
       const int s1 = p.col_slot[c1];
       if (s1 < 0 || p.slot_cross[s1] < 0) continue;
       const int a = c1 - p.slot_col[s1];
-      for (int b = 0; b < p.elim_dim; ++b) out[p.slot_cross[s1] + a * p.elim_dim + b] = 0.0;
 #pragma unroll
       for (int c2 = 0; c2 < DM; ++c2) {
         const int s2 = p.col_slot[c2];
@@ -333,10 +370,11 @@ __global__ void __launch_bounds__(128) linearize_kernel(const LinParams p) {
           double g = 0.0;
 #pragma unroll
           for (int i = 0; i < RM; ++i) g += J[i][c1] * J[i][c2];
-          out[p.slot_cross[s1] + a * p.elim_dim + (c2 - p.slot_col[s2])] += g;
+          row[p.slot_cross[s1] + a * p.elim_dim + (c2 - p.slot_col[s2])] += g;
         }
       }
     }
+    warp_flush(buf, p.cross_width, p.cross, f0, nvalid);
   }
 }
 
@@ -345,10 +383,16 @@ static int launch_lin(const LinParams& p, int jac_dtype, cudaStream_t st) {
   const int block = 128;
   const int64_t grid = (p.n + block - 1) / block;
   if (p.n == 0) return TLS_OK;
-  if (jac_dtype == TLS_F32)
-    linearize_kernel<RM, DM, KIND, CAM, PT, ALIAS, float><<<grid, block, 0, st>>>(p);
-  else
-    linearize_kernel<RM, DM, KIND, CAM, PT, ALIAS, double><<<grid, block, 0, st>>>(p);
+  const int smem = block * p.stage_w * (int)sizeof(double);
+  if (jac_dtype == TLS_F32) {
+    auto k = linearize_kernel<RM, DM, KIND, CAM, PT, ALIAS, float>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k<<<grid, block, smem, st>>>(p);
+  } else {
+    auto k = linearize_kernel<RM, DM, KIND, CAM, PT, ALIAS, double>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k<<<grid, block, smem, st>>>(p);
+  }
   TLS_CHECK_LAUNCH();
   return TLS_OK;
 }
@@ -410,6 +454,12 @@ extern "C" int tls_linearize(const tls_linearize_args* a, tls_stream_t stream) {
       if (fg.slot_group[o] == fg.slot_group[s]) alias = true;
   }
   p.W = W;
+  {
+    int sw = fg.rdim > fg.total_dim ? fg.rdim : fg.total_dim;
+    if (W > sw) sw = W;
+    if (cross && cross_width > sw) sw = cross_width;
+    p.stage_w = sw < 1 ? 1 : sw;
+  }
   p.elim_mask = elim_mask;
   p.elim_dim = elim_dim;
   p.cross_width = cross_width;

@@ -49,23 +49,30 @@ __device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
 }
 
 // z = (L L^T)^-1 r for one block of runtime size dim <= D (registers only).
+// The lower triangle is loaded into registers first (independent loads, one
+// memory latency), then the two substitutions run from registers.
 template <int D>
 __device__ __forceinline__ void solve_block(const double* __restrict__ L, int dim, const double (&r)[D],
                                             double (&z)[D]) {
+  double l[D * (D + 1) / 2];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int k = 0; k <= i; ++k) l[i * (i + 1) / 2 + k] = (i < dim) ? __ldg(L + i * dim + k) : 1.0;
   double y[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     double t = r[i];
 #pragma unroll
-    for (int k = 0; k < i; ++k) t -= (i < dim) ? L[i * dim + k] * y[k] : 0.0;
-    y[i] = (i < dim) ? t / L[i * dim + i] : 0.0;
+    for (int k = 0; k < i; ++k) t -= (i < dim) ? l[i * (i + 1) / 2 + k] * y[k] : 0.0;
+    y[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
   }
 #pragma unroll
   for (int i = D - 1; i >= 0; --i) {
     double t = y[i];
 #pragma unroll
-    for (int k = i + 1; k < D; ++k) t -= (k < dim) ? L[k * dim + i] * z[k] : 0.0;
-    z[i] = (i < dim) ? t / L[i * dim + i] : 0.0;
+    for (int k = i + 1; k < D; ++k) t -= (k < dim) ? l[k * (k + 1) / 2 + i] * z[k] : 0.0;
+    z[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
   }
 }
 
@@ -276,6 +283,102 @@ __device__ void pcg_decide(PcgState* st, double s0, double s1, double s2) {
 }
 
 // ---------------------------------------------------------------- update
+// One PCG step's vector work on blocks [b0, nblocks) with stride `step`:
+// ITER: x += alpha p, r -= alpha Ap, z = M r; sums r.r, r.z.
+// CHECK/FINAL: ap holds A x; true residual tr = rhs - A x (into ap), ztrue = M tr;
+// sums tr.tr, (tr - r).(tr - r), tr.ztrue.
+template <int D, typename TV>
+__device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nblocks, int64_t b0, int64_t step,
+                                                  int mode, double alpha, const TV* __restrict__ rhs, TV* x, TV* r,
+                                                  TV* z, const TV* p, TV* ap, TV* ztrue, double& a0, double& a1,
+                                                  double& a2) {
+  for (int64_t b = b0; b < nblocks; b += step) {
+    const int gi = find_group(bs, b);
+    const int64_t i = b - bs.block_begin[gi];
+    const tls_block_group& g = bs.g[gi];
+    const int dim = g.dim;
+    int64_t cols[D];
+    block_cols<D>(g, i, cols);
+    double rb[D], zb[D];
+    if (mode == M_ITER) {
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        rb[k] = 0.0;
+        if (k < dim) {
+          const int64_t col = cols[k];
+          x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(p[col]));
+          const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
+          r[col] = rn;
+          rb[k] = to_d(rn);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        rb[k] = 0.0;
+        if (k < dim) {
+          const int64_t col = cols[k];
+          const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
+          ap[col] = tr;
+          const double t = to_d(tr);
+          rb[k] = t;
+          a0 += t * t;
+          const double dr = t - to_d(r[col]);
+          a1 += dr * dr;
+        }
+      }
+    }
+    if (mode == M_FINAL) continue;
+    if (bs.identity || g.factor == nullptr) {
+#pragma unroll
+      for (int k = 0; k < D; ++k) zb[k] = rb[k];
+    } else {
+      solve_block<D>(g.factor + i * dim * dim, dim, rb, zb);
+    }
+    TV* zdst = (mode == M_ITER) ? z : ztrue;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      if (k < dim) {
+        const TV zk = static_cast<TV>(zb[k]);
+        zdst[cols[k]] = zk;
+        const double zd = to_d(zk);
+        if (mode == M_ITER) {
+          a0 += rb[k] * rb[k];
+          a1 += rb[k] * zd;
+        } else {
+          a2 += rb[k] * zd;
+        }
+      }
+    }
+  }
+}
+
+// Direction / restart / swap for elements [i0, n) with stride `step`.
+template <typename TV>
+__device__ __forceinline__ void pcg_direction_elems(int64_t n, int64_t i0, int64_t step, int action, double beta,
+                                                    bool to_final, const TV* x, TV* r, const TV* z, TV* p, TV* psave,
+                                                    const TV* ap, const TV* ztrue) {
+  for (int64_t i = i0; i < n; i += step) {
+    switch (action) {
+      case A_DIR:
+        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(p[i]));
+        break;
+      case A_RESTART:
+        r[i] = ap[i];
+        p[i] = ztrue[i];
+        break;
+      case A_RESTORE_DIR:
+        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(psave[i]));
+        break;
+      case A_SWAP_TO_X:
+        psave[i] = p[i];
+        p[i] = x[i];
+        break;
+    }
+    if (to_final) p[i] = x[i];
+  }
+}
+
 template <int D, typename TV>
 __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, int64_t nblocks, PcgState* st,
                                                                  const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
@@ -292,69 +395,9 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, in
     if (!st->alpha_ok) work = false;
     else alpha = c.alpha;
   }
-  if (work) {
-    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks;
-         b += (int64_t)gridDim.x * blockDim.x) {
-      const int gi = find_group(bs, b);
-      const int64_t i = b - bs.block_begin[gi];
-      const tls_block_group& g = bs.g[gi];
-      const int dim = g.dim;
-      int64_t cols[D];
-      block_cols<D>(g, i, cols);
-      double rb[D], zb[D];
-      if (mode == M_ITER) {
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-          rb[k] = 0.0;
-          if (k < dim) {
-            const int64_t col = cols[k];
-            x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(p[col]));
-            const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
-            r[col] = rn;
-            rb[k] = to_d(rn);
-          }
-        }
-      } else {
-        // ap holds A x: true residual tr = rhs - A x (stored into ap)
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-          rb[k] = 0.0;
-          if (k < dim) {
-            const int64_t col = cols[k];
-            const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
-            ap[col] = tr;
-            const double t = to_d(tr);
-            rb[k] = t;
-            a0 += t * t;
-            const double dr = t - to_d(r[col]);
-            a1 += dr * dr;
-          }
-        }
-      }
-      if (mode == M_FINAL) continue;
-      if (bs.identity || g.factor == nullptr) {
-#pragma unroll
-        for (int k = 0; k < D; ++k) zb[k] = rb[k];
-      } else {
-        solve_block<D>(g.factor + i * dim * dim, dim, rb, zb);
-      }
-      TV* zdst = (mode == M_ITER) ? z : ztrue;
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        if (k < dim) {
-          const TV zk = static_cast<TV>(zb[k]);
-          zdst[cols[k]] = zk;
-          const double zd = to_d(zk);
-          if (mode == M_ITER) {
-            a0 += rb[k] * rb[k];
-            a1 += rb[k] * zd;
-          } else {
-            a2 += rb[k] * zd;
-          }
-        }
-      }
-    }
-  }
+  if (work)
+    pcg_update_blocks<D, TV>(bs, nblocks, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                             (int64_t)gridDim.x * blockDim.x, mode, alpha, rhs, x, r, z, p, ap, ztrue, a0, a1, a2);
   double* up = partials + kOpPartials;
   const double s0 = block_sum<kUpdThreads>(a0, sm);
   const double s1 = block_sum<kUpdThreads>(a1, sm);
@@ -389,27 +432,50 @@ __global__ void __launch_bounds__(256) pcg_direction_kernel(int64_t n, const Pcg
                                                             const TV* ztrue) {
   const int action = st->action;
   if (action == A_NONE) return;
-  const double beta = st->pub.beta;
   const bool to_final = st->pub.mode == M_FINAL && action != A_SWAP_TO_X;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    switch (action) {
-      case A_DIR:
-        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(p[i]));
-        break;
-      case A_RESTART:
-        r[i] = ap[i];
-        p[i] = ztrue[i];
-        break;
-      case A_RESTORE_DIR:
-        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(psave[i]));
-        break;
-      case A_SWAP_TO_X:
-        psave[i] = p[i];
-        p[i] = x[i];
-        break;
-    }
-    if (to_final) p[i] = x[i];
+  pcg_direction_elems<TV>(n, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x,
+                          action, st->pub.beta, to_final, x, r, z, p, psave, ap, ztrue);
+}
+
+// Small systems (few preconditioner blocks): the whole post-operator part of a
+// PCG step in ONE block -- update, preconditioner, dot products, decision and
+// direction -- without grid-wide atomics or a second launch.
+constexpr int kSmallThreads = 512;
+constexpr int64_t kSmallMaxBlocks = 8192;
+
+template <int D, typename TV>
+__global__ void __launch_bounds__(kSmallThreads) pcg_step_small_kernel(BlockSet bs, int64_t nblocks, int64_t n,
+                                                                       PcgState* st, const TV* __restrict__ rhs,
+                                                                       TV* x, TV* r, TV* z, TV* p, TV* psave, TV* ap,
+                                                                       TV* ztrue) {
+  __shared__ double sm[kSmallThreads / 32];
+  __shared__ int s_action, s_tofinal;
+  __shared__ double s_beta;
+  const tls_pcg_control& c = st->pub;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  const int mode = c.mode;
+  bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
+  double alpha = 0.0;
+  if (work && mode == M_ITER) {
+    if (!st->alpha_ok) work = false;
+    else alpha = c.alpha;
   }
+  if (work)
+    pcg_update_blocks<D, TV>(bs, nblocks, threadIdx.x, kSmallThreads, mode, alpha, rhs, x, r, z, p, ap, ztrue, a0,
+                             a1, a2);
+  const double t0 = block_sum<kSmallThreads>(a0, sm);
+  const double t1 = block_sum<kSmallThreads>(a1, sm);
+  const double t2 = block_sum<kSmallThreads>(a2, sm);
+  if (threadIdx.x == 0) {
+    pcg_decide(st, t0, t1, t2);
+    s_action = st->action;
+    s_beta = st->pub.beta;
+    s_tofinal = st->pub.mode == M_FINAL && st->action != A_SWAP_TO_X;
+  }
+  __syncthreads();
+  if (s_action == A_NONE) return;
+  pcg_direction_elems<TV>(n, threadIdx.x, kSmallThreads, s_action, s_beta, s_tofinal != 0, x, r, z, p, psave, ap,
+                          ztrue);
 }
 
 __host__ BlockSet make_blocks(const tls_pcg_args* a, int64_t* total, int* maxdim) {
@@ -517,6 +583,13 @@ static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
         rc = tls_schur_apply(a->schur, a->p, a->ap, a->partials, &launched, st, s);
       if (rc) return rc;
       if (launched != op_blocks) return tls_set_error(TLS_ERR_INVALID, "operator block count changed");
+      if (nb <= kSmallMaxBlocks) {
+        pcg_step_small_kernel<D, TV><<<1, kSmallThreads, 0, s>>>(bs, nb, a->n, st, (const TV*)a->rhs, (TV*)a->x,
+                                                                 (TV*)a->r, (TV*)a->z, (TV*)a->p, (TV*)a->psave,
+                                                                 (TV*)a->ap, (TV*)a->ztrue);
+        TLS_CHECK_LAUNCH();
+        continue;
+      }
       pcg_update_kernel<D, TV><<<gb, kUpdThreads, 0, s>>>(bs, nb, st, (const TV*)a->rhs, (TV*)a->x, (TV*)a->r,
                                                           (TV*)a->z, (const TV*)a->p, (TV*)a->ap, (TV*)a->ztrue,
                                                           a->partials);

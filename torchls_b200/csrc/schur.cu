@@ -10,9 +10,13 @@
 //   on an mbarrier; two stages, so chunk c+grid loads while chunk c computes.
 //     phase 1   t_e = W_e^T x_i                 (per edge, into shared memory)
 //     phase 1.5 y_p = sum_{e in p} t_e          (per eliminated variable, fixed order)
-//     phase 2   u_e = W_e y_p; warp-segmented inclusive scan over runs of
-//               equal retained variable (runs never cross a 32-edge window);
-//               the run's last lane stores the run partial, retained-major.
+//     phase 2   u_e = W_e y_p; each thread takes cap/256 consecutive edges,
+//               sums runs of equal retained variable sequentially, then a
+//               warp-segmented inclusive scan joins runs across lanes (runs
+//               never cross one warp's window); the run's tail stores the
+//               run partial, retained-major.
+//   Products and sums are float64 (W stored as float32 or float64). x is
+//   staged in shared memory when it fits next to the two slab stages.
 //   gather kernel (one block per retained variable) sums its contiguous run
 //   partials in a fixed order and adds the diagonal term; its last block
 //   finalises the PCG curvature.
@@ -83,24 +87,74 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity
   }
 }
 
-template <int DR, int DE, int CAP, typename TW>
+template <int DR, int DE, int CAP, typename TW, typename TA>
 struct SlabShape {
   static constexpr int kWBytes = DR * DE * CAP * (int)sizeof(TW);
   static constexpr int kMetaInts = 5 * CAP + 8;
   static constexpr int kMetaBytes = kMetaInts * 4;
   static constexpr int kStageBytes = kWBytes + kMetaBytes;
-  static constexpr int kTBytes = CAP * DE * (int)sizeof(double);
-  static constexpr int kSmemBytes = 2 * kStageBytes + kTBytes;
+  static constexpr int kTBytes = CAP * 4 * (int)sizeof(TA);  // [CAP][4] per-edge / per-variable 3-vectors
+  static constexpr int kBaseSmem = 2 * kStageBytes + kTBytes;
+  static constexpr int kEpt = CAP / kChunkThreads;  // consecutive edges per thread
   static_assert(kWBytes % 16 == 0 && kMetaBytes % 16 == 0, "slabs must be 16-byte multiples");
+  static_assert(kEpt == 1 || kEpt == 2 || kEpt == 4, "edges per thread");
+  static_assert(DE <= 4, "eliminated blocks up to 4 wide");
 };
 
+// EPT consecutive shared-memory values starting at p (p aligned to EPT values).
+template <int EPT, typename T>
+__device__ __forceinline__ void lds_vec(const T* p, T (&v)[EPT]) {
+  if constexpr (EPT == 1) {
+    v[0] = p[0];
+  } else if constexpr (EPT == 2 && sizeof(T) == 4) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    v[0] = q.x, v[1] = q.y;
+  } else if constexpr (EPT == 2 && sizeof(T) == 8) {
+    const double2 q = *reinterpret_cast<const double2*>(p);
+    v[0] = q.x, v[1] = q.y;
+  } else if constexpr (EPT == 4 && sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) v[j] = p[j];
+  }
+}
+
+template <typename TA>
+__device__ __forceinline__ void lds4(const TA* p, TA (&v)[4]) {
+  if constexpr (sizeof(TA) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+  } else {
+    const double2 q0 = reinterpret_cast<const double2*>(p)[0], q1 = reinterpret_cast<const double2*>(p)[1];
+    v[0] = q0.x, v[1] = q0.y, v[2] = q1.x, v[3] = q1.y;
+  }
+}
+
+template <typename TA>
+__device__ __forceinline__ void sts4(TA* p, const TA (&v)[4]) {
+  if constexpr (sizeof(TA) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+  }
+}
+
 // MODE 0: S x partials (phase 1 from x); MODE 1: reduced rhs (y_p = a.ybuf[p]).
-template <int DR, int DE, int CAP, int MODE, typename TW>
+// TA: arithmetic type of the per-edge products and of the run sums (float64:
+// S = U - W W^T cancels heavily, and float32 products stalled CG); W is
+// stored as TW. Per-variable sums y_p and every sum across runs are float64.
+// XS: the reduced vector x is staged in shared memory (as TA) at kernel start.
+template <int DR, int DE, int CAP, int MODE, typename TW, typename TA, bool XS>
 __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
-  using S = SlabShape<DR, DE, CAP, TW>;
+  using S = SlabShape<DR, DE, CAP, TW, TA>;
+  constexpr int EPT = S::kEpt;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
-  double* t_s = reinterpret_cast<double*>(smem + 2 * S::kStageBytes);  // [CAP][DE], reused for y
+  TA* t_s = reinterpret_cast<TA*>(smem + 2 * S::kStageBytes);  // [CAP][4]: t_e, then y_p
+  TA* x_s = reinterpret_cast<TA*>(smem + S::kBaseSmem);         // [nretained*DR] when XS
   const int tid = threadIdx.x, lane = tid & 31;
   const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
   const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
@@ -118,6 +172,11 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &bar[stg]);
   };
   if (tid == 0 && (int)blockIdx.x < a.nchunks) issue(blockIdx.x, 0);
+  if constexpr (XS && MODE == 0) {
+    const int nx = a.nretained * DR;
+    for (int j = tid; j < nx; j += kChunkThreads) x_s[j] = static_cast<TA>(__ldg(x + j));
+    __syncthreads();
+  }
   int it = 0;
   for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x, ++it) {
     const int stg = it & 1;
@@ -131,24 +190,36 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     const int32_t* tpos = Ms + kMetaHead + 2 * CAP;
     const int32_t* pp = Ms + kMetaHead + 3 * CAP;
     const int32_t* pe = Ms + 2 * kMetaHead + 4 * CAP;
-    // ---- phase 1: t_e = W_e^T x_i
+    const int le0 = tid * EPT;  // this thread's first edge
+    // ---- phase 1: t_e = W_e^T x_i (TA products)
     if constexpr (MODE == 0) {
-      for (int le = tid; le < ne; le += kChunkThreads) {
-        const int64_t i = er[le];
-        double xr[DR];
+      if (le0 < ne) {
+        TW w[DR * DE][EPT];
 #pragma unroll
-        for (int k = 0; k < DR; ++k) xr[k] = __ldg(x + i * DR + k);
+        for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
 #pragma unroll
-        for (int b = 0; b < DE; ++b) {
-          double acc = 0.0;
+        for (int j = 0; j < EPT; ++j) {
+          if (le0 + j < ne) {
+            const int i = er[le0 + j];
+            TA xr[DR];
 #pragma unroll
-          for (int k = 0; k < DR; ++k) acc += static_cast<double>(Ws[(k * DE + b) * CAP + le]) * xr[k];
-          t_s[le * DE + b] = acc;
+            for (int k = 0; k < DR; ++k) {
+              if constexpr (XS) xr[k] = x_s[i * DR + k];
+              else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
+            }
+            TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
+#pragma unroll
+            for (int b = 0; b < DE; ++b) {
+#pragma unroll
+              for (int k = 0; k < DR; ++k) t[b] = fma(static_cast<TA>(w[k * DE + b][j]), xr[k], t[b]);
+            }
+            sts4(t_s + (le0 + j) * 4, t);
+          }
         }
       }
       __syncthreads();
     }
-    // ---- phase 1.5: y_p per eliminated variable (<= CAP / 256 per thread), then overwrite t_s
+    // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges), then overwrite t_s
     constexpr int PPT = CAP / kChunkThreads;
     double yreg[PPT][DE];
 #pragma unroll
@@ -158,10 +229,20 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
       for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
       if (pl < np) {
         if constexpr (MODE == 0) {
-          for (int j = pp[pl]; j < pp[pl + 1]; ++j) {
-            const int lj = pe[j];
+          // four edges per round: independent shared-memory loads, fixed-order sums
+          const int jb = pp[pl], je = pp[pl + 1];
+          for (int j = jb; j < je; j += 4) {
+            TA t[4][4];
 #pragma unroll
-            for (int b = 0; b < DE; ++b) yreg[q][b] += t_s[lj * DE + b];
+            for (int u = 0; u < 4; ++u) {
+              if (j + u < je) lds4(t_s + pe[j + u] * 4, t[u]);
+              else t[u][0] = t[u][1] = t[u][2] = t[u][3] = TA(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int b = 0; b < DE; ++b)
+                if (j + u < je) yreg[q][b] += static_cast<double>(t[u][b]);
           }
         } else {
           const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + pe[pp[pl]]);
@@ -175,61 +256,105 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     for (int q = 0; q < PPT; ++q) {
       const int pl = tid + q * kChunkThreads;
       if (pl < np) {
+        TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
 #pragma unroll
-        for (int b = 0; b < DE; ++b) t_s[pl * DE + b] = yreg[q][b];
+        for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[q][b]);
+        sts4(t_s + pl * 4, y);
       }
     }
     __syncthreads();
-    // ---- phase 2: u_e = W_e y_p, warp-segmented run sums
-    for (int base = 0; base < ne; base += kChunkThreads) {
-      const int le = base + tid;
-      const bool valid = le < ne;
-      const uint32_t m = valid ? meta[le] : 0u;
-      const int pl = m & 0xFFFFu;
-      const int head = (m >> 16) & 31;
-      const bool tail = valid && ((m >> 21) & 1u);
-      double y[DE];
+    // ---- phase 2: u_e = W_e y_p; segmented sums over runs of equal retained
+    // variable (runs never cross a window of 32 * EPT edges): sequential within
+    // the thread, then a warp-segmented inclusive scan of the carries.
+    {
+      TA v[EPT][DR];
+      int head[EPT];
+      bool tail[EPT];
+      TW wv[DR * DE][EPT];
 #pragma unroll
-      for (int b = 0; b < DE; ++b) y[b] = valid ? t_s[pl * DE + b] : 0.0;
-      const int64_t pos = tail ? (int64_t)tpos[le] : 0;
+      for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, wv[kb]);
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        const int le = le0 + j;
+        const int pos = lane * EPT + j;  // position inside the 32*EPT-edge window
+        const bool valid = le < ne;
+        const uint32_t m = valid ? meta[le] : 0u;
+        head[j] = valid ? (int)((m >> 16) & 63u) : pos;
+        tail[j] = valid && ((m >> 22) & 1u);
+        TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
+        if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);
+        const bool cont = j > 0 && head[j] < pos;  // same run as edge j-1
+#pragma unroll
+        for (int k = 0; k < DR; ++k) {
+          TA u = TA(0);
+#pragma unroll
+          for (int b = 0; b < DE; ++b) u = fma(static_cast<TA>(wv[k * DE + b][j]), y[b], u);
+          v[j][k] = cont ? v[j > 0 ? j - 1 : 0][k] + u : u;
+        }
+      }
+      const int hl = head[EPT - 1] / EPT;           // lane holding the start of this thread's last run
+      const bool from_left = head[0] < lane * EPT;  // this thread's first run began in an earlier lane
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
-        double u = 0.0;
-        if (valid) {
-#pragma unroll
-          for (int b = 0; b < DE; ++b) u += static_cast<double>(Ws[(k * DE + b) * CAP + le]) * y[b];
-        }
+        TA cval = v[EPT - 1][k];
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-          const double v = __shfl_up_sync(0xffffffffu, u, off);
-          if (lane - off >= head) u += v;
+          const TA o = __shfl_up_sync(0xffffffffu, cval, off);
+          if (lane - off >= hl) cval += o;
         }
-        if (tail) a.run_partial[pos * DR + k] = u;
+        const TA prev = __shfl_up_sync(0xffffffffu, cval, 1);
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+          if (tail[j]) {
+            // only the thread's first run can have begun in an earlier lane
+            const TA tot = (from_left && head[j] == head[0]) ? v[j][k] + prev : v[j][k];
+            reinterpret_cast<TA*>(a.run_partial)[(int64_t)tpos[le0 + j] * DR + k] = tot;
+          }
+        }
       }
     }
     __syncthreads();
   }
 }
 
-// One block per retained variable: sum its contiguous run partials in a fixed
-// order, then
+// One block per retained variable: sum its contiguous run partials (float64,
+// fixed order), then
 // MODE 0: out = s U s x + lambda x - sum  (matvec; dot partial + PCG epilogue)
 // MODE 1: out = b_retained - sum          (reduced rhs, b float64 full vector)
-template <int DR, int MODE, typename TV>
+template <int DR, int MODE, typename TV, typename TP>
 __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, const TV* __restrict__ x,
                                                            const double* __restrict__ b, TV* __restrict__ out,
                                                            double* __restrict__ dot_partials, PcgState* pst) {
   __shared__ double sm[8][DR];
+  __shared__ double ux[DR * DR];
   __shared__ double smd[8];
   const int64_t i = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const TP* part = reinterpret_cast<const TP*>(a.run_partial);
+  if constexpr (MODE == 0) {
+    if (tid < DR * DR) {
+      const int l = tid % DR;
+      const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
+      ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * to_d(x[i * DR + l]));
+    }
+  }
   double acc[DR];
 #pragma unroll
   for (int k = 0; k < DR; ++k) acc[k] = 0.0;
   const int rb = __ldg(a.rrun_ptr + i), re = __ldg(a.rrun_ptr + i + 1);
-  for (int j = rb + tid; j < re; j += 256) {
+  // four runs per thread in flight per round; fixed order j, j+256, j+512, j+768
+  for (int j0 = rb + tid; j0 < re; j0 += 1024) {
+    TP v[4][DR];
 #pragma unroll
-    for (int k = 0; k < DR; ++k) acc[k] += a.run_partial[(int64_t)j * DR + k];
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + q * 256;
+#pragma unroll
+      for (int k = 0; k < DR; ++k) v[q][k] = j < re ? __ldcg(part + (int64_t)j * DR + k) : TP(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int k = 0; k < DR; ++k) acc[k] += static_cast<double>(v[q][k]);
   }
 #pragma unroll
   for (int k = 0; k < DR; ++k) {
@@ -237,39 +362,30 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
     if (lane == 0) sm[warp][k] = v;
   }
   __syncthreads();
-  if (tid == 0) {
-    double tot[DR];
+  if (warp == 0) {
+    double dot = 0.0;
+    if (lane < DR) {
+      const int k = lane;
+      double tot = 0.0;
 #pragma unroll
-    for (int k = 0; k < DR; ++k) {
-      double v = 0.0;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v += sm[q][k];
-      tot[k] = v;
-    }
-    if constexpr (MODE == 0) {
-      double xs[DR], xv[DR], s[DR];
-#pragma unroll
-      for (int k = 0; k < DR; ++k) {
-        xv[k] = to_d(x[i * DR + k]);
-        s[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
-        xs[k] = s[k] * xv[k];
-      }
-      const double* U = a.ret_diag + i * DR * DR;
-      double dot = 0.0;
-#pragma unroll
-      for (int k = 0; k < DR; ++k) {
+      for (int q = 0; q < 8; ++q) tot += sm[q][k];
+      if constexpr (MODE == 0) {
+        const double xv = to_d(x[i * DR + k]);
+        const double sk = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
         double v = 0.0;
 #pragma unroll
-        for (int l = 0; l < DR; ++l) v += U[k * DR + l] * xs[l];
-        v = s[k] * v + a.damping * xv[k] - tot[k];
+        for (int l = 0; l < DR; ++l) v += ux[k * DR + l];
+        v = sk * v + a.damping * xv - tot;
         const TV o = static_cast<TV>(v);
         out[i * DR + k] = o;
-        dot += xv[k] * to_d(o);
+        dot = xv * to_d(o);
+      } else {
+        out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - tot);
       }
-      if (dot_partials) dot_partials[i] = dot;
-    } else {
-#pragma unroll
-      for (int k = 0; k < DR; ++k) out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - tot[k]);
+    }
+    if constexpr (MODE == 0) {
+      dot = warp_sum(dot);
+      if (lane == 0 && dot_partials) dot_partials[i] = dot;
     }
   }
   if (MODE == 0 && pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
@@ -449,26 +565,40 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
 
 template <int DR, int DE>
 struct SchurOps {
-  template <int MODE, typename TW, int CAP>
-  static int chunks_cap(const tls_schur_args& a, const double* x, cudaStream_t s) {
-    using S = SlabShape<DR, DE, CAP, TW>;
-    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
-    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
-      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
-    auto k = schur_chunk_kernel<DR, DE, CAP, MODE, TW>;
-    static int grid_cap = 0;  // resident CTAs per SM x SMs, computed once per instantiation
-    if (grid_cap == 0) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes);
+  template <int MODE, typename TW, int CAP, bool XS>
+  static int launch_chunks(const tls_schur_args& a, const double* x, int smem, cudaStream_t s) {
+    auto k = schur_chunk_kernel<DR, DE, CAP, MODE, TW, double, XS>;
+    // resident CTAs per SM x SMs for the last shared-memory size, per instantiation
+    static int grid_cap = 0, grid_smem = -1;
+    if (grid_smem != smem) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       int per_sm = 0, dev = 0, sms = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, S::kSmemBytes);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
       grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+      grid_smem = smem;
     }
     const int grid = a.nchunks < grid_cap ? a.nchunks : grid_cap;
-    k<<<grid, kChunkThreads, S::kSmemBytes, s>>>(a, x);
+    k<<<grid, kChunkThreads, smem, s>>>(a, x);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
+  }
+  template <int MODE, typename TW, int CAP>
+  static int chunks_cap(const tls_schur_args& a, const double* x, cudaStream_t s) {
+    using S = SlabShape<DR, DE, CAP, TW, double>;
+    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
+    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
+      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
+    // Stage x in shared memory when two CTAs per SM still fit (228 KB per SM,
+    // 1 KB reserved per CTA, static barriers).
+    constexpr int kTwoCtaSmem = (233472 / 2) - 1024 - 64;
+    const int xbytes = ((a.nretained * DR * (int)sizeof(double)) + 15) & ~15;
+    if constexpr (MODE == 0) {
+      if (S::kBaseSmem + xbytes <= kTwoCtaSmem)
+        return launch_chunks<MODE, TW, CAP, true>(a, x, S::kBaseSmem + xbytes, s);
+    }
+    return launch_chunks<MODE, TW, CAP, false>(a, x, S::kBaseSmem, s);
   }
   template <int MODE, typename TW>
   static int chunks(const tls_schur_args& a, const double* x, cudaStream_t s) {
@@ -488,7 +618,8 @@ struct SchurOps {
     int rc = chunks<0, TW>(a, reinterpret_cast<const double*>(x), s);
     if (rc) return rc;
     if (gblocks) *gblocks = a.nretained;
-    if (a.nretained > 0) schur_gather_kernel<DR, 0, TV><<<a.nretained, 256, 0, s>>>(a, x, nullptr, out, dots, pst);
+    if (a.nretained > 0)
+      schur_gather_kernel<DR, 0, TV, double><<<a.nretained, 256, 0, s>>>(a, x, nullptr, out, dots, pst);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
@@ -499,7 +630,7 @@ struct SchurOps {
     int rc = chunks<1, TW>(a, nullptr, s);
     if (rc) return rc;
     if (a.nretained > 0)
-      schur_gather_kernel<DR, 1, TV><<<a.nretained, 256, 0, s>>>(a, nullptr, b, out, nullptr, nullptr);
+      schur_gather_kernel<DR, 1, TV, double><<<a.nretained, 256, 0, s>>>(a, nullptr, b, out, nullptr, nullptr);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }

@@ -127,8 +127,9 @@ class ChunkLayout:
     Eliminated variables are ordered by their smallest retained neighbour (so
     a chunk's edges touch few retained variables) and packed into chunks of
     whole variables with at most ``cap`` edges. Inside a chunk edges are
-    sorted by retained variable and cut into runs that never cross a 32-edge
-    window. Each chunk owns a fixed-size, 16-byte aligned slab: W as
+    sorted by retained variable and cut into runs that never cross a window of
+    32 * (cap // 256) edges (one warp's edges; each thread takes cap // 256
+    consecutive edges). Each chunk owns a fixed-size, 16-byte aligned slab: W as
     [dr*de][cap] and an int32 metadata block
         [ne, np, 0, 0][edge_r: cap][meta: cap][tail run position: cap]
         [point edge ptr: cap + 4][point edge list: cap]
@@ -168,15 +169,17 @@ class ChunkLayout:
         ne = np.diff(chunk_ptr)
         local = np.arange(E) - chunk_ptr[cid] if E else np.zeros(0, np.int64)
         sidx = cid * cap + local
-        # runs: equal retained variable, split at 32-edge windows
+        # runs: equal retained variable, split at warp windows
+        win = 32 * max(1, cap // self.THREADS)
+        self.window = win
         newrun = newchunk.copy()
         newrun[1:] |= c_r[1:] != c_r[:-1]
-        newrun |= (local % 32) == 0
+        newrun |= (local % win) == 0
         run_starts = np.flatnonzero(newrun)
         nruns = len(run_starts)
         run_id = np.cumsum(newrun) - 1
         run_end = np.concatenate((run_starts[1:], [E]))
-        head = (local[run_starts] % 32)[run_id] if E else np.zeros(0, np.int64)
+        head = (local[run_starts] % win)[run_id] if E else np.zeros(0, np.int64)
         run_r = c_r[run_starts]
         cm = np.argsort(run_r, kind="stable")  # retained-major position -> run id
         run_pos = np.empty(nruns, np.int64)
@@ -195,7 +198,8 @@ class ChunkLayout:
         cpt_ptr = np.searchsorted(cpt_chunk, np.arange(nchunks + 1))
         npts = np.diff(cpt_ptr)
         pl = cp_inv - cpt_ptr[cid] if E else np.zeros(0, np.int64)
-        meta = pl | (head << 16) | (tail.astype(np.int64) << 21)
+        # meta word: local variable (16 bits) | run start inside the window (6 bits) | run tail flag
+        meta = pl | (head << 16) | (tail.astype(np.int64) << 22)
         # ---- metadata slab
         self.meta_ints = 5 * cap + 8
         M = np.zeros((max(nchunks, 1), self.meta_ints), np.int64)
