@@ -273,9 +273,13 @@ typedef struct tls_pcg_args {
 TLS_API int tls_pcg_start(const tls_pcg_args* args, double rtol, double atol, int32_t max_iterations,
                   int32_t check_interval, int32_t periodic, double drift_tolerance, tls_stream_t stream);
 
-/* Run `steps` state-machine steps (each = one operator application plus its
- * vector updates); steps after termination leave x unchanged. Launches only:
- * a sequence of calls can be captured into a CUDA graph. */
+/* Run up to `steps` state-machine steps (each = one operator application plus
+ * its vector updates); steps after termination leave x unchanged. Launches
+ * only. Small Schur systems (float64 vectors, <= 8192 preconditioner blocks,
+ * retained/eliminated dims 6/3, 7/3 or 3/3) run all `steps` in ONE
+ * persistent cooperative kernel that stops at termination; otherwise each
+ * step is 2-3 kernels and at most 16 steps are enqueued per call (poll the
+ * control block and call again while it is active). */
 TLS_API int tls_pcg_run(const tls_pcg_args* args, int32_t steps, tls_stream_t stream);
 
 /* Size in bytes of the device control block (tls_pcg_control first). */

@@ -19,6 +19,7 @@
 
 #include "blocks.cuh"
 #include "common.cuh"
+#include "pcg_device.cuh"
 #include "pcg_state.cuh"
 
 int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
@@ -29,69 +30,11 @@ int tls_normal_gather_blocks(const tls_normal_args* a);
 
 namespace tls {
 
-struct BlockSet {
-  int32_t ngroups;
-  int32_t identity;                         // no preconditioner: unit blocks
-  int64_t block_begin[TLS_MAX_GROUPS + 1];  // prefix of block counts
-  tls_block_group g[TLS_MAX_GROUPS];
-};
-
 constexpr int kUpdThreads = 128;
 constexpr int kMaxUpdBlocks = 1024;
 // partials layout: [0, kOpPartials) operator dots; update partials at
 // kOpPartials + k * kMaxUpdBlocks (k = 0, 1, 2).
 constexpr int kOpPartials = 65536;
-
-__device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
-  int gi = 0;
-  while (gi + 1 < bs.ngroups && b >= bs.block_begin[gi + 1]) ++gi;
-  return gi;
-}
-
-// z = (L L^T)^-1 r for one block of runtime size dim <= D (registers only).
-// The lower triangle is loaded into registers first (independent loads, one
-// memory latency), then the two substitutions run from registers.
-template <int D>
-__device__ __forceinline__ void solve_block(const double* __restrict__ L, int dim, const double (&r)[D],
-                                            double (&z)[D]) {
-  double l[D * (D + 1) / 2];
-#pragma unroll
-  for (int i = 0; i < D; ++i)
-#pragma unroll
-    for (int k = 0; k <= i; ++k) l[i * (i + 1) / 2 + k] = (i < dim) ? __ldg(L + i * dim + k) : 1.0;
-  double y[D];
-#pragma unroll
-  for (int i = 0; i < D; ++i) {
-    double t = r[i];
-#pragma unroll
-    for (int k = 0; k < i; ++k) t -= (i < dim) ? l[i * (i + 1) / 2 + k] * y[k] : 0.0;
-    y[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
-  }
-#pragma unroll
-  for (int i = D - 1; i >= 0; --i) {
-    double t = y[i];
-#pragma unroll
-    for (int k = i + 1; k < D; ++k) t -= (k < dim) ? l[k * (k + 1) / 2 + i] * z[k] : 0.0;
-    z[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
-  }
-}
-
-template <int D>
-__device__ __forceinline__ void block_cols(const tls_block_group& g, int64_t i, int64_t (&cols)[D]) {
-  int m = 0, start = 0;
-#pragma unroll
-  for (int k = 0; k < D; ++k) {
-    if (k < g.dim) {
-      while (k >= start + g.member_dim[m]) {
-        start += g.member_dim[m];
-        ++m;
-      }
-      cols[k] = g.member_offset[m] + i * g.member_dim[m] + (k - start);
-    } else {
-      cols[k] = 0;
-    }
-  }
-}
 
 // ---------------------------------------------------------------- start
 template <typename TV>
@@ -139,6 +82,7 @@ __global__ void __launch_bounds__(256) pcg_init_finish_kernel(PcgState* st, cons
   st->alpha_ok = 0;
   st->ticket_op = 0;
   st->ticket_upd = 0;
+  st->bar_count = 0;
   if (!isfinite(nrm)) {
     c.status = TLS_PCG_NONFINITE;
     c.mode = M_DONE;
@@ -194,191 +138,7 @@ __global__ void pcg_rz_finish_kernel(PcgState* st, const double* partials, int b
   st->pub.rz = s;
 }
 
-// ---------------------------------------------------------------- decision (last update block)
-__device__ void pcg_decide(PcgState* st, double s0, double s1, double s2) {
-  tls_pcg_control& c = st->pub;
-  st->action = A_NONE;
-  if (c.status != TLS_PCG_ACTIVE || c.mode == M_DONE) return;
-  const double thr = c.threshold;
-  if (c.mode == M_ITER) {
-    const double curv = c.curvature;
-    const double rz = c.rz;
-    const int it = ++c.iterations;
-    if (!isfinite(curv) || !isfinite(rz)) {
-      st->pending = TLS_PCG_NONFINITE;
-      c.mode = M_FINAL;
-      st->action = A_SWAP_TO_X;
-      return;
-    }
-    if (curv <= 0.0 || rz <= 0.0) {
-      st->pending = TLS_PCG_NONPOSITIVE;
-      c.mode = M_FINAL;
-      st->action = A_SWAP_TO_X;
-      return;
-    }
-    c.rr = s0;
-    c.rz_new = s1;
-    const double rec = sqrt(s0);
-    st->rec = rec;
-    const bool periodic = c.check_interval > 0 && (it % c.check_interval) == 0;
-    st->rec_hit = rec <= thr;
-    st->periodic_hit = periodic;
-    if (rec <= thr || periodic) {
-      c.mode = M_CHECK;
-      st->action = A_SWAP_TO_X;
-      return;
-    }
-    if (it >= c.max_iterations) {
-      c.mode = M_FINAL;
-      st->action = A_SWAP_TO_X;
-      return;
-    }
-    c.beta = s1 / rz;
-    c.rz = s1;
-    c.mode = M_ITER;
-    st->action = A_DIR;
-    return;
-  }
-  if (c.mode == M_CHECK) {
-    const double tn = sqrt(s0);
-    c.checks += 1;
-    c.true_rr = s0;
-    c.residual_norm = tn;
-    if (!isfinite(tn)) {
-      c.status = TLS_PCG_NONFINITE;
-      c.mode = M_DONE;
-      return;
-    }
-    if (tn <= thr) {
-      c.status = TLS_PCG_CONVERGED;
-      c.mode = M_DONE;
-      return;
-    }
-    const double drift = sqrt(s1);
-    c.drift_rr = s1;
-    const bool last = c.iterations >= c.max_iterations;
-    if (st->rec_hit || c.periodic || drift > c.drift_tolerance * fmax(tn, thr)) {
-      c.rz = s2;
-      c.rz_true = s2;
-      c.restarts += 1;
-      st->action = A_RESTART;
-      c.mode = last ? M_FINAL : M_ITER;
-      return;
-    }
-    c.beta = c.rz_new / c.rz;
-    c.rz = c.rz_new;
-    st->action = A_RESTORE_DIR;
-    c.mode = last ? M_FINAL : M_ITER;
-    return;
-  }
-  // M_FINAL
-  const double tn = sqrt(s0);
-  c.checks += 1;
-  c.true_rr = s0;
-  c.residual_norm = tn;
-  if (isfinite(tn) && tn <= thr) c.status = TLS_PCG_CONVERGED;
-  else if (!isfinite(tn)) c.status = TLS_PCG_NONFINITE;
-  else c.status = st->pending;
-  c.mode = M_DONE;
-}
-
 // ---------------------------------------------------------------- update
-// One PCG step's vector work on blocks [b0, nblocks) with stride `step`:
-// ITER: x += alpha p, r -= alpha Ap, z = M r; sums r.r, r.z.
-// CHECK/FINAL: ap holds A x; true residual tr = rhs - A x (into ap), ztrue = M tr;
-// sums tr.tr, (tr - r).(tr - r), tr.ztrue.
-template <int D, typename TV>
-__device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nblocks, int64_t b0, int64_t step,
-                                                  int mode, double alpha, const TV* __restrict__ rhs, TV* x, TV* r,
-                                                  TV* z, const TV* p, TV* ap, TV* ztrue, double& a0, double& a1,
-                                                  double& a2) {
-  for (int64_t b = b0; b < nblocks; b += step) {
-    const int gi = find_group(bs, b);
-    const int64_t i = b - bs.block_begin[gi];
-    const tls_block_group& g = bs.g[gi];
-    const int dim = g.dim;
-    int64_t cols[D];
-    block_cols<D>(g, i, cols);
-    double rb[D], zb[D];
-    if (mode == M_ITER) {
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        rb[k] = 0.0;
-        if (k < dim) {
-          const int64_t col = cols[k];
-          x[col] = static_cast<TV>(to_d(x[col]) + alpha * to_d(p[col]));
-          const TV rn = static_cast<TV>(to_d(r[col]) - alpha * to_d(ap[col]));
-          r[col] = rn;
-          rb[k] = to_d(rn);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        rb[k] = 0.0;
-        if (k < dim) {
-          const int64_t col = cols[k];
-          const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ap[col]));
-          ap[col] = tr;
-          const double t = to_d(tr);
-          rb[k] = t;
-          a0 += t * t;
-          const double dr = t - to_d(r[col]);
-          a1 += dr * dr;
-        }
-      }
-    }
-    if (mode == M_FINAL) continue;
-    if (bs.identity || g.factor == nullptr) {
-#pragma unroll
-      for (int k = 0; k < D; ++k) zb[k] = rb[k];
-    } else {
-      solve_block<D>(g.factor + i * dim * dim, dim, rb, zb);
-    }
-    TV* zdst = (mode == M_ITER) ? z : ztrue;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      if (k < dim) {
-        const TV zk = static_cast<TV>(zb[k]);
-        zdst[cols[k]] = zk;
-        const double zd = to_d(zk);
-        if (mode == M_ITER) {
-          a0 += rb[k] * rb[k];
-          a1 += rb[k] * zd;
-        } else {
-          a2 += rb[k] * zd;
-        }
-      }
-    }
-  }
-}
-
-// Direction / restart / swap for elements [i0, n) with stride `step`.
-template <typename TV>
-__device__ __forceinline__ void pcg_direction_elems(int64_t n, int64_t i0, int64_t step, int action, double beta,
-                                                    bool to_final, const TV* x, TV* r, const TV* z, TV* p, TV* psave,
-                                                    const TV* ap, const TV* ztrue) {
-  for (int64_t i = i0; i < n; i += step) {
-    switch (action) {
-      case A_DIR:
-        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(p[i]));
-        break;
-      case A_RESTART:
-        r[i] = ap[i];
-        p[i] = ztrue[i];
-        break;
-      case A_RESTORE_DIR:
-        p[i] = static_cast<TV>(to_d(z[i]) + beta * to_d(psave[i]));
-        break;
-      case A_SWAP_TO_X:
-        psave[i] = p[i];
-        p[i] = x[i];
-        break;
-    }
-    if (to_final) p[i] = x[i];
-  }
-}
-
 template <int D, typename TV>
 __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, int64_t nblocks, PcgState* st,
                                                                  const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
@@ -572,6 +332,30 @@ static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
   if (op_blocks > kOpPartials) return tls_set_error(TLS_ERR_UNSUPPORTED, "operator uses too many blocks");
   set_block_counts_kernel<<<1, 1, 0, s>>>(st, op_blocks, gb);
   TLS_CHECK_LAUNCH();
+  if constexpr (sizeof(TV) == 8) {
+    // small Schur systems: the whole loop in one persistent cooperative launch
+    if (a->op_kind == 1 && nb <= kSmallMaxBlocks && steps > 0) {
+      PcgLoop q{};
+      q.bs = bs;
+      q.nb = nb;
+      q.n = a->n;
+      q.st = st;
+      q.rhs = (const double*)a->rhs;
+      q.x = (double*)a->x;
+      q.r = (double*)a->r;
+      q.z = (double*)a->z;
+      q.p = (double*)a->p;
+      q.psave = (double*)a->psave;
+      q.ap = (double*)a->ap;
+      q.ztrue = (double*)a->ztrue;
+      q.dots = a->partials;
+      q.steps = steps;
+      const int rc = tls_schur_pcg_launch(a->schur, q, maxdim, s);
+      if (rc != TLS_ERR_UNSUPPORTED) return rc;
+    }
+  }
+  // multi-kernel path: at most 16 queued steps per call (the host polls between calls)
+  if (steps > 16) steps = 16;
   return with_dim(maxdim, [&](auto dim) -> int {
     constexpr int D = decltype(dim)::value;
     for (int k = 0; k < steps; ++k) {

@@ -21,7 +21,8 @@ struct PcgState {
   int32_t alpha_ok;      // curvature and r.z finite and positive this step
   uint32_t ticket_op;    // last-block-done counters (reset by the last block)
   uint32_t ticket_upd;
-  int32_t pad_;
+  uint32_t bar_count;    // grid barrier of the persistent Schur-PCG kernel
+  uint32_t bar_gen;
 };
 
 // Deterministic sum of p[0..n) by one block (fixed strided order, fixed tree).

@@ -28,6 +28,7 @@
 
 #include "blocks.cuh"
 #include "common.cuh"
+#include "pcg_device.cuh"
 #include "pcg_state.cuh"
 
 namespace tls {
@@ -142,20 +143,164 @@ __device__ __forceinline__ void sts4(TA* p, const TA (&v)[4]) {
   }
 }
 
+// Compute one chunk held in shared memory (W slab `Ws`, metadata `Ms`):
 // MODE 0: S x partials (phase 1 from x); MODE 1: reduced rhs (y_p = a.ybuf[p]).
 // TA: arithmetic type of the per-edge products and of the run sums (float64:
 // S = U - W W^T cancels heavily, and float32 products stalled CG); W is
 // stored as TW. Per-variable sums y_p and every sum across runs are float64.
-// XS: the reduced vector x is staged in shared memory (as TA) at kernel start.
+// XS: x was staged in shared memory (as TA). COH: x is rewritten by this
+// kernel between matvecs (persistent loop): plain coherent loads after the
+// grid barrier instead of the read-only (.nc) path.
+template <int DR, int DE, int CAP, int MODE, typename TW, typename TA, bool XS, bool COH>
+__device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const double* __restrict__ x, const TA* x_s,
+                                              TA* t_s, const TW* Ws, const int32_t* Ms, int c) {
+  constexpr int EPT = CAP / kChunkThreads;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int ne = Ms[0], np = Ms[1];
+  const int32_t* er = Ms + kMetaHead;
+  const uint32_t* meta = reinterpret_cast<const uint32_t*>(Ms + kMetaHead + CAP);
+  const int32_t* tpos = Ms + kMetaHead + 2 * CAP;
+  const int32_t* pp = Ms + kMetaHead + 3 * CAP;
+  const int32_t* pe = Ms + 2 * kMetaHead + 4 * CAP;
+  const int le0 = tid * EPT;  // this thread's first edge
+  // ---- phase 1: t_e = W_e^T x_i
+  if constexpr (MODE == 0) {
+    if (le0 < ne) {
+      TW w[DR * DE][EPT];
+#pragma unroll
+      for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        if (le0 + j < ne) {
+          const int i = er[le0 + j];
+          TA xr[DR];
+#pragma unroll
+          for (int k = 0; k < DR; ++k) {
+            if constexpr (XS) xr[k] = x_s[i * DR + k];
+            else if constexpr (COH) xr[k] = static_cast<TA>(x[(int64_t)i * DR + k]);  // written by this kernel: no .nc path
+            else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
+          }
+          TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
+#pragma unroll
+          for (int b = 0; b < DE; ++b) {
+#pragma unroll
+            for (int k = 0; k < DR; ++k) t[b] = fma(static_cast<TA>(w[k * DE + b][j]), xr[k], t[b]);
+          }
+          sts4(t_s + (le0 + j) * 4, t);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges), then overwrite t_s
+  constexpr int PPT = CAP / kChunkThreads;
+  double yreg[PPT][DE];
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const int pl = tid + q * kChunkThreads;
+#pragma unroll
+    for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
+    if (pl < np) {
+      if constexpr (MODE == 0) {
+        // four edges per round: independent shared-memory loads, fixed-order sums
+        const int jb = pp[pl], je = pp[pl + 1];
+        for (int j = jb; j < je; j += 4) {
+          TA t[4][4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (j + u < je) lds4(t_s + pe[j + u] * 4, t[u]);
+            else t[u][0] = t[u][1] = t[u][2] = t[u][3] = TA(0);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int b = 0; b < DE; ++b)
+              if (j + u < je) yreg[q][b] += static_cast<double>(t[u][b]);
+        }
+      } else {
+        const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + pe[pp[pl]]);
+#pragma unroll
+        for (int b = 0; b < DE; ++b) yreg[q][b] = a.ybuf[p * DE + b];
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const int pl = tid + q * kChunkThreads;
+    if (pl < np) {
+      TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
+#pragma unroll
+      for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[q][b]);
+      sts4(t_s + pl * 4, y);
+    }
+  }
+  __syncthreads();
+  // ---- phase 2: u_e = W_e y_p; segmented sums over runs of equal retained
+  // variable (runs never cross a window of 32 * EPT edges): sequential within
+  // the thread, then a warp-segmented inclusive scan of the carries over as
+  // many steps as the warp's longest run needs.
+  {
+    TA v[EPT][DR];
+    int head[EPT];
+    bool tail[EPT];
+    TW wv[DR * DE][EPT];
+#pragma unroll
+    for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, wv[kb]);
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+      const int le = le0 + j;
+      const int pos = lane * EPT + j;  // position inside the 32*EPT-edge window
+      const bool valid = le < ne;
+      const uint32_t m = valid ? meta[le] : 0u;
+      head[j] = valid ? (int)((m >> 16) & 63u) : pos;
+      tail[j] = valid && ((m >> 22) & 1u);
+      TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
+      if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);
+      const bool cont = j > 0 && head[j] < pos;  // same run as edge j-1
+#pragma unroll
+      for (int k = 0; k < DR; ++k) {
+        TA u = TA(0);
+#pragma unroll
+        for (int b = 0; b < DE; ++b) u = fma(static_cast<TA>(wv[k * DE + b][j]), y[b], u);
+        v[j][k] = cont ? v[j > 0 ? j - 1 : 0][k] + u : u;
+      }
+    }
+    const int hl = head[EPT - 1] / EPT;           // lane holding the start of this thread's last run
+    const bool from_left = head[0] < lane * EPT;  // this thread's first run began in an earlier lane
+    // lanes any run spans backwards; offsets 1, 2, 4, ... <= span cover it
+    const unsigned span = __reduce_max_sync(0xffffffffu, (unsigned)(lane - hl));
+#pragma unroll
+    for (int k = 0; k < DR; ++k) {
+      TA cval = v[EPT - 1][k];
+      for (unsigned off = 1; off <= span; off <<= 1) {
+        const TA o = __shfl_up_sync(0xffffffffu, cval, off);
+        if (lane - (int)off >= hl) cval += o;
+      }
+      const TA prev = __shfl_up_sync(0xffffffffu, cval, 1);
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        if (tail[j]) {
+          // only the thread's first run can have begun in an earlier lane
+          const TA tot = (from_left && head[j] == head[0]) ? v[j][k] + prev : v[j][k];
+          reinterpret_cast<TA*>(a.run_partial)[(int64_t)tpos[le0 + j] * DR + k] = tot;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// MODE 0: S x partials; MODE 1: reduced rhs. Persistent over chunks: thread 0
+// streams chunk slabs with 1-D bulk copies into two shared-memory stages.
 template <int DR, int DE, int CAP, int MODE, typename TW, typename TA, bool XS>
 __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur_args a, const double* __restrict__ x) {
   using S = SlabShape<DR, DE, CAP, TW, TA>;
-  constexpr int EPT = S::kEpt;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   TA* t_s = reinterpret_cast<TA*>(smem + 2 * S::kStageBytes);  // [CAP][4]: t_e, then y_p
   TA* x_s = reinterpret_cast<TA*>(smem + S::kBaseSmem);         // [nretained*DR] when XS
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x;
   const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
   const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
   if (tid == 0) {
@@ -184,158 +329,27 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
     const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
     const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
-    const int ne = Ms[0], np = Ms[1];
-    const int32_t* er = Ms + kMetaHead;
-    const uint32_t* meta = reinterpret_cast<const uint32_t*>(Ms + kMetaHead + CAP);
-    const int32_t* tpos = Ms + kMetaHead + 2 * CAP;
-    const int32_t* pp = Ms + kMetaHead + 3 * CAP;
-    const int32_t* pe = Ms + 2 * kMetaHead + 4 * CAP;
-    const int le0 = tid * EPT;  // this thread's first edge
-    // ---- phase 1: t_e = W_e^T x_i (TA products)
-    if constexpr (MODE == 0) {
-      if (le0 < ne) {
-        TW w[DR * DE][EPT];
-#pragma unroll
-        for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
-#pragma unroll
-        for (int j = 0; j < EPT; ++j) {
-          if (le0 + j < ne) {
-            const int i = er[le0 + j];
-            TA xr[DR];
-#pragma unroll
-            for (int k = 0; k < DR; ++k) {
-              if constexpr (XS) xr[k] = x_s[i * DR + k];
-              else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
-            }
-            TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
-#pragma unroll
-            for (int b = 0; b < DE; ++b) {
-#pragma unroll
-              for (int k = 0; k < DR; ++k) t[b] = fma(static_cast<TA>(w[k * DE + b][j]), xr[k], t[b]);
-            }
-            sts4(t_s + (le0 + j) * 4, t);
-          }
-        }
-      }
-      __syncthreads();
-    }
-    // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges), then overwrite t_s
-    constexpr int PPT = CAP / kChunkThreads;
-    double yreg[PPT][DE];
-#pragma unroll
-    for (int q = 0; q < PPT; ++q) {
-      const int pl = tid + q * kChunkThreads;
-#pragma unroll
-      for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
-      if (pl < np) {
-        if constexpr (MODE == 0) {
-          // four edges per round: independent shared-memory loads, fixed-order sums
-          const int jb = pp[pl], je = pp[pl + 1];
-          for (int j = jb; j < je; j += 4) {
-            TA t[4][4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (j + u < je) lds4(t_s + pe[j + u] * 4, t[u]);
-              else t[u][0] = t[u][1] = t[u][2] = t[u][3] = TA(0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-              for (int b = 0; b < DE; ++b)
-                if (j + u < je) yreg[q][b] += static_cast<double>(t[u][b]);
-          }
-        } else {
-          const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + pe[pp[pl]]);
-#pragma unroll
-          for (int b = 0; b < DE; ++b) yreg[q][b] = a.ybuf[p * DE + b];
-        }
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PPT; ++q) {
-      const int pl = tid + q * kChunkThreads;
-      if (pl < np) {
-        TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
-#pragma unroll
-        for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[q][b]);
-        sts4(t_s + pl * 4, y);
-      }
-    }
-    __syncthreads();
-    // ---- phase 2: u_e = W_e y_p; segmented sums over runs of equal retained
-    // variable (runs never cross a window of 32 * EPT edges): sequential within
-    // the thread, then a warp-segmented inclusive scan of the carries.
-    {
-      TA v[EPT][DR];
-      int head[EPT];
-      bool tail[EPT];
-      TW wv[DR * DE][EPT];
-#pragma unroll
-      for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, wv[kb]);
-#pragma unroll
-      for (int j = 0; j < EPT; ++j) {
-        const int le = le0 + j;
-        const int pos = lane * EPT + j;  // position inside the 32*EPT-edge window
-        const bool valid = le < ne;
-        const uint32_t m = valid ? meta[le] : 0u;
-        head[j] = valid ? (int)((m >> 16) & 63u) : pos;
-        tail[j] = valid && ((m >> 22) & 1u);
-        TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
-        if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);
-        const bool cont = j > 0 && head[j] < pos;  // same run as edge j-1
-#pragma unroll
-        for (int k = 0; k < DR; ++k) {
-          TA u = TA(0);
-#pragma unroll
-          for (int b = 0; b < DE; ++b) u = fma(static_cast<TA>(wv[k * DE + b][j]), y[b], u);
-          v[j][k] = cont ? v[j > 0 ? j - 1 : 0][k] + u : u;
-        }
-      }
-      const int hl = head[EPT - 1] / EPT;           // lane holding the start of this thread's last run
-      const bool from_left = head[0] < lane * EPT;  // this thread's first run began in an earlier lane
-#pragma unroll
-      for (int k = 0; k < DR; ++k) {
-        TA cval = v[EPT - 1][k];
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const TA o = __shfl_up_sync(0xffffffffu, cval, off);
-          if (lane - off >= hl) cval += o;
-        }
-        const TA prev = __shfl_up_sync(0xffffffffu, cval, 1);
-#pragma unroll
-        for (int j = 0; j < EPT; ++j) {
-          if (tail[j]) {
-            // only the thread's first run can have begun in an earlier lane
-            const TA tot = (from_left && head[j] == head[0]) ? v[j][k] + prev : v[j][k];
-            reinterpret_cast<TA*>(a.run_partial)[(int64_t)tpos[le0 + j] * DR + k] = tot;
-          }
-        }
-      }
-    }
-    __syncthreads();
+    chunk_compute<DR, DE, CAP, MODE, TW, TA, XS, false>(a, x, x_s, t_s, Ws, Ms, c);
   }
 }
 
-// One block per retained variable: sum its contiguous run partials (float64,
-// fixed order), then
-// MODE 0: out = s U s x + lambda x - sum  (matvec; dot partial + PCG epilogue)
-// MODE 1: out = b_retained - sum          (reduced rhs, b float64 full vector)
-template <int DR, int MODE, typename TV, typename TP>
-__global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, const TV* __restrict__ x,
-                                                           const double* __restrict__ b, TV* __restrict__ out,
-                                                           double* __restrict__ dot_partials, PcgState* pst) {
-  __shared__ double sm[8][DR];
-  __shared__ double ux[DR * DR];
-  __shared__ double smd[8];
-  const int64_t i = blockIdx.x;
+// Sum retained variable i's contiguous run partials (float64, fixed order) and
+// finish its rows, with 256 threads:
+// MODE 0: out = s U s x + lambda x - sum; returns x_i . out_i to thread 0
+// MODE 1: out = b_retained - sum
+// COH: x is rewritten by this kernel (persistent loop): plain loads, not .nc.
+template <int DR, int MODE, typename TV, typename TP, bool COH>
+__device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* __restrict__ x,
+                                             const double* __restrict__ b, TV* __restrict__ out, int64_t i,
+                                             double (*sm)[DR], double* ux) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const TP* part = reinterpret_cast<const TP*>(a.run_partial);
   if constexpr (MODE == 0) {
     if (tid < DR * DR) {
       const int l = tid % DR;
       const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
-      ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * to_d(x[i * DR + l]));
+      const double xl = to_d(x[i * DR + l]);
+      ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * xl);
     }
   }
   double acc[DR];
@@ -349,7 +363,7 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
     for (int q = 0; q < 4; ++q) {
       const int j = j0 + q * 256;
 #pragma unroll
-      for (int k = 0; k < DR; ++k) v[q][k] = j < re ? __ldcg(part + (int64_t)j * DR + k) : TP(0);
+      for (int k = 0; k < DR; ++k) v[q][k] = j < re ? part[(int64_t)j * DR + k] : TP(0);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -362,8 +376,8 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
     if (lane == 0) sm[warp][k] = v;
   }
   __syncthreads();
+  double dot = 0.0;
   if (warp == 0) {
-    double dot = 0.0;
     if (lane < DR) {
       const int k = lane;
       double tot = 0.0;
@@ -383,12 +397,183 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
         out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - tot);
       }
     }
-    if constexpr (MODE == 0) {
-      dot = warp_sum(dot);
-      if (lane == 0 && dot_partials) dot_partials[i] = dot;
-    }
+    if constexpr (MODE == 0) dot = warp_sum(dot);
   }
-  if (MODE == 0 && pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
+  __syncthreads();  // sm and ux are reused by the caller's next variable
+  return dot;
+}
+
+// One block per retained variable (gather_one), then for MODE 0 the dot
+// partial and the PCG epilogue (curvature and alpha in the last block).
+template <int DR, int MODE, typename TV, typename TP>
+__global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, const TV* __restrict__ x,
+                                                           const double* __restrict__ b, TV* __restrict__ out,
+                                                           double* __restrict__ dot_partials, PcgState* pst) {
+  __shared__ double sm[8][DR];
+  __shared__ double ux[DR * DR];
+  __shared__ double smd[8];
+  const double dot = gather_one<DR, MODE, TV, TP, false>(a, x, b, out, blockIdx.x, sm, ux);
+  if constexpr (MODE == 0) {
+    if (threadIdx.x == 0 && dot_partials) dot_partials[blockIdx.x] = dot;
+    if (pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
+  }
+}
+
+// ---------------------------------------------------------------- persistent Schur-PCG
+// The whole PCG loop on the reduced system in ONE cooperative launch (all
+// CTAs co-resident): per step
+//   A  every CTA streams its chunks (Ap partials from p), prefetching the
+//      next step's first chunk while B and C run (W does not change)
+//   -- grid barrier --
+//   B  gather: one retained variable per CTA at a time -> Ap, x.Ap partials
+//   -- grid barrier; before releasing, the last CTA to arrive runs --
+//   C  curvature and alpha, update x, r, z = M r, the decision and the
+//      direction (the same state machine as the multi-kernel path)
+// Every wait is bounded (about a second); on timeout the kernel flags a.err
+// and every CTA leaves after draining its own bulk copy.
+// Grid barrier over all CTAs of a cooperative launch; the last CTA to arrive
+// runs `tail()` (all its threads) before releasing the others. Waiters poll
+// with a short sleep; false on timeout (about a second).
+template <typename F>
+__device__ __forceinline__ bool grid_barrier(PcgState* st, int32_t* err, F&& tail) {
+  __shared__ int ok, last;
+  __shared__ uint32_t gen0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* gen = &st->bar_gen;
+    gen0 = *gen;
+    __threadfence();
+    ok = 1;
+    last = atomicAdd(&st->bar_count, 1u) == gridDim.x - 1;
+    if (last) __threadfence();
+  }
+  __syncthreads();
+  if (last) {
+    tail();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      st->bar_count = 0;
+      __threadfence();
+      atomicExch(&st->bar_gen, gen0 + 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    volatile uint32_t* gen = &st->bar_gen;
+    const long long t0 = clock64();
+    while (*gen == gen0) {
+      __nanosleep(64);
+      if (clock64() - t0 > (1LL << 31)) {
+        if (err) atomicExch(err, 2);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+template <int DR, int DE, int CAP, typename TW, int D>
+__global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_args a, PcgLoop q) {
+  using TA = double;
+  using S = SlabShape<DR, DE, CAP, TW, TA>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double sm[8][DR];
+  __shared__ double ux[DR * DR];
+  __shared__ double smd[kChunkThreads / 32];
+  __shared__ int s_action, s_tofinal, s_go;
+  __shared__ double s_beta;
+  TA* t_s = reinterpret_cast<TA*>(smem + 2 * S::kStageBytes);
+  const int tid = threadIdx.x;
+  const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
+  const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
+  PcgState* st = q.st;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int c, int stg) {
+    unsigned char* base = smem + stg * S::kStageBytes;
+    fence_proxy_async();
+    mbar_expect_tx(&bar[stg], S::kStageBytes);
+    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &bar[stg]);
+    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &bar[stg]);
+  };
+  // this CTA's chunks: blockIdx.x + j * gridDim.x, j < kct, cycled every step
+  const int kct = (int)blockIdx.x < a.nchunks ? (a.nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * (int)gridDim.x; };
+  int it = 0;  // chunk consumptions so far; the copy for `it` is always in flight
+  if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
+  for (int step = 0; step < q.steps; ++step) {
+    if (tid == 0) {
+      const int status = __ldcg(&st->pub.status), mode = __ldcg(&st->pub.mode);
+      s_go = status == TLS_PCG_ACTIVE && mode != M_DONE;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    // ---- A: chunk partials of A p
+    for (int j = 0; j < kct; ++j, ++it) {
+      const int stg = it & 1;
+      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
+      mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+      const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
+      const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
+      chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
+    }
+    if (!grid_barrier(st, a.err, [] {})) break;
+    // ---- B: gather per retained variable
+    for (int64_t i = blockIdx.x; i < a.nretained; i += gridDim.x) {
+      const double dot = gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
+      if (tid == 0) q.dots[i] = dot;
+    }
+    // ---- C (the last CTA through the barrier): curvature and alpha, update,
+    // preconditioner, decision, direction
+    auto phase_c = [&] {
+      tls_pcg_control& c = st->pub;
+      const int mode = c.mode;
+      if (c.status == TLS_PCG_ACTIVE && mode == M_ITER) {
+        const double curv = block_sum_cg<kChunkThreads>(q.dots, a.nretained, smd);
+        if (tid == 0) {
+          const double rz = c.rz;
+          c.curvature = curv;
+          const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
+          st->alpha_ok = ok;
+          c.alpha = ok ? rz / curv : 0.0;
+        }
+        __syncthreads();
+      }
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
+      double alpha = 0.0;
+      if (work && mode == M_ITER) {
+        if (!st->alpha_ok) work = false;
+        else alpha = c.alpha;
+      }
+      if (work)
+        pcg_update_blocks<D, double, true>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, q.x, q.r, q.z, q.p,
+                                           q.ap, q.ztrue, a0, a1, a2);
+      const double t0 = block_sum<kChunkThreads>(a0, smd);
+      const double t1 = block_sum<kChunkThreads>(a1, smd);
+      const double t2 = block_sum<kChunkThreads>(a2, smd);
+      if (tid == 0) {
+        pcg_decide(st, t0, t1, t2);
+        s_action = st->action;
+        s_beta = st->pub.beta;
+        s_tofinal = st->pub.mode == M_FINAL && st->action != A_SWAP_TO_X;
+      }
+      __syncthreads();
+      if (s_action != A_NONE)
+        pcg_direction_elems<double, true>(q.n, tid, kChunkThreads, s_action, s_beta, s_tofinal != 0, q.x, q.r, q.z,
+                                          q.p, q.psave, q.ap, q.ztrue);
+    };
+    if (!grid_barrier(st, a.err, phase_c)) break;
+  }
+  // drain this CTA's copy in flight before leaving (bounded)
+  if (kct > 0) mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, a.err);
+  __syncthreads();
 }
 
 // W slab index of component k of slab entry s.
@@ -634,6 +819,55 @@ struct SchurOps {
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
+  template <typename TW, int CAP, int D>
+  static int pcg_go(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
+    using S = SlabShape<DR, DE, CAP, TW, double>;
+    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
+    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
+      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
+    auto k = schur_pcg_kernel<DR, DE, CAP, TW, D>;
+    const int smem = S::kBaseSmem;
+    static int grid = 0;  // co-resident CTAs: per-SM occupancy x SMs, once per instantiation
+    if (grid == 0) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      int per_sm = 0, dev = 0, sms = 0, coop = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
+      grid = (coop && per_sm > 0 && sms > 0) ? per_sm * sms : -1;
+    }
+    if (grid <= 0) return tls_set_error(TLS_ERR_UNSUPPORTED, "cooperative launch unavailable");
+    tls_schur_args aa = a;
+    PcgLoop qq = q;
+    void* args[] = {&aa, &qq};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k, dim3(grid), dim3(kChunkThreads), args,
+                                                      (size_t)smem, s);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+      cudaGetLastError();  // clear; the caller falls back to the multi-kernel loop
+      return tls_set_error(TLS_ERR_UNSUPPORTED, "cooperative grid does not fit");
+    }
+    if (e != cudaSuccess) return tls_set_error(TLS_ERR_CUDA, cudaGetErrorString(e));
+    tls_count_launch();
+    return TLS_OK;
+  }
+  template <typename TW, int D>
+  static int pcg_cap(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
+    if constexpr (sizeof(TW) == 4) {
+      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs");
+      return pcg_go<TW, 512, D>(a, q, s);
+    } else {
+      if (a.cap != 256) return tls_set_error(TLS_ERR_INVALID, "float64 W uses 256-edge chunk slabs");
+      return pcg_go<TW, 256, D>(a, q, s);
+    }
+  }
+  template <typename TW>
+  static int pcg(const tls_schur_args& a, const PcgLoop& q, int maxdim, cudaStream_t s) {
+    constexpr int DB = DR <= 3 ? 3 : (DR <= 6 ? 6 : 8);
+    if (maxdim <= 1) return pcg_cap<TW, 1>(a, q, s);
+    if (maxdim <= DB) return pcg_cap<TW, DB>(a, q, s);
+    return tls_set_error(TLS_ERR_UNSUPPORTED, "preconditioner blocks wider than the retained blocks");
+  }
   template <typename TW>
   static int damp(const tls_schur_args& a, cudaStream_t s) {
     cudaMemsetAsync(a.bad, 0, sizeof(int32_t), s);
@@ -692,6 +926,22 @@ int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* d
       return O::template matvec<double, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, pst, s);
     return O::template matvec<float, double, double>(*a, (const double*)x, (double*)out, dots, gblocks, pst, s);
   });
+}
+
+// The whole Schur-PCG loop (up to q.steps state-machine steps) in one
+// cooperative launch; TLS_ERR_UNSUPPORTED when the block shapes have no
+// persistent instantiation (the caller then runs the multi-kernel loop).
+int tls_schur_pcg_launch(const tls_schur_args* a, const PcgLoop& q, int maxdim, cudaStream_t s) {
+  if (a->vec_dtype != TLS_F64) return tls_set_error(TLS_ERR_UNSUPPORTED, "reduced Schur vectors are float64");
+  if (a->nchunks == 0 || a->nretained == 0) return tls_set_error(TLS_ERR_UNSUPPORTED, "empty Schur system");
+  auto go = [&](auto ops) -> int {
+    using O = decltype(ops);
+    return a->wdtype == TLS_F64 ? O::template pcg<double>(*a, q, maxdim, s) : O::template pcg<float>(*a, q, maxdim, s);
+  };
+  if (a->dr == 6 && a->de == 3) return go(SchurOps<6, 3>{});
+  if (a->dr == 7 && a->de == 3) return go(SchurOps<7, 3>{});
+  if (a->dr == 3 && a->de == 3) return go(SchurOps<3, 3>{});
+  return tls_set_error(TLS_ERR_UNSUPPORTED, "no persistent Schur-PCG for these block dims");
 }
 
 extern "C" int tls_schur_damp(const tls_schur_args* a, tls_stream_t stream) {

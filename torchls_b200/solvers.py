@@ -324,9 +324,9 @@ class DevicePCG:
 
     def run(self, rhs: Tensor, config: ConjugateGradientConfig, *, normal_args=None, schur_args=None,
             preconditioner: BlockJacobiPreconditioner | None = None, error_word: Tensor | None = None) -> PCGResult:
-        """``error_word``: the operator's device error flag (the Schur chunk
-        kernel's bounded bulk-copy waits set it instead of hanging); read once
-        after the loop."""
+        """``error_word``: the operator's device error flag (the Schur kernels'
+        bounded bulk-copy and grid-barrier waits set it instead of hanging);
+        read once after the loop."""
         a = L.PcgArgs()
         a.n = self.n
         a.vec_dtype = L.dtype_code(self.dtype)
@@ -353,13 +353,17 @@ class DevicePCG:
                int(config.residual_check_interval), int(config.restart_strategy == "periodic"),
                float(config.residual_drift_tolerance), stream)
         batch = config.graph_batch_iterations
+        if schur_args is not None:
+            # small Schur systems run the whole loop in one persistent launch;
+            # otherwise the library queues at most 16 steps per call
+            batch = max(batch, 4 * int(config.max_iterations) + 16)
         while True:
             ctrl = self._read()
             if ctrl.status != L.PCG_ACTIVE:
                 break
             L.call("tls_pcg_run", C.byref(a), batch, stream)
         if error_word is not None and int(error_word.item()) != 0:
-            raise RuntimeError("Schur matvec: a device wait for a bulk copy timed out")
+            raise RuntimeError("Schur PCG: a bounded device wait (bulk copy or grid barrier) timed out")
         return PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
                          ctrl.status == L.PCG_CONVERGED, _REASONS[ctrl.status], int(ctrl.restarts),
                          int(ctrl.checks), float(ctrl.rhs_norm))
