@@ -395,6 +395,7 @@ def run_cuda(args, world, rank, local):
         "lm_iterations_per_s": summ.iterations / mixed_s,
         "fp64_s": None if fp64 is None else fp64[0],
         "fp64_final_cost": None if fp64 is None else fp64[1].final_cost,
+        "fp64_cg_iterations": None if fp64 is None else fp64[1].linear_iterations_history,
         "mixed_speedup_vs_fp64": None if fp64 is None else fp64[0] / mixed_s,
         "normal_matvec": {"gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
                           "bytes": roof["normal_bytes"]},

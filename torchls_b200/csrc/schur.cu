@@ -694,47 +694,63 @@ __global__ void schur_backsub_kernel(tls_schur_args a, const TV* __restrict__ xc
   }
 }
 
-// out_i = s U s - sum_{e in i} W_e W_e^T (lambda added by the Cholesky)
+// out_i = s U s - sum_{e in i} W_e W_e^T (lambda added by the Cholesky), one
+// 256-thread block per retained variable, one thread per run of its edges.
+// W_e is recomputed in float64 from the cross block and L_p^-1 with the
+// whitening kernel's arithmetic (each run's cross blocks are contiguous, so
+// the reads are whole sectors; the stored W slab is strided by the chunk cap).
 template <int DR, int DE, typename TW>
 __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, double* __restrict__ out) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const TW* w = reinterpret_cast<const TW*>(a.w);
-  double acc[DR * (DR + 1) / 2];
+  constexpr int NU = DR * (DR + 1) / 2;
+  __shared__ double red[8][NU];
+  const int64_t i = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double sr[DR];
 #pragma unroll
-  for (int k = 0; k < DR * (DR + 1) / 2; ++k) acc[k] = 0.0;
-  const bool live = warp < a.nretained;
-  if (live) {
-    const int rb = a.rrun_ptr[warp], re = a.rrun_ptr[warp + 1];
-    for (int j = rb + lane; j < re; j += 32) {
-      const int64_t s0 = a.crun_start[j];
-      const int len = a.crun_len[j];
-      for (int64_t s = s0; s < s0 + len; ++s) {
-        double wv[DR][DE];
+  for (int k = 0; k < DR; ++k) sr[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+  double acc[NU];
 #pragma unroll
-        for (int r = 0; r < DR; ++r)
+  for (int k = 0; k < NU; ++k) acc[k] = 0.0;
+  const int rb = a.rrun_ptr[i], re = a.rrun_ptr[i + 1];
+  for (int j = rb + tid; j < re; j += 256) {
+    const int64_t s0 = a.crun_start[j];
+    const int len = a.crun_len[j];
+    for (int64_t s = s0; s < s0 + len; ++s) {
+      const int64_t p = a.slab_e[s];
+      double se[DE];
 #pragma unroll
-          for (int c = 0; c < DE; ++c) wv[r][c] = to_d(w[w_index<DR, DE>(s, r * DE + c, a.cap)]);
-        int idx = 0;
+      for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
+      const double* Li = a.inv_l + p * DE * DE;
+      const double* E = a.cross + s * DR * DE;
+      double wv[DR][DE];
 #pragma unroll
-        for (int r = 0; r < DR; ++r)
+      for (int r = 0; r < DR; ++r)
 #pragma unroll
-          for (int q = r; q < DR; ++q) {
-            double v = 0.0;
+        for (int c = 0; c < DE; ++c) {
+          double v = 0.0;
 #pragma unroll
-            for (int c = 0; c < DE; ++c) v += wv[r][c] * wv[q][c];
-            acc[idx++] += v;
-          }
-      }
+          for (int k = 0; k < DE; ++k) v += sr[r] * E[r * DE + k] * se[k] * Li[c * DE + k];
+          wv[r][c] = to_d(static_cast<TW>(v));  // the operator's (stored) precision
+        }
+      int idx = 0;
+#pragma unroll
+      for (int r = 0; r < DR; ++r)
+#pragma unroll
+        for (int q = r; q < DR; ++q) {
+          double v = 0.0;
+#pragma unroll
+          for (int c = 0; c < DE; ++c) v += wv[r][c] * wv[q][c];
+          acc[idx++] += v;
+        }
     }
   }
 #pragma unroll
-  for (int k = 0; k < DR * (DR + 1) / 2; ++k) acc[k] = warp_sum(acc[k]);
-  if (!live || lane != 0) return;
-  const int64_t i = warp;
-  double s[DR];
-#pragma unroll
-  for (int k = 0; k < DR; ++k) s[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+  for (int k = 0; k < NU; ++k) {
+    const double v = warp_sum(acc[k]);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (tid != 0) return;
   const double* U = a.ret_diag + i * DR * DR;
   double* o = out + i * DR * DR;
   int idx = 0;
@@ -742,9 +758,13 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
   for (int r = 0; r < DR; ++r)
 #pragma unroll
     for (int q = r; q < DR; ++q) {
-      const double v = s[r] * U[r * DR + q] * s[q] - acc[idx++];
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) t += red[w][idx];
+      const double v = sr[r] * U[r * DR + q] * sr[q] - t;
       o[r * DR + q] = v;
       o[q * DR + r] = v;
+      ++idx;
     }
 }
 
@@ -887,8 +907,7 @@ struct SchurOps {
   }
   template <typename TW>
   static int precond(const tls_schur_args& a, double* out, cudaStream_t s) {
-    const int blocks = (a.nretained * 32 + 255) / 256;
-    if (blocks > 0) schur_precond_kernel<DR, DE, TW><<<blocks, 256, 0, s>>>(a, out);
+    if (a.nretained > 0) schur_precond_kernel<DR, DE, TW><<<a.nretained, 256, 0, s>>>(a, out);
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
