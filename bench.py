@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--small", action="store_true", help="10-camera / 4,000-observation case (debug)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="only build the workload and time the matvec kernels (the ncu capture target)")
+    ap.add_argument("--workload", choices=["ba_mid", "pose_graph", "adjoint"], default="ba_mid",
+                    help="ba_mid: the 1M-observation bundle adjustment (default); pose_graph: the "
+                         "100,000-pose SE(3) graph with full-system PCG; adjoint: gradients of a "
+                         "160,000-observation bundle adjustment through the implicit adjoint")
     return ap.parse_args()
 
 
@@ -167,11 +171,11 @@ def flush_l2(buf):
     buf.add_(1.0)
 
 
-def time_solves(problem, init, tls, precision, steps, warmup, device, flush):
+def time_solves(problem, init, tls, precision, steps, warmup, device, flush, opts=None):
     """Warm up, then time `steps` solves individually with CUDA events."""
     from torchls_b200 import _lib
 
-    opts = solve_opts(tls, precision)
+    opts = solve_opts(tls, precision) if opts is None else opts
     for _ in range(warmup):
         problem.parameters = {k: v.clone() for k, v in init.items()}
         problem.solve(**opts)
@@ -310,6 +314,191 @@ def cpu_sample(small: bool):
     return one * iters, one, iters, np.__name__
 
 
+# ----------------------------------------------------------------------------- pose graph workload
+POSE_TARGET_FILE = os.path.join(ROOT, "tests", "golden", "pose_graph_target.json")
+POSE_METRIC = "pose-graph LM solve s (30 iterations, full-system PCG; mixed vs FP64 CUDA)"
+
+
+def pose_opts(tls, precision):
+    return dict(linear_solver="conjugate_gradient",
+                conjugate_gradient=tls.ConjugateGradientConfig(precision=precision),
+                termination=tls.TerminationConfig(max_iterations=30), return_summary=True)
+
+
+def run_pose(args, world, rank, local):
+    """SE(3) pose graph: 100,000 poses on a random walk, 99,999 odometry edges
+    and 300,000 loop closures (drawn with replacement among pairs within 3 m),
+    pose 0 fixed; LM with full-system block-Jacobi PCG, 30 iterations."""
+    import ctypes
+
+    import torchls_b200 as tls
+    from torchls_b200 import _lib as L
+    from torchls_b200 import synthetic
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    data = synthetic.make_pose_graph(100_000, 300_000, seed=0)
+    problem = synthetic.build_pose_graph(data, tls, device=device)
+    init = {k: v.clone() for k, v in problem.parameters.items()}
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    target = json.load(open(POSE_TARGET_FILE))["final_cost"] if os.path.exists(POSE_TARGET_FILE) else None
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        times, summ, launches = time_solves(problem, init, tls, "mixed", args.steps, args.warmup, device, flush,
+                                            opts=pose_opts(tls, "mixed"))
+    mixed_s = dist_max(sum(times) / len(times), world, device)
+    t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush,
+                              opts=pose_opts(tls, "native"))
+    fp64_s = dist_max(sum(t64) / len(t64), world, device)
+    # full-system normal matvec on this workload (float32 J, float64 vectors)
+    problem.parameters = {k: v.clone() for k, v in init.items()}
+    J = problem.linearize(jacobian_dtype=torch.float32).jacobian
+    v = torch.randn(J.shape[1], device=device, dtype=torch.float64)
+    y = torch.empty_like(v)
+    nargs = J.normal_args(torch.float64, 1e-3)
+    stream = L.stream_handle(device)
+    for _ in range(5):
+        L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    ev0.record()
+    for _ in range(reps):
+        L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
+    ev1.record()
+    torch.cuda.synchronize(device)
+    normal_s = ev0.elapsed_time(ev1) / 1e3 / reps
+    st = J.structure
+    nnz = sum(p.count * st.rdims[k] * st.D[k] for k, p in enumerate(st.plans))
+    slots = sum(p.count * len(p.type_indices) for p in st.plans)
+    normal_bytes = nnz * 4 + slots * 4 + 2 * J.shape[1] * 8
+    barrier(world)
+    if rank != 0:
+        return
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    gbs = normal_bytes / normal_s / 1e9
+    rel = None if target is None else abs(summ.final_cost - target) / target
+    line = {
+        "metric": POSE_METRIC, "value": mixed_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed_s * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
+        "config": {"workload": "pose_graph_100k", "poses": 100_000, "edges": int(data.edge_i.numel()),
+                   "solver": "conjugate_gradient", "max_lm_iterations": 30, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MB write); working set also exceeds L2"},
+        "final_cost": summ.final_cost, "target_cost": target, "rel_cost_error": rel,
+        "lm_iterations": summ.iterations, "cg_iterations": summ.linear_iterations_history,
+        "lm_iterations_per_s": summ.iterations / mixed_s, "fp64_s": fp64_s, "fp64_final_cost": s64.final_cost,
+        "fp64_cg_iterations": s64.linear_iterations_history, "mixed_speedup_vs_fp64": fp64_s / mixed_s,
+        "roofline": {"kernel": "full normal matvec (factor pass + gather)", "bound": "hbm", "achieved": gbs,
+                     "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
+                     "algorithmic_bytes": normal_bytes, "traffic": None},
+        "gpu_launches": launches, "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- implicit adjoint workload
+ADJ_METRIC = "implicit-adjoint BA gradient s (forward solve + adjoint) and max rel error vs central FD"
+
+
+def run_adjoint(args, world, rank, local):
+    """64 cameras, 20,000 points seen by 8 cameras each (160,000 observations),
+    Huber 0.01, camera 0 fixed, scale prior; gradients of the point/pose error
+    with respect to every observation (u, v) and every per-observation weight."""
+    import torchls_b200 as tls
+    from torchls_b200 import synthetic
+    from torchls_b200.adjoint import newton_polish, solve_implicit
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    data = synthetic.make_bundle_adjustment(64, 20_000, 8, seed=0)
+    prob, inp = synthetic.build_differentiable_bundle_adjustment(data, tls, device=device,
+                                                                 loss=tls.HuberLoss(0.01))
+    init = {k: v.clone() for k, v in prob.parameters.items()}
+    names = ["uv_free", "uv_fixed", "w_free", "w_fixed"]
+    theta = [inp[k].requires_grad_(True) for k in names]
+    term = tls.TerminationConfig(max_iterations=80, cost_tolerance=1e-15, gradient_tolerance=1e-16,
+                                 parameter_tolerance=1e-15)
+    exact = dict(linear_solver="schur_dense", termination=term)
+
+    def run(opts):
+        prob.parameters = {k: v.clone() for k, v in init.items()}
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        sol = solve_implicit(prob, theta, eliminate="points", **opts)
+        loss = synthetic.differentiable_loss(sol, data)
+        e1.record()
+        grads = torch.autograd.grad(loss, theta)
+        e2.record()
+        torch.cuda.synchronize(device)
+        return float(loss), grads, e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
+
+    for _ in range(max(1, args.warmup)):
+        run(exact)
+    fw, bw = [], []
+    for _ in range(args.steps):
+        loss, grads, f_s, b_s = run(exact)
+        fw.append(f_s)
+        bw.append(b_s)
+    refine = list(solve_implicit.last.get("refinement_history", []))
+    mixed_opts = dict(linear_solver="schur_cg", termination=term,
+                      conjugate_gradient=tls.ConjugateGradientConfig(precision="mixed", rtol=1e-10))
+    _, grads_mixed, mixed_fs, mixed_bs = run(mixed_opts)
+    mixed_err = max(float((a - b).abs().max()) / max(float(b.abs().max()), 1e-300)
+                    for a, b in zip(grads_mixed, grads))
+
+    def loss_now():
+        prob.parameters = {k: v.clone() for k, v in init.items()}
+        prob.refresh_data()
+        prob.solve(eliminate="points", **exact)
+        return float(synthetic.differentiable_loss(newton_polish(prob, eliminate="points"), data))
+
+    gen = torch.Generator().manual_seed(0)
+    h = 1e-6
+    errs, errs_rich, mags = [], [], []
+
+    def central(flat, k, step):
+        with torch.no_grad():
+            base = float(flat[k])
+            flat[k] = base + step
+            lp = loss_now()
+            flat[k] = base - step
+            lm = loss_now()
+            flat[k] = base
+        return (lp - lm) / (2 * step)
+
+    for t, g, count in zip(theta, grads, (24, 8, 24, 8)):
+        flat, gflat = t.view(-1), g.reshape(-1)
+        for k in torch.randperm(flat.numel(), generator=gen)[:count].tolist():
+            d1 = central(flat, k, h)
+            d2 = central(flat, k, 2 * h)
+            rich = (4 * d1 - d2) / 3  # Richardson: cancels the O(h^2) truncation term
+            errs.append(abs(d1 - float(gflat[k])))
+            errs_rich.append(abs(rich - float(gflat[k])))
+            mags.append(abs(float(gflat[k])))
+    prob.refresh_data()
+    if rank != 0:
+        return
+    total = statistics.median(f + b for f, b in zip(fw, bw))
+    line = {
+        "metric": ADJ_METRIC, "value": total, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": "ba_adjoint_160k_obs", "cameras": 64, "points": 20_000, "observations": 160_000,
+                   "forward": "LM, schur_dense, float64, tight tolerances", "parallelism": f"replicas x{world}"},
+        "forward_s": statistics.median(fw), "backward_s": statistics.median(bw), "loss": loss,
+        "adjoint_refinement_residuals": refine,
+        "fd_coordinates": len(errs), "fd_step": h, "fd_solves": "LM then two exact Newton steps",
+        "fd_max_abs_error": max(errs), "fd_max_rel_error": max(errs) / max(mags),
+        "fd_richardson_max_rel_error": max(errs_rich) / max(mags),
+        "fd_rel_error_median": statistics.median(errs) / max(mags),
+        "mixed_forward": {"solver": "schur_cg rtol 1e-10, float32 W", "forward_s": mixed_fs, "backward_s": mixed_bs,
+                          "max_rel_gradient_difference_vs_fp64": mixed_err},
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- arms
 def run_reference(args, world, rank):
     if rank != 0:
@@ -422,6 +611,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "pose_graph":
+            run_pose(args, world, rank, local)
+        elif args.workload == "adjoint":
+            run_adjoint(args, world, rank, local)
         else:
             run_cuda(args, world, rank, local)
     finally:

@@ -83,6 +83,13 @@ class Problem:
             self._signature = signature
         return self._analyzed
 
+    def refresh_data(self) -> Problem:
+        """Re-read residual data and weights after in-place changes, keeping the
+        analysis (structure, Schur plans) of the unchanged sparsity pattern."""
+        if self._analyzed is not None:
+            self._analyzed.refresh_data()
+        return self
+
     def analyze(self) -> Problem:
         self._state(None)
         return self

@@ -77,15 +77,7 @@ class CostPlan:
             rows.append(pos)
         self.type_indices = tuple(types)
         self.indices = tuple(rows)
-        self.weights = None
-        if cost.weights is not None:
-            w = torch.as_tensor(cost.weights)
-            if w.ndim > 1 or w.numel() not in (1, self.count) or w.is_complex():
-                raise ValueError("Weights must be a real scalar or one value per observation")
-            w = torch.as_tensor(cost.weights, dtype=torch.float64).detach().reshape(-1)
-            if not bool((torch.isfinite(w) & (w >= 0)).all()):
-                raise ValueError("Weights must be finite and nonnegative")
-            self.weights = w.cpu().expand(self.count).clone()
+        self._read_weights()
         for i, arg in enumerate(cost.args):
             if _is_ref(arg):
                 axis = 0 if as_ids(arg.id).ndim == 1 else None
@@ -98,6 +90,23 @@ class CostPlan:
         self._linearizers = {}
         self._batch = {}
         self._device_data = {}
+
+    def _read_weights(self):
+        cost = self.cost
+        self.weights = None
+        if cost.weights is not None:
+            w = torch.as_tensor(cost.weights)
+            if w.ndim > 1 or w.numel() not in (1, self.count) or w.is_complex():
+                raise ValueError("Weights must be a real scalar or one value per observation")
+            w = torch.as_tensor(cost.weights, dtype=torch.float64).detach().reshape(-1)
+            if not bool((torch.isfinite(w) & (w >= 0)).all()):
+                raise ValueError("Weights must be finite and nonnegative")
+            self.weights = w.cpu().expand(self.count).clone()
+
+    def refresh_data(self):
+        """Re-read weights and data tensors (changed in place); indices stay."""
+        self._read_weights()
+        self._device_data = {k: v for k, v in self._device_data.items() if k[0] == "rows"}
 
     def data_axis(self, i, tensor):
         if self.cost.in_dims is not None:
@@ -332,6 +341,12 @@ class AnalyzedLeastSquaresProblem:
         self.plans = tuple(CostPlan(c, layout) for c in costs)
         self._has_loss = any(p.cost.loss is not None or p.cost.weights is not None for p in self.plans)
         self._structures = {}
+
+    def refresh_data(self):
+        """Data tensors or weights of the residuals were changed in place: drop
+        the cached device copies (the symbolic analysis and plans stay)."""
+        for plan in self.plans:
+            plan.refresh_data()
 
     # ------------------------------------------------------------------ values
     def _validate_values(self, vals):

@@ -79,7 +79,15 @@ def point_prior(point: Tensor, reference: Tensor) -> Tensor:
 
 
 reprojection.cuda_residual = "reprojection"
+def camera_distance_prior(camera: Tensor, reference: Tensor, distance: Tensor) -> Tensor:
+    """|c - c_ref| - distance for world-to-camera poses (c = -R^T t): fixes the
+    global scale of a bundle adjustment whose first camera is held fixed."""
+    c = -(camera[:3, :3].transpose(-1, -2) @ camera[:3, 3])
+    c0 = -(reference[:3, :3].transpose(-1, -2) @ reference[:3, 3])
+    return (torch.linalg.vector_norm(c - c0) - distance).reshape(1)
+
+
 se3_between.cuda_residual = "se3_between"
 sim3_between.cuda_residual = "sim3_between"
 
-__all__ = ["point_prior", "reprojection", "se3_between", "sim3_between", "sim3_inverse", "sim3_log"]
+__all__ = ["camera_distance_prior", "point_prior", "reprojection", "se3_between", "sim3_between", "sim3_inverse", "sim3_log"]

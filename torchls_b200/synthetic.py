@@ -173,6 +173,56 @@ def build_bundle_adjustment(data: BundleAdjustmentData, api, *, device="cpu", dt
     return problem
 
 
+def build_differentiable_bundle_adjustment(data: BundleAdjustmentData, api, *, device="cpu", dtype=torch.float64,
+                                           loss=None, residual=None):
+    """Bundle adjustment with camera 0 fixed, per-observation weights and a
+    scale prior (distance of camera 1 from camera 0 at its true value), so
+    the solution is an isolated minimum and can be differentiated.
+
+    Returns ``(problem, inputs)``; ``inputs`` holds the observation and weight
+    tensors used by the problem ("uv_free", "uv_fixed", "w_free", "w_fixed").
+    """
+    if residual is None:
+        from .residuals import reprojection as residual
+    from .residuals import camera_distance_prior
+
+    free, fixed = data.split_fixed_camera()
+    problem = api.Problem(
+        {
+            "cams": data.cameras_init[1:].to(device=device, dtype=dtype),
+            "points": data.points_init.to(device=device, dtype=dtype),
+        },
+        manifolds={"cams": api.SE3Var},
+    )
+    inputs = {
+        "uv_free": data.uv[free].to(device=device, dtype=dtype).clone(),
+        "uv_fixed": data.uv[fixed].to(device=device, dtype=dtype).clone(),
+        "w_free": torch.ones(int(free.sum()), device=device, dtype=dtype),
+        "w_fixed": torch.ones(int(fixed.sum()), device=device, dtype=dtype),
+    }
+    problem.add_residual(residual, ("cams", data.camera_index[free] - 1), ("points", data.point_index[free]),
+                         inputs["uv_free"], loss=loss, weights=inputs["w_free"])
+    problem.add_residual(residual, data.cameras_true[0].to(device=device, dtype=dtype),
+                         ("points", data.point_index[fixed]), inputs["uv_fixed"], in_dims=(None, 0, 0), loss=loss,
+                         weights=inputs["w_fixed"])
+    c = lambda T: -(T[:3, :3].T @ T[:3, 3])  # noqa: E731
+    dist = torch.linalg.vector_norm(c(data.cameras_true[1]) - c(data.cameras_true[0])).reshape(())
+    problem.add_residual(camera_distance_prior, ("cams", torch.tensor([0])),
+                         data.cameras_true[0].to(device=device, dtype=dtype), dist.to(device=device, dtype=dtype),
+                         in_dims=(0, None, None))
+    return problem, inputs
+
+
+def differentiable_loss(solution, data: BundleAdjustmentData) -> Tensor:
+    """Mean squared distance of the solved points to the true points plus the
+    squared translation error of the solved (free) camera poses."""
+    pts = solution["points"]
+    cams = solution["cams"]
+    pt = data.points_true.to(pts)
+    ct = data.cameras_true[1:].to(cams)
+    return ((pts - pt) ** 2).sum(-1).mean() + ((cams[:, :3, 3] - ct[:, :3, 3]) ** 2).sum()
+
+
 @dataclass
 class PoseGraphData:
     poses_true: Tensor  # [N, 4, 4]
