@@ -1,0 +1,406 @@
+"""Many independent least-squares problems solved together on one GPU.
+
+``solve_batched(problems)`` merges problems with the same parameter groups and
+residual batches into one block-diagonal problem and runs Levenberg-Marquardt
+with PER-PROBLEM damping, acceptance and convergence:
+
+* one linearization, Schur elimination and reduced-system PCG for all
+  problems per trial (every kernel launch covers every problem), the PCG with
+  per-problem alpha, beta, tolerance and convergence mask (segmented dot
+  products), so each problem's CG runs as if alone;
+* per-problem damping lambda_p enters as a column scale 1/sqrt(lambda_p) with
+  unit damping: (s A s + I) y = s b, x = s y equals (A + lambda_p I) x = b on
+  each diagonal block, so the shared kernels need no per-problem parameter;
+* per-problem trial cost, exact reduction (Huber divided difference),
+  predicted reduction and gain ratio are fixed-order segmented sums
+  (``tls_segment_reduce``) over each problem's factors and tangent entries;
+* accepted problems keep their new values and wait for the next
+  linearization; rejected ones raise lambda_p and are solved again in the
+  next trial (the others contribute a zero right-hand side, so their blocks
+  of the PCG iterate stay zero); converged or failed problems leave the
+  active mask.
+
+Per-problem LM decisions follow torchls solvers.py:288-696 (fixed-factor
+damping, step quality 1e-4, cost and gradient tolerances); the per-problem
+CG stops on its recurrence residual (no true-residual restarts).
+"""
+
+from __future__ import annotations
+
+import math
+from collections.abc import Sequence
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from . import _lib as L
+from .kernels import segment_reduce
+from .losses import HuberLoss
+from .named import Problem
+from .variables import NamedValues, ParameterRef
+
+__all__ = ["BatchedProblem", "BatchedSummary", "merge_problems", "solve_batched"]
+
+
+def merge_problems(problems: Sequence[Problem]):
+    """One block-diagonal ``Problem`` from problems with identical parameter
+    groups (names, manifolds, trailing shapes) and residual batches (same
+    function, loss and argument kinds at each position).
+
+    Returns ``(merged, var_problem, slices)``: ``var_problem[name]`` is the
+    problem id of each variable of group ``name``; ``slices[p][name]`` the
+    rows of problem p in that group.
+    """
+    if not problems:
+        raise ValueError("no problems to merge")
+    first = problems[0]
+    names = list(first.parameters)
+    for p in problems:
+        if list(p.parameters) != names or dict(p.manifolds) != dict(first.manifolds):
+            raise ValueError("problems must share parameter groups and manifolds")
+        if len(p._costs) != len(first._costs):
+            raise ValueError("problems must share residual batches")
+    counts = {n: [int(p.parameters[n].shape[0]) for p in problems] for n in names}
+    offsets = {n: np.concatenate(([0], np.cumsum(counts[n]))) for n in names}
+    params = {n: torch.cat([p.parameters[n] for p in problems]) for n in names}
+    merged = Problem(params, manifolds=dict(first.manifolds))
+    for k, c0 in enumerate(first._costs):
+        cs = [p._costs[k] for p in problems]
+        if any(c.residual_fn is not c0.residual_fn or type(c.loss) is not type(c0.loss) for c in cs):
+            raise ValueError(f"residual batch {k} differs between problems")
+        n_obs = [_count(c) for c in cs]
+        args, dims = [], []
+        for i, a0 in enumerate(c0.args):
+            if isinstance(a0, ParameterRef):
+                ids = torch.cat([torch.as_tensor(c.args[i].id).reshape(-1) + int(offsets[a0.name][j])
+                                 for j, c in enumerate(cs)])
+                args.append((a0.name, ids))
+                dims.append(0)
+            else:
+                axis = c0.in_dims[i] if c0.in_dims is not None else (0 if torch.as_tensor(a0).ndim > 0 else None)
+                parts = []
+                for c, n in zip(cs, n_obs):
+                    t = torch.as_tensor(c.args[i])
+                    parts.append(t.unsqueeze(0).expand(n, *t.shape) if axis is None else t)
+                args.append(torch.cat(parts))
+                dims.append(0)
+        weights = None
+        if c0.weights is not None:
+            weights = torch.cat([torch.as_tensor(c.weights, dtype=torch.float64).reshape(-1).expand(n)
+                                 for c, n in zip(cs, n_obs)])
+        merged.add_residual(c0.residual_fn, *args, in_dims=tuple(dims), loss=c0.loss, weights=weights,
+                            jac_mode=c0.jac_mode)
+    var_problem = {n: torch.repeat_interleave(torch.arange(len(problems)), torch.tensor(counts[n])) for n in names}
+    slices = [{n: slice(int(offsets[n][j]), int(offsets[n][j + 1])) for n in names} for j in range(len(problems))]
+    return merged, var_problem, slices
+
+
+def _count(cost) -> int:
+    for a in cost.args:
+        if isinstance(a, ParameterRef):
+            ids = torch.as_tensor(a.id)
+            if ids.ndim == 1:
+                return int(ids.numel())
+    raise ValueError("each residual batch needs a batched parameter reference")
+
+
+@dataclass
+class BatchedSummary:
+    problems: int
+    iterations: int = 0
+    linear_solves: int = 0
+    linear_iterations: int = 0
+    initial_cost: Tensor | None = None
+    final_cost: Tensor | None = None
+    accepted_steps: Tensor | None = None
+    rejected_steps: Tensor | None = None
+    termination: list = field(default_factory=list)
+
+
+class _Segments:
+    """Fixed-order per-problem sums of a float64 vector (CSR over element ids)."""
+
+    def __init__(self, pid: Tensor, nproblems: int, device):
+        pid = pid.to(torch.int64).cpu()
+        order = torch.argsort(pid, stable=True)
+        ptr = torch.zeros(nproblems + 1, dtype=torch.int64)
+        ptr[1:] = torch.cumsum(torch.bincount(pid, minlength=nproblems), 0)
+        self.ptr = ptr.to(device=device, dtype=torch.int32)
+        self.src = order.to(device=device, dtype=torch.int32)
+        mean = float(pid.numel()) / max(nproblems, 1)
+        lanes = 256 if mean > 64 else (32 if mean > 16 else 8)
+        self.seg = L.Segments(nproblems, 1, lanes, 0, self.ptr.data_ptr(), self.src.data_ptr())
+        self.n = nproblems
+        self.pid = pid.to(device)
+
+    def sum(self, x: Tensor) -> Tensor:
+        out = torch.empty(self.n, dtype=torch.float64, device=x.device)
+        return segment_reduce(self.seg, x.to(torch.float64).contiguous(), out)
+
+
+def _batched_pcg(matvec, precond, b: Tensor, seg: _Segments, pid: Tensor, rtol: float, atol: float,
+                 max_iterations: int, check_every: int = 4):
+    """Preconditioned CG with per-problem scalars on a block-diagonal operator:
+    each problem p has its own alpha_p, beta_p, threshold max(atol, rtol |b_p|)
+    and convergence mask; the operator and preconditioner launches cover all
+    problems, converged problems keep a zero direction. Returns (x, iterations
+    per problem)."""
+    x = torch.zeros_like(b)
+    r = b.clone()
+    z = precond(r)
+    p = z.clone()
+    rz = seg.sum(r * z)
+    bn = seg.sum(b * b).sqrt()
+    thr = torch.clamp(rtol * bn, min=atol)
+    active = bn > thr
+    its = torch.zeros(seg.n, dtype=torch.int64, device=b.device)
+    for it in range(max_iterations):
+        if it % check_every == 0 and not bool(active.any()):
+            break
+        ap = matvec(p)
+        pap = seg.sum(p * ap)
+        ok = active & (pap > 0) & torch.isfinite(pap)
+        alpha = torch.where(ok, rz / torch.where(ok, pap, torch.ones_like(pap)), torch.zeros_like(pap))
+        at = alpha[pid]
+        x = x + at * p
+        r = r - at * ap
+        its += active.to(torch.int64)
+        rr = seg.sum(r * r)
+        active = ok & (rr.sqrt() > thr)
+        z = precond(r)
+        rz_new = seg.sum(r * z)
+        beta = torch.where(active, rz_new / torch.where(active, rz, torch.ones_like(rz)), torch.zeros_like(rz))
+        p = (z + beta[pid] * p) * active[pid].to(z.dtype)
+        rz = rz_new
+    return x, its
+
+
+def _huber_terms(loss, s_old, s_new, sqdiff):
+    """Per-factor rho(s_new) and the exact reduction rho(s_old) - rho(s_new)
+    (torchls losses.py:92-107: (a-b)(a+b) for the quadratic part, a divided
+    difference across the kink)."""
+    if loss is None:
+        return s_new, sqdiff
+    if isinstance(loss, HuberLoss):
+        d = loss.delta
+        d2 = d * d
+        n_old, n_new = s_old.clamp_min(0).sqrt(), s_new.clamp_min(0).sqrt()
+        rho_new = torch.where(s_new > d2, d * (2 * n_new - d), s_new)
+        rho_old = torch.where(s_old > d2, d * (2 * n_old - d), s_old)
+        both_in = (s_old <= d2) & (s_new <= d2)
+        both_out = (s_old > d2) & (s_new > d2)
+        red = torch.where(both_in, sqdiff, rho_old - rho_new)
+        red = torch.where(both_out, 2 * d * sqdiff / (n_old + n_new).clamp_min(1e-300), red)
+        return rho_new, red
+    rho_new = loss.evaluate(s_new)[0]
+    rho_old = loss.evaluate(s_old)[0]
+    return rho_new, rho_old - rho_new
+
+
+class BatchedProblem:
+    """Independent problems merged once (structure, segments and Schur plan
+    are analysed here) and solved many times with :meth:`solve`."""
+
+    def __init__(self, problems: Sequence[Problem], *, eliminate: str | None = "points"):
+        from .schur import SchurPlan
+
+        self.merged, self.var_problem, self.slices = merge_problems(problems)
+        self.P = len(problems)
+        self.eliminate = eliminate
+        an, vals = self.merged._state(None)
+        self.device = vals.device
+        L.require_cuda(next(iter(vals._values.values())), "batched solve")
+        self.initial = {k: v.clone() for k, v in self.merged.parameters.items()}
+        layout = an.layout
+        P, device = self.P, self.device
+        # problem id per tangent entry and per factor (structure order)
+        self.pid_t = torch.cat([self.var_problem[e.key].repeat_interleave(e.dim) for e in layout]).to(device)
+        pid_f = []
+        for plan in an.plans:
+            for a in plan.cost.args:
+                if isinstance(a, ParameterRef):
+                    pid_f.append(self.var_problem[a.name][torch.as_tensor(a.id)])
+                    break
+        self.pid_f = torch.cat(pid_f).to(device)
+        self.seg_t, self.seg_f = _Segments(self.pid_t, P, device), _Segments(self.pid_f, P, device)
+        an.structure(device)
+        self.plan = SchurPlan(an, eliminate, device) if eliminate is not None else None
+        if self.plan is not None:
+            self.pid_red = self.pid_t[self.plan.r.offset : self.plan.r.offset + self.plan.dim].contiguous()
+            self.seg_red = _Segments(self.pid_red, P, device)
+            self.plan.chunks_for(torch.float32)
+            self.plan.chunks_for(torch.float64)
+
+    def reset(self):
+        """Restore the initial values of every problem."""
+        self.merged.parameters = {k: v.clone() for k, v in self.initial.items()}
+
+    def solve(self, *, precision: str = "native", max_iterations: int = 20, lambda_initial: float = 1e-3,
+              lambda_factor: float = 4.0, lambda_min: float = 1e-12, lambda_max: float = 1e12,
+              step_quality_min: float = 1e-4, max_trials: int = 20, cost_tolerance: float = 1e-10,
+              gradient_tolerance: float = 1e-8, pcg_rtol: float = 1e-6, pcg_max_iterations: int = 200):
+        """LM over every problem from the current values (see the module
+        docstring). Returns ``(solutions, summary)``: one dict of solved
+        parameters per problem and a :class:`BatchedSummary` with per-problem
+        costs, step counts and termination reasons ("gradient_tolerance",
+        "cost_tolerance", "max_iterations", "trials_exhausted")."""
+        from .schur import SchurLinearization
+        from .solvers import BlockJacobiPreconditioner, ConjugateGradientConfig, DevicePCG
+
+        merged, var_problem, slices, P = self.merged, self.var_problem, self.slices, self.P
+        an, vals = merged._state(None)
+        layout, device, n = an.layout, self.device, an.tangent_dim
+        jdt = torch.float32 if precision == "mixed" else torch.float64
+        pid_t, seg_t, seg_f = self.pid_t, self.seg_t, self.seg_f
+        st = an.structure(device)
+        plan = self.plan
+        if plan is not None:
+            pid_red, seg_red = self.pid_red, self.seg_red
+        cg = ConjugateGradientConfig(rtol=pcg_rtol, max_iterations=pcg_max_iterations, precision=precision)
+        pcg_ws = DevicePCG(plan.dim if plan is not None else n, torch.float64, device)
+        def factor_sums(rows: Tensor) -> Tensor:
+            """Per-factor sums of squares of factor-major rows [sum N_k r_k]."""
+            parts = []
+            for k in range(len(an.plans)):
+                R, N, rb = st.rdims[k], an.plans[k].count, st.res_base[k]
+                v = rows[rb : rb + N * R].view(N, R)
+                parts.append((v * v).sum(-1))
+            return torch.cat(parts)
+
+        def objective_terms(lin, new_raw):
+            """Per-factor new objective 1/2 w rho(s_new) and exact reduction."""
+            old_raw = lin.raw_residual if an._has_loss else lin.residual
+            objs, reds = [], []
+            for k, p in enumerate(an.plans):
+                R, N, rb = st.rdims[k], p.count, st.res_base[k]
+                ro, rn = old_raw[rb : rb + N * R].view(N, R), new_raw[rb : rb + N * R].view(N, R)
+                s_old, s_new = (ro * ro).sum(-1), (rn * rn).sum(-1)
+                sqdiff = ((ro - rn) * (ro + rn)).sum(-1)
+                obj, red = _huber_terms(p.cost.loss, s_old, s_new, sqdiff)
+                if p.weights is not None:
+                    w = p.weights.to(device)
+                    obj, red = w * obj, w * red
+                objs.append(obj)
+                reds.append(red)
+            return 0.5 * torch.cat(objs), 0.5 * torch.cat(reds)
+
+        def masked(values: NamedValues, proposed: NamedValues, accept: Tensor) -> NamedValues:
+            out = {}
+            for e in layout:
+                a = accept[var_problem[e.key].to(device)]
+                a = a.view(-1, *([1] * (proposed._values[e.key].ndim - 1)))
+                out[e.key] = torch.where(a, proposed._values[e.key], values._values[e.key])
+            return NamedValues(out, layout)
+
+        lam = torch.full((P,), float(lambda_initial), dtype=torch.float64, device=device)
+        active = torch.ones(P, dtype=torch.bool, device=device)
+        reason = ["max_iterations"] * P
+        accepted = torch.zeros(P, dtype=torch.int64, device=device)
+        rejected = torch.zeros(P, dtype=torch.int64, device=device)
+        summary = BatchedSummary(problems=P)
+
+        lin = merged.linearize(dict(vals._values), jacobian_dtype=jdt, schur=plan)
+        first_obj, _ = objective_terms(lin, lin.raw_residual if an._has_loss else lin.residual)
+        cost = seg_f.sum(first_obj)
+        summary.initial_cost = cost.clone()
+        for it in range(max_iterations):
+            g = lin.gradient
+            gmax = torch.zeros(P, dtype=torch.float64, device=device).scatter_reduce(0, pid_t, g.abs(), "amax")
+            done_g = active & (gmax <= gradient_tolerance)
+            for j in torch.nonzero(done_g).flatten().tolist():
+                reason[j] = "gradient_tolerance"
+            active &= ~done_g
+            if not bool(active.any()):
+                break
+            summary.iterations += 1
+            raw_diag = lin.jacobian.diagonal_blocks()
+            pending = active.clone()
+            any_accept = False
+            for _ in range(max_trials):
+                if not bool(pending.any()):
+                    break
+                s = (1.0 / lam.sqrt())[pid_t]
+                mask = pending[pid_t].to(torch.float64)
+                tried = pending.clone()
+                if plan is not None:
+                    slin = SchurLinearization(plan, lin, raw_diag, s, wdtype=jdt, vec_dtype=torch.float64)
+                    system = slin.damped(1.0)
+                    # Schur preconditioner blocks that are not positive definite reject
+                    # their problem's trial (lambda_p grows); an identity block stands in
+                    blocks = system.preconditioner_blocks()
+                    eye = torch.eye(plan.dr, dtype=torch.float64, device=device)
+                    info = torch.linalg.cholesky_ex(blocks + eye)[1]
+                    bad_block = info > 0
+                    if bool(bad_block.any()):
+                        first_col = plan.r.offset + torch.arange(plan.r.count, device=device) * plan.dr
+                        badp = torch.zeros(P, dtype=torch.bool, device=device)
+                        badp[pid_t[first_col[bad_block]]] = True
+                        badp &= pending
+                        lam = torch.where(badp, (lam * lambda_factor).clamp_max(lambda_max), lam)
+                        rejected += badp.to(torch.int64)
+                        mask = mask * (~badp)[pid_t].to(torch.float64)
+                        tried &= ~badp
+                        blocks = torch.where(bad_block[:, None, None], eye.expand_as(blocks), blocks)
+                    pre = BlockJacobiPreconditioner.from_blocks([(blocks, [(0, plan.dr)], plan.r.count, plan.dr)], 1.0,
+                                                                None, plan.dim)
+                    rhs = system.reduced_rhs(-(g * s) * mask)
+                    xc, its = _batched_pcg(system.matvec, pre, rhs, seg_red, pid_red, pcg_rtol, 1e-10,
+                                           pcg_max_iterations)
+                    if int(plan.err.item()) != 0:
+                        raise RuntimeError("Schur matvec: a bounded device wait timed out")
+                    delta = s * system.backsubstitute(xc)
+                    n_its = int(its.max())
+                else:
+                    from .solvers import _layout_specs
+
+                    scaled = lin.jacobian.scale_columns(s)
+                    pre = BlockJacobiPreconditioner.from_blocks(_layout_specs(layout, raw_diag), 1.0, s, n)
+                    res = pcg_ws.run(-(g * s) * mask, cg, normal_args=scaled.normal_args(torch.float64, 1.0),
+                                     preconditioner=pre)
+                    delta = s * res.solution.to(torch.float64)
+                    n_its = int(res.iterations)
+                summary.linear_solves += 1
+                summary.linear_iterations += n_its
+                delta = delta * mask
+                proposed = vals.retract(delta, layout)
+                new_raw = an.residuals(proposed)
+                obj_new, red = objective_terms(lin, new_raw)
+                actual = seg_f.sum(red)
+                jd = lin.jacobian.matvec(delta)
+                predicted = -seg_t.sum(g * delta) - 0.5 * seg_f.sum(factor_sums(jd.to(torch.float64)))
+                quality = torch.where(predicted > 0, actual / predicted, torch.full_like(actual, -math.inf))
+                new_cost = seg_f.sum(obj_new)
+                ok = tried & torch.isfinite(new_cost) & (actual > 0) & (quality >= step_quality_min)
+                vals = masked(vals, proposed, ok)
+                cost = torch.where(ok, new_cost, cost)
+                up = ok & (quality > 0.75)
+                lam = torch.where(up, (lam / lambda_factor).clamp_min(lambda_min), lam)
+                bad = tried & ~ok
+                lam = torch.where(bad, (lam * lambda_factor).clamp_max(lambda_max), lam)
+                accepted += ok.to(torch.int64)
+                rejected += bad.to(torch.int64)
+                conv = ok & (actual.abs() <= cost_tolerance * (cost + actual).clamp_min(1e-300))
+                for j in torch.nonzero(conv).flatten().tolist():
+                    reason[j] = "cost_tolerance"
+                active &= ~conv
+                pending &= ~ok
+                any_accept = any_accept or bool(ok.any())
+            for j in torch.nonzero(pending).flatten().tolist():
+                reason[j] = "trials_exhausted"
+            active &= ~pending
+            if any_accept:
+                lin = merged.linearize(dict(vals._values), jacobian_dtype=jdt, schur=plan)
+        summary.final_cost = cost
+        summary.accepted_steps = accepted
+        summary.rejected_steps = rejected
+        summary.termination = reason
+        merged.parameters.update(dict(vals._values))
+        sols = [{k: vals._values[k][sl[k]] for k in vals._values} for sl in slices]
+        return sols, summary
+
+
+def solve_batched(problems: Sequence[Problem], *, eliminate: str | None = "points", **options):
+    """Merge ``problems`` (see :class:`BatchedProblem`) and solve them once."""
+    return BatchedProblem(problems, eliminate=eliminate).solve(**options)

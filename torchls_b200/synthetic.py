@@ -223,6 +223,19 @@ def differentiable_loss(solution, data: BundleAdjustmentData) -> Tensor:
     return ((pts - pt) ** 2).sum(-1).mean() + ((cams[:, :3, 3] - ct[:, :3, 3]) ** 2).sum()
 
 
+def batched_bundle_adjustment(count: int = 4096, first_seed: int = 0) -> list[BundleAdjustmentData]:
+    """Independent problems of uneven size, one per seed: cameras uniform in
+    {2..32}, points log-uniform in [20, 2000], each point seen by min(6,
+    cameras) distinct cameras (about 2.3M observations for 4,096 problems)."""
+    out = []
+    for seed in range(first_seed, first_seed + count):
+        g = torch.Generator().manual_seed(1_000_003 * seed + 17)
+        cams = int(torch.randint(2, 33, (1,), generator=g))
+        pts = int(round(math.exp(math.log(20) + (math.log(2000) - math.log(20)) * float(torch.rand(1, generator=g)))))
+        out.append(make_bundle_adjustment(cams, pts, min(6, cams), seed=seed))
+    return out
+
+
 @dataclass
 class PoseGraphData:
     poses_true: Tensor  # [N, 4, 4]
