@@ -34,10 +34,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "BA solve s to rel-cost 1e-8 (mixed vs FP64 CUDA); normal-matvec HBM GB/s vs peak"
 TARGET_FILE = os.path.join(ROOT, "tests", "golden", "ba_mid_target.json")
-# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the persistent
-# Schur-PCG kernel in the roofline measurement (100 iterations on the 1M-observation
-# reduced system); None until captured.
-NCU_TRAFFIC_BYTES = None
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the persistent
+# Schur-PCG kernel in the roofline measurement (100 iterations + 3 residual checks
+# on the 1M-observation reduced system): 5.713 GB + 0.317 GB
+# (profiles/schur_pcg_kernel_ba_mid_1M.md).
+NCU_TRAFFIC_BYTES = 6_030_313_488
 
 
 def parse():
