@@ -529,12 +529,16 @@ def run_batched(args, world, rank, local):
     extrapolated to 4,096)."""
     import torchls_b200 as tls
     from torchls_b200 import synthetic
-    from torchls_b200.batched import BatchedProblem
+    from torchls_b200.batched import BatchedProblem, partition_problems
 
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    datas = synthetic.batched_bundle_adjustment(4096, first_seed=0)
-    obs = sum(d.num_observations for d in datas)
+    all_datas = synthetic.batched_bundle_adjustment(4096, first_seed=0)
+    obs = sum(d.num_observations for d in all_datas)
+    # several GPUs: each rank solves its share of the problems (by observation
+    # count); no data-path exchange, timing is the max over ranks
+    mine = partition_problems([d.num_observations for d in all_datas], world)[rank]
+    datas = [all_datas[j] for j in mine]
 
     def build(d):
         return synthetic.build_bundle_adjustment(d, tls, device=device, loss=tls.HuberLoss(0.01))
@@ -561,9 +565,10 @@ def run_batched(args, world, rank, local):
         for _ in range(args.steps):
             t, summ = batched_once("mixed")
             times.append(t)
-    batched_s = statistics.median(times)
+    batched_s = dist_max(statistics.median(times), world, device)
     t64, summ64 = batched_once("native")
-    sample = list(range(0, 4096, 64))
+    t64 = dist_max(t64, world, device)
+    sample = list(range(0, 4096, 64)) if world == 1 else []
     single, diffs = [], []
     opts = dict(linear_solver="schur_cg", eliminate="points", return_summary=True,
                 conjugate_gradient=tls.ConjugateGradientConfig(precision="mixed"),
@@ -581,7 +586,8 @@ def run_batched(args, world, rank, local):
         torch.cuda.synchronize(device)
         single.append(e0.elapsed_time(e1) / 1e3)
         diffs.append(abs(float(summ.final_cost[j]) - s.final_cost) / max(s.final_cost, 1e-300))
-    per_problem_s = sum(single) / len(single) * 4096
+    per_problem_s = sum(single) / len(single) * 4096 if single else None
+    barrier(world)
     if rank != 0:
         return
     reasons = {}
@@ -592,11 +598,11 @@ def run_batched(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": batched_s * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
         "config": {"workload": "ba_batched_4096", "problems": 4096, "observations": obs,
-                   "max_lm_iterations": 20, "parallelism": f"replicas x{world}"},
+                   "max_lm_iterations": 20, "parallelism": f"problems sharded x{world}"},
         "fp64_s": t64, "analysis_s": analysis_s, "one_solve_per_problem_s": per_problem_s,
-        "one_solve_per_problem_sample": f"{len(sample)} problems (every 64th seed), mean x 4096",
-        "speedup_vs_one_solve_per_problem": per_problem_s / batched_s,
-        "max_rel_cost_difference_vs_individual_solves": max(diffs),
+        "one_solve_per_problem_sample": f"{len(sample)} problems (every 64th seed), mean x 4096" if single else None,
+        "speedup_vs_one_solve_per_problem": per_problem_s / batched_s if single else None,
+        "max_rel_cost_difference_vs_individual_solves": max(diffs) if diffs else None,
         "batched_iterations": summ.iterations, "linear_solves": summ.linear_solves,
         "pcg_iterations": summ.linear_iterations, "termination": reasons, "clocks": clocks.summary(),
     }

@@ -41,7 +41,7 @@ from .losses import HuberLoss
 from .named import Problem
 from .variables import NamedValues, ParameterRef
 
-__all__ = ["BatchedProblem", "BatchedSummary", "merge_problems", "solve_batched"]
+__all__ = ["BatchedProblem", "BatchedSummary", "merge_problems", "partition_problems", "solve_batched"]
 
 
 def merge_problems(problems: Sequence[Problem]):
@@ -404,3 +404,21 @@ class BatchedProblem:
 def solve_batched(problems: Sequence[Problem], *, eliminate: str | None = "points", **options):
     """Merge ``problems`` (see :class:`BatchedProblem`) and solve them once."""
     return BatchedProblem(problems, eliminate=eliminate).solve(**options)
+
+
+def partition_problems(work: Sequence[float], parts: int) -> list[list[int]]:
+    """Split problems across ``parts`` GPUs by estimated work (for example
+    observations x iterations): longest-processing-time first, each problem to
+    the currently lightest part; ties go to the lowest part index, so every
+    rank computes the same partition. Problems solve independently, so the
+    only exchange is gathering the solutions at the end."""
+    if parts < 1:
+        raise ValueError("parts must be positive")
+    order = sorted(range(len(work)), key=lambda j: (-float(work[j]), j))
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for j in order:
+        k = min(range(parts), key=lambda i: (load[i], i))
+        out[k].append(j)
+        load[k] += float(work[j])
+    return [sorted(o) for o in out]
