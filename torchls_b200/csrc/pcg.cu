@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(256) pcg_init_finish_kernel(PcgState* st, cons
   st->ticket_op = 0;
   st->ticket_upd = 0;
   st->bar_count = 0;
+  st->bar_count2 = 0;
   if (!isfinite(nrm)) {
     c.status = TLS_PCG_NONFINITE;
     c.mode = M_DONE;

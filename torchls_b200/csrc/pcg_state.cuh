@@ -23,6 +23,8 @@ struct PcgState {
   uint32_t ticket_upd;
   uint32_t bar_count;    // grid barrier of the persistent Schur-PCG kernel
   uint32_t bar_gen;
+  uint32_t bar_count2;   // arrivals the vector CTA waits for (persistent kernel)
+  uint32_t pad2_;
 };
 
 // Deterministic sum of p[0..n) by one block (fixed strided order, fixed tree).

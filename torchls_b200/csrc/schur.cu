@@ -576,6 +576,222 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
   __syncthreads();
 }
 
+// Variant for small reduced systems: the LAST CTA is a "vector CTA" that
+// keeps x, r, z, p, psave and Ap of the PCG in its shared memory (where the
+// other CTAs keep chunk slabs) and runs the whole vector phase; the other
+// CTAs stream the chunks and gather. Per step:
+//   A  chunk CTAs: chunk partials of A p            -- barrier over chunk CTAs --
+//   B  chunk CTAs: gather Ap and x.Ap partials, then arrive at the vector CTA
+//   C  vector CTA (after every arrival): curvature and alpha, update,
+//      preconditioner, decision, direction in shared memory; publishes p and
+//      the control block, then releases the chunk CTAs.
+// The arithmetic (and its order) is that of schur_pcg_kernel. Every wait is
+// bounded; on timeout the kernel flags a.err and every CTA leaves.
+template <int DR, int DE, int CAP, typename TW, int D>
+__global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schur_args a, PcgLoop q) {
+  using TA = double;
+  using S = SlabShape<DR, DE, CAP, TW, TA>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double sm[8][DR];
+  __shared__ double ux[DR * DR];
+  __shared__ double smd[kChunkThreads / 32];
+  __shared__ int s_go, s_ok, last;
+  __shared__ uint32_t gen0;
+  const int tid = threadIdx.x;
+  PcgState* st = q.st;
+  const int G = (int)gridDim.x - 1;  // chunk CTAs
+  const bool vcta = (int)blockIdx.x == G;
+  if (vcta) {
+    // ---------------- the vector CTA
+    const int64_t n = q.n;
+    double* x = reinterpret_cast<double*>(smem);
+    double* r = x + n;
+    double* z = r + n;
+    double* p = z + n;
+    double* psave = p + n;
+    double* ap = psave + n;
+    for (int64_t i = tid; i < n; i += kChunkThreads) {
+      x[i] = q.x[i];
+      r[i] = q.r[i];
+      z[i] = q.z[i];
+      p[i] = q.p[i];
+      psave[i] = q.psave[i];
+    }
+    __syncthreads();
+    for (int step = 0; step < q.steps; ++step) {
+      if (tid == 0) s_go = st->pub.status == TLS_PCG_ACTIVE && st->pub.mode != M_DONE;
+      __syncthreads();
+      if (!s_go) break;
+      // wait until every chunk CTA has gathered its variables
+      if (tid == 0) {
+        s_ok = 1;
+        volatile uint32_t* cnt = &st->bar_count2;
+        const long long t0 = clock64();
+        while (*cnt != (uint32_t)G) {
+          __nanosleep(32);
+          if (clock64() - t0 > (1LL << 31)) {
+            if (a.err) atomicExch(a.err, 2);
+            s_ok = 0;
+            break;
+          }
+        }
+        __threadfence();
+      }
+      __syncthreads();
+      if (!s_ok) break;
+      for (int64_t i = tid; i < n; i += kChunkThreads) ap[i] = __ldcg(q.ap + i);
+      tls_pcg_control& c = st->pub;
+      const int mode = c.mode;
+      if (c.status == TLS_PCG_ACTIVE && mode == M_ITER) {
+        const double curv = block_sum_cg<kChunkThreads>(q.dots, a.nretained, smd);
+        if (tid == 0) {
+          const double rz = c.rz;
+          c.curvature = curv;
+          const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
+          st->alpha_ok = ok;
+          c.alpha = ok ? rz / curv : 0.0;
+        }
+      }
+      __syncthreads();
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
+      double alpha = 0.0;
+      if (work && mode == M_ITER) {
+        if (!st->alpha_ok) work = false;
+        else alpha = c.alpha;
+      }
+      if (work)
+        pcg_update_blocks<D, double, false>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, x, r, z, p, ap,
+                                            q.ztrue, a0, a1, a2);
+      const double t0 = block_sum<kChunkThreads>(a0, smd);
+      const double t1 = block_sum<kChunkThreads>(a1, smd);
+      const double t2 = block_sum<kChunkThreads>(a2, smd);
+      __shared__ int s_action, s_tofinal;
+      __shared__ double s_beta;
+      if (tid == 0) {
+        pcg_decide(st, t0, t1, t2);
+        s_action = st->action;
+        s_beta = st->pub.beta;
+        s_tofinal = st->pub.mode == M_FINAL && st->action != A_SWAP_TO_X;
+      }
+      __syncthreads();
+      if (s_action != A_NONE)
+        pcg_direction_elems<double, false>(n, tid, kChunkThreads, s_action, s_beta, s_tofinal != 0, x, r, z, p,
+                                           psave, ap, q.ztrue);
+      __syncthreads();
+      for (int64_t i = tid; i < n; i += kChunkThreads) q.p[i] = p[i];  // the operator reads p
+      __syncthreads();
+      if (tid == 0) {
+        st->bar_count2 = 0;
+        __threadfence();
+        atomicExch(&st->bar_gen, st->bar_gen + 1u);
+      }
+    }
+    __syncthreads();
+    for (int64_t i = tid; i < n; i += kChunkThreads) {
+      q.x[i] = x[i];
+      q.r[i] = r[i];
+      q.z[i] = z[i];
+      q.p[i] = p[i];
+      q.psave[i] = psave[i];
+    }
+    return;
+  }
+  // ---------------- chunk CTAs
+  TA* t_s = reinterpret_cast<TA*>(smem + 2 * S::kStageBytes);
+  const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
+  const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int c, int stg) {
+    unsigned char* base = smem + stg * S::kStageBytes;
+    fence_proxy_async();
+    mbar_expect_tx(&bar[stg], S::kStageBytes);
+    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &bar[stg]);
+    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &bar[stg]);
+  };
+  const int kct = (int)blockIdx.x < a.nchunks ? (a.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+  auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * G; };
+  int it = 0;
+  if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
+  for (int step = 0; step < q.steps; ++step) {
+    if (tid == 0) {
+      const int status = __ldcg(&st->pub.status), mode = __ldcg(&st->pub.mode);
+      s_go = status == TLS_PCG_ACTIVE && mode != M_DONE;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    // ---- A
+    for (int j = 0; j < kct; ++j, ++it) {
+      const int stg = it & 1;
+      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
+      mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+      const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
+      const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
+      chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
+    }
+    // ---- barrier over the chunk CTAs
+    __syncthreads();
+    if (tid == 0) {
+      volatile uint32_t* gen = &st->bar_gen;
+      gen0 = *gen;
+      __threadfence();
+      s_ok = 1;
+      last = atomicAdd(&st->bar_count, 1u) == (uint32_t)G - 1;
+      if (last) {
+        st->bar_count = 0;
+        __threadfence();
+        atomicExch(&st->bar_gen, gen0 + 1u);
+      } else {
+        const long long t0 = clock64();
+        while (*gen == gen0) {
+          __nanosleep(64);
+          if (clock64() - t0 > (1LL << 31)) {
+            if (a.err) atomicExch(a.err, 2);
+            s_ok = 0;
+            break;
+          }
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (!s_ok) break;
+    // ---- B
+    for (int64_t i = blockIdx.x; i < a.nretained; i += G) {
+      const double dot = gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
+      if (tid == 0) q.dots[i] = dot;
+    }
+    // ---- arrive at the vector CTA, wait for its release
+    __syncthreads();
+    if (tid == 0) {
+      volatile uint32_t* gen = &st->bar_gen;
+      gen0 = *gen;
+      __threadfence();
+      atomicAdd(&st->bar_count2, 1u);
+      const long long t0 = clock64();
+      while (*gen == gen0) {
+        __nanosleep(64);
+        if (clock64() - t0 > (1LL << 31)) {
+          if (a.err) atomicExch(a.err, 2);
+          s_ok = 0;
+          break;
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (!s_ok) break;
+  }
+  if (kct > 0) mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, a.err);
+  __syncthreads();
+}
+
 // W slab index of component k of slab entry s.
 template <int DR, int DE>
 __device__ __forceinline__ int64_t w_index(int64_t s, int k, int cap) {
@@ -845,7 +1061,14 @@ struct SchurOps {
     if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
     if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
       return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
-    auto k = schur_pcg_kernel<DR, DE, CAP, TW, D>;
+    // six float64 vectors of the reduced system in one CTA's shared memory?
+    if (q.n * 6 * (int64_t)sizeof(double) <= S::kBaseSmem) return pcg_launch<TW, CAP, D, true>(a, q, s);
+    return pcg_launch<TW, CAP, D, false>(a, q, s);
+  }
+  template <typename TW, int CAP, int D, bool VC>
+  static int pcg_launch(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
+    using S = SlabShape<DR, DE, CAP, TW, double>;
+    auto k = VC ? schur_pcg_vc_kernel<DR, DE, CAP, TW, D> : schur_pcg_kernel<DR, DE, CAP, TW, D>;
     const int smem = S::kBaseSmem;
     static int grid = 0;  // co-resident CTAs: per-SM occupancy x SMs, once per instantiation
     if (grid == 0) {
