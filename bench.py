@@ -666,7 +666,7 @@ def run_cuda(args, world, rank, local):
     mixed_s = dist_max(sum(times) / len(times), world, device)
     fp64 = None
     if not args.no_fp64:
-        t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush)
+        t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), args.warmup, device, flush)
         fp64 = (dist_max(sum(t64) / len(t64), world, device), s64)
     roof = kernel_roofline(problem, tls, device)
     e2e_s, h2d, d2h = e2e_steps(data, tls, device, args.steps, "mixed")

@@ -273,18 +273,20 @@ class SchurLinearization:
         self.run_partial = torch.empty((max(lay.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
         self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
 
-    def damped(self, damping):
-        return DampedSchurSystem(self, damping)
+    def damped(self, damping, check: bool = True):
+        return DampedSchurSystem(self, damping, check)
 
 
 class DampedSchurSystem:
     """schur.py:263-397 on the GPU."""
 
-    def __init__(self, lin: SchurLinearization, damping: float):
+    def __init__(self, lin: SchurLinearization, damping: float, check: bool = True):
+        """``check=False`` defers the host read of the count of eliminated blocks
+        that are not positive definite (``plan.bad``) to the caller."""
         self.linear, self.plan, self.damping = lin, lin.plan, float(damping)
         self.args = self._args()
         L.call("tls_schur_damp", C.byref(self.args), L.stream_handle(self.plan.device))
-        if int(self.plan.bad.item()) > 0:
+        if check and int(self.plan.bad.item()) > 0:
             raise torch.linalg.LinAlgError("damped eliminated block is not positive definite")
         self._rhs_ready = False
 
@@ -348,14 +350,14 @@ class DampedSchurSystem:
         L.call("tls_schur_preconditioner_blocks", C.byref(self.args), out.data_ptr(), self.stream)
         return out
 
-    def preconditioner(self, *, graph_safe: bool = False):
+    def preconditioner(self, *, graph_safe: bool = False, check: bool = True):
         """Exact Schur block-diagonal preconditioner (schur.py:353-378)."""
         from .solvers import BlockJacobiPreconditioner
 
         p = self.plan
         blocks = self.preconditioner_blocks()
         return BlockJacobiPreconditioner.from_blocks([(blocks, [(0, p.dr)], p.r.count, p.dr)], self.damping,
-                                                     None, p.dim)
+                                                     None, p.dim, check=check)
 
     def dense_matrix(self) -> torch.Tensor:
         """Dense reduced matrix (s U s + lambda I) - W W^T, symmetrised (schur.py:380-397)."""

@@ -203,8 +203,12 @@ class BlockJacobiPreconditioner:
         self._array = (L.BlockGroup * max(len(groups), 1))(*groups)
 
     @classmethod
-    def from_blocks(cls, specs, damping, scale, n):
-        """specs: [(blocks [count,dim,dim] f64, [(offset, dim), ...] members, count, dim)]."""
+    def from_blocks(cls, specs, damping, scale, n, check: bool = True):
+        """specs: [(blocks [count,dim,dim] f64, [(offset, dim), ...] members, count, dim)].
+
+        ``check=False`` skips the host read of the non-positive-definite count;
+        the device word is kept as ``bad_word`` for the caller to read later
+        (``DevicePCG.run`` reads it with the PCG control block)."""
         if len(specs) > L.MAX_GROUPS:
             raise ValueError("too many preconditioner groups")
         groups, keep = [], []
@@ -229,7 +233,8 @@ class BlockJacobiPreconditioner:
         bad = torch.zeros(1, dtype=torch.int32, device=device)
         L.call("tls_block_cholesky", pre._array, len(groups), float(damping), bad.data_ptr(),
                L.stream_handle(device))
-        if int(bad.item()) > 0:
+        pre.bad_word = bad
+        if check and int(bad.item()) > 0:
             raise torch.linalg.LinAlgError("damped block is not positive definite")
         return pre
 
@@ -321,12 +326,17 @@ class DevicePCG:
         nbytes = L.lib().tls_pcg_state_bytes()
         self.control = torch.zeros(nbytes, dtype=torch.uint8, device=device)
         self.host = torch.empty(C.sizeof(L.PcgControl), dtype=torch.uint8, pin_memory=True)
+        self.words_host = torch.zeros(8, dtype=torch.int32, pin_memory=True)
 
     def run(self, rhs: Tensor, config: ConjugateGradientConfig, *, normal_args=None, schur_args=None,
-            preconditioner: BlockJacobiPreconditioner | None = None, error_word: Tensor | None = None) -> PCGResult:
+            preconditioner: BlockJacobiPreconditioner | None = None, error_word: Tensor | None = None,
+            bad_words=()) -> PCGResult:
         """``error_word``: the operator's device error flag (the Schur kernels'
         bounded bulk-copy and grid-barrier waits set it instead of hanging);
-        read once after the loop."""
+        ``bad_words``: device counts of blocks that were not positive definite
+        when the operator or preconditioner was factored (raised as
+        ``LinAlgError``). All are read with the last control-block read, so
+        they cost no extra host synchronisation."""
         a = L.PcgArgs()
         a.n = self.n
         a.vec_dtype = L.dtype_code(self.dtype)
@@ -352,26 +362,33 @@ class DevicePCG:
         L.call("tls_pcg_start", C.byref(a), float(config.rtol), float(config.atol), int(config.max_iterations),
                int(config.residual_check_interval), int(config.restart_strategy == "periodic"),
                float(config.residual_drift_tolerance), stream)
+        words = ([error_word] if error_word is not None else []) + [w for w in bad_words if w is not None]
         batch = config.graph_batch_iterations
         if schur_args is not None:
             # small Schur systems run the whole loop in one persistent launch;
             # otherwise the library queues at most 16 steps per call
             batch = max(batch, 4 * int(config.max_iterations) + 16)
         while True:
-            ctrl = self._read()
+            # steps after termination are no-ops, so run first and read after
+            L.call("tls_pcg_run", C.byref(a), batch, stream)
+            ctrl, flags = self._read(words)
             if ctrl.status != L.PCG_ACTIVE:
                 break
-            L.call("tls_pcg_run", C.byref(a), batch, stream)
-        if error_word is not None and int(error_word.item()) != 0:
+        if error_word is not None and flags[0] != 0:
             raise RuntimeError("Schur PCG: a bounded device wait (bulk copy or grid barrier) timed out")
+        if any(f > 0 for f in flags[1 if error_word is not None else 0 :]):
+            raise torch.linalg.LinAlgError("damped block is not positive definite")
         return PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
                          ctrl.status == L.PCG_CONVERGED, _REASONS[ctrl.status], int(ctrl.restarts),
                          int(ctrl.checks), float(ctrl.rhs_norm))
 
-    def _read(self) -> L.PcgControl:
+    def _read(self, words=()):
+        for k, w in enumerate(words):
+            self.words_host[k : k + 1].copy_(w.view(-1)[:1].to(torch.int32), non_blocking=True)
         self.host.copy_(self.control[: self.host.numel()], non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
-        return L.PcgControl.from_buffer_copy(self.host.numpy().tobytes())
+        flags = self.words_host[: len(words)].tolist()
+        return L.PcgControl.from_buffer_copy(self.host.numpy().tobytes()), flags
 
 
 def _generic_pcg(matvec, rhs, preconditioner, config):
@@ -563,9 +580,6 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             summary.termination_reason = "time_limit"
             break
         summary.iterations = iteration + 1
-        if not _finite(lin.residual, *lin.jacobian.jacs):
-            summary.termination_reason = "nonfinite_linearization"
-            break
         gradient = lin.gradient
         jacobian = lin.jacobian
         mask = None
@@ -573,8 +587,15 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             mask = bplan.free_mask(vals, gradient)
             gradient = gradient * mask
             jacobian = jacobian.scale_columns(mask)
-        summary.gradient_norm = float(reduce(gradient, 2))
-        if termination.target_cost is not None and float(lin.cost) <= termination.target_cost:
+        # one host read: finiteness of the linearization, |g|_inf and the cost
+        checks = [reduce(t, 2) for t in (lin.residual, *lin.jacobian.jacs)]
+        head = torch.stack((torch.stack(checks).max(), reduce(gradient, 2), lin.cost)).tolist()
+        if not math.isfinite(head[0]):
+            summary.termination_reason = "nonfinite_linearization"
+            break
+        summary.gradient_norm = head[1]
+        lin_cost = head[2]
+        if termination.target_cost is not None and lin_cost <= termination.target_cost:
             summary.termination_reason = "target_cost"
             break
         if summary.gradient_norm <= termination.gradient_tolerance:
@@ -610,7 +631,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                     joint_specs = _joint_specs(layout, cg.preconditioner_groups, scaled, sdiag)
                 else:
                     joint_specs = _layout_specs(layout, raw_diag)
-        old_cost = float(lin.cost)
+        old_cost = lin_cost
         accepted = False
         for _ in range(trust_region.max_trials if trust_region else 1):
             if timed_out():
@@ -620,7 +641,8 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             try:
                 if is_schur:
                     with _region("prepare_schur", profile):
-                        system = schur_lin.damped(damping)
+                        # schur_cg reads the non-positive-definite counts with the PCG control block
+                        system = schur_lin.damped(damping, check=linear_solver == "schur_dense")
                         rhs = system.reduced_rhs(-linear_gradient)
                     with _region("linear_solve", profile):
                         if linear_solver == "schur_dense":
@@ -632,11 +654,13 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                             usable = _finite(retained)
                             summary.linear_relative_residual_history.append(None)
                         else:
-                            pre = system.preconditioner() if cg.preconditioner else None
+                            pre = system.preconditioner(check=False) if cg.preconditioner else None
                             res = pcg_ws.run(rhs, cg, schur_args=system.args, preconditioner=pre,
-                                             error_word=schur_plan.err)
+                                             error_word=schur_plan.err,
+                                             bad_words=(schur_plan.bad, None if pre is None else pre.bad_word))
                             retained, its, conv = res.solution, res.iterations, res.converged
-                            usable = res.reason in ("residual_tolerance", "max_iterations") and _finite(retained)
+                            # finiteness of the step is read with the trial terms
+                            usable = res.reason in ("residual_tolerance", "max_iterations")
                             summary.linear_restarts += res.restarts
                             summary.linear_residual_checks += res.residual_checks
                             summary.linear_relative_residual_history.append(
@@ -661,7 +685,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                     summary.linear_relative_residual_history.append(
                         res.residual_norm / res.rhs_norm if res.rhs_norm else res.residual_norm)
                     delta = res.solution.to(torch.float64)
-                    usable = res.reason in ("residual_tolerance", "max_iterations") and _finite(delta)
+                    usable = res.reason in ("residual_tolerance", "max_iterations")
             except torch.linalg.LinAlgError:
                 usable = False
             if usable:
@@ -675,7 +699,11 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                 with _region("trial_residual", profile):
                     objective, reduction = problem._evaluate_trial(proposed, lin)
                 pred = -torch.dot(gradient, delta) - 0.5 * original.squared_matvec_norm(delta)
-                proposed_cost, actual, predicted = torch.stack((objective, reduction, pred)).tolist()
+                proposed_cost, actual, predicted, step_max = torch.stack(
+                    (objective, reduction, pred, reduce(delta, 2))).tolist()
+                if not math.isfinite(step_max):  # an unusable step: rejected, not a trial
+                    usable = False
+            if usable:
                 quality = actual / predicted if predicted > 0 else -math.inf
                 accepted = math.isfinite(proposed_cost) and (
                     trust_region is None or (actual > 0 and quality >= trust_region.step_quality_min))
@@ -701,14 +729,15 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                     fg = lin.gradient
                     if bplan is not None:
                         fg = bplan.projected_gradient(vals, fg)
-                    summary.gradient_norm = float(reduce(fg, 2))
+                    gnorm, step_norm = torch.stack((reduce(fg, 2), reduce(delta, 1).sqrt())).tolist()
+                    summary.gradient_norm = gnorm
                     if termination.target_cost is not None and proposed_cost <= termination.target_cost:
                         summary.termination_reason = "target_cost"
                     elif summary.gradient_norm <= termination.gradient_tolerance:
                         summary.termination_reason = "gradient_tolerance"
                     elif abs(actual) <= termination.cost_tolerance * max(old_cost, torch.finfo(vals.dtype).tiny):
                         summary.termination_reason = "cost_tolerance"
-                    elif float(reduce(delta, 1).sqrt()) <= termination.parameter_tolerance:
+                    elif step_norm <= termination.parameter_tolerance:
                         summary.termination_reason = "parameter_tolerance"
                     break
             summary.rejected_steps += 1
