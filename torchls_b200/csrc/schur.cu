@@ -270,21 +270,30 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
     const bool from_left = head[0] < lane * EPT;  // this thread's first run began in an earlier lane
     // lanes any run spans backwards; offsets 1, 2, 4, ... <= span cover it
     const unsigned span = __reduce_max_sync(0xffffffffu, (unsigned)(lane - hl));
+    // all DR components advance together, so the shuffle latencies overlap
+    TA cval[DR];
 #pragma unroll
-    for (int k = 0; k < DR; ++k) {
-      TA cval = v[EPT - 1][k];
-      for (unsigned off = 1; off <= span; off <<= 1) {
-        const TA o = __shfl_up_sync(0xffffffffu, cval, off);
-        if (lane - (int)off >= hl) cval += o;
-      }
-      const TA prev = __shfl_up_sync(0xffffffffu, cval, 1);
+    for (int k = 0; k < DR; ++k) cval[k] = v[EPT - 1][k];
+    for (unsigned off = 1; off <= span; off <<= 1) {
+      const bool take = lane - (int)off >= hl;
+      TA o[DR];
 #pragma unroll
-      for (int j = 0; j < EPT; ++j) {
-        if (tail[j]) {
-          // only the thread's first run can have begun in an earlier lane
-          const TA tot = (from_left && head[j] == head[0]) ? v[j][k] + prev : v[j][k];
-          reinterpret_cast<TA*>(a.run_partial)[(int64_t)tpos[le0 + j] * DR + k] = tot;
-        }
+      for (int k = 0; k < DR; ++k) o[k] = __shfl_up_sync(0xffffffffu, cval[k], off);
+#pragma unroll
+      for (int k = 0; k < DR; ++k)
+        if (take) cval[k] += o[k];
+    }
+    TA prev[DR];
+#pragma unroll
+    for (int k = 0; k < DR; ++k) prev[k] = __shfl_up_sync(0xffffffffu, cval[k], 1);
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+      if (tail[j]) {
+        // only the thread's first run can have begun in an earlier lane
+        const bool join = from_left && head[j] == head[0];
+        TA* dst = reinterpret_cast<TA*>(a.run_partial) + (int64_t)tpos[le0 + j] * DR;
+#pragma unroll
+        for (int k = 0; k < DR; ++k) dst[k] = join ? v[j][k] + prev[k] : v[j][k];
       }
     }
   }
