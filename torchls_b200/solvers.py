@@ -327,16 +327,19 @@ class DevicePCG:
         self.control = torch.zeros(nbytes, dtype=torch.uint8, device=device)
         self.host = torch.empty(C.sizeof(L.PcgControl), dtype=torch.uint8, pin_memory=True)
         self.words_host = torch.zeros(8, dtype=torch.int32, pin_memory=True)
+        self.extra_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
+        self._pending = None
 
     def run(self, rhs: Tensor, config: ConjugateGradientConfig, *, normal_args=None, schur_args=None,
             preconditioner: BlockJacobiPreconditioner | None = None, error_word: Tensor | None = None,
-            bad_words=()) -> PCGResult:
+            bad_words=(), defer: bool = False) -> PCGResult | None:
         """``error_word``: the operator's device error flag (the Schur kernels'
         bounded bulk-copy and grid-barrier waits set it instead of hanging);
         ``bad_words``: device counts of blocks that were not positive definite
         when the operator or preconditioner was factored (raised as
         ``LinAlgError``). All are read with the last control-block read, so
-        they cost no extra host synchronisation."""
+        they cost no extra host synchronisation. ``defer=True`` returns right
+        after the launch; :meth:`finish` completes the call."""
         a = L.PcgArgs()
         a.n = self.n
         a.vec_dtype = L.dtype_code(self.dtype)
@@ -368,27 +371,53 @@ class DevicePCG:
             # small Schur systems run the whole loop in one persistent launch;
             # otherwise the library queues at most 16 steps per call
             batch = max(batch, 4 * int(config.max_iterations) + 16)
+        # steps after termination are no-ops, so run first and read after
+        L.call("tls_pcg_run", C.byref(a), batch, stream)
+        self._pending = dict(a=a, keep=(keep, rhs), words=words, error_word=error_word, batch=batch, stream=stream)
+        if defer:
+            return None
+        return self.finish()[0]
+
+    def finish(self, extra: Tensor | None = None):
+        """Wait for the PCG launched by ``run(..., defer=True)``; ``extra`` (a
+        small float64 device tensor computed from the solution in stream order)
+        is read in the same host synchronisation. Returns ``(PCGResult,
+        extra_values)``; ``extra_values`` is None when the loop needed further
+        host-driven steps (then ``extra`` was computed from an unfinished x)."""
+        pend, self._pending = self._pending, None
+        a, words, error_word = pend["a"], pend["words"], pend["error_word"]
+        extra_vals = None
+        first = True
         while True:
-            # steps after termination are no-ops, so run first and read after
-            L.call("tls_pcg_run", C.byref(a), batch, stream)
-            ctrl, flags = self._read(words)
+            ctrl, flags, ev = self._read(words, extra if first else None)
+            if first:
+                extra_vals = ev
             if ctrl.status != L.PCG_ACTIVE:
                 break
+            first = False
+            extra_vals = None
+            L.call("tls_pcg_run", C.byref(a), pend["batch"], pend["stream"])
         if error_word is not None and flags[0] != 0:
             raise RuntimeError("Schur PCG: a bounded device wait (bulk copy or grid barrier) timed out")
         if any(f > 0 for f in flags[1 if error_word is not None else 0 :]):
             raise torch.linalg.LinAlgError("damped block is not positive definite")
-        return PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
-                         ctrl.status == L.PCG_CONVERGED, _REASONS[ctrl.status], int(ctrl.restarts),
-                         int(ctrl.checks), float(ctrl.rhs_norm))
+        res = PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
+                        ctrl.status == L.PCG_CONVERGED, _REASONS[ctrl.status], int(ctrl.restarts),
+                        int(ctrl.checks), float(ctrl.rhs_norm))
+        return res, extra_vals
 
-    def _read(self, words=()):
+    def _read(self, words=(), extra: Tensor | None = None):
         for k, w in enumerate(words):
             self.words_host[k : k + 1].copy_(w.view(-1)[:1].to(torch.int32), non_blocking=True)
+        ne = 0
+        if extra is not None:
+            ne = extra.numel()
+            self.extra_host[:ne].copy_(extra.reshape(-1).to(torch.float64), non_blocking=True)
         self.host.copy_(self.control[: self.host.numel()], non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
         flags = self.words_host[: len(words)].tolist()
-        return L.PcgControl.from_buffer_copy(self.host.numpy().tobytes()), flags
+        ev = self.extra_host[:ne].tolist() if extra is not None else None
+        return L.PcgControl.from_buffer_copy(self.host.numpy().tobytes()), flags, ev
 
 
 def _generic_pcg(matvec, rhs, preconditioner, config):
@@ -575,6 +604,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
     layout = problem.layout
     with _region("linearize", profile):
         lin = problem.linearize(vals, jacobian_dtype=jdt, schur=schur_plan)
+    cached_head = None
     for iteration in range(termination.max_iterations):
         if timed_out():
             summary.termination_reason = "time_limit"
@@ -588,8 +618,12 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             gradient = gradient * mask
             jacobian = jacobian.scale_columns(mask)
         # one host read: finiteness of the linearization, |g|_inf and the cost
-        checks = [reduce(t, 2) for t in (lin.residual, *lin.jacobian.jacs)]
-        head = torch.stack((torch.stack(checks).max(), reduce(gradient, 2), lin.cost)).tolist()
+        # (already read together with the previous step's norms when possible)
+        if cached_head is not None:
+            head, cached_head = cached_head, None
+        else:
+            checks = [reduce(t, 2) for t in (lin.residual, *lin.jacobian.jacs)]
+            head = torch.stack((torch.stack(checks).max(), reduce(gradient, 2), lin.cost)).tolist()
         if not math.isfinite(head[0]):
             summary.termination_reason = "nonfinite_linearization"
             break
@@ -633,11 +667,28 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                     joint_specs = _layout_specs(layout, raw_diag)
         old_cost = lin_cost
         accepted = False
+
+        def trial_tensors(step):
+            """Step in the problem's coordinates, proposed values and the device
+            vector (trial objective, exact reduction, predicted reduction, max |step|)."""
+            step = step.to(torch.float64)
+            if solve_scale is not None:
+                step = solve_scale * step
+            if bplan is None:
+                prop = vals.retract(step, layout)
+            else:
+                prop, step = bplan.retract(vals, step)
+            with _region("trial_residual", profile):
+                objective, reduction = problem._evaluate_trial(prop, lin)
+            pred = -torch.dot(gradient, step) - 0.5 * original.squared_matvec_norm(step)
+            return step, prop, torch.stack((objective, reduction, pred, reduce(step, 2)))
+
         for _ in range(trust_region.max_trials if trust_region else 1):
             if timed_out():
                 summary.termination_reason = "time_limit"
                 break
             summary.lambda_history.append(damping)
+            trial = None
             try:
                 if is_schur:
                     with _region("prepare_schur", profile):
@@ -653,11 +704,21 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                             its, conv = 1, True
                             usable = _finite(retained)
                             summary.linear_relative_residual_history.append(None)
+                            delta = system.backsubstitute(retained)
                         else:
                             pre = system.preconditioner(check=False) if cg.preconditioner else None
-                            res = pcg_ws.run(rhs, cg, schur_args=system.args, preconditioner=pre,
-                                             error_word=schur_plan.err,
-                                             bad_words=(schur_plan.bad, None if pre is None else pre.bad_word))
+                            pcg_ws.run(rhs, cg, schur_args=system.args, preconditioner=pre,
+                                       error_word=schur_plan.err,
+                                       bad_words=(schur_plan.bad, None if pre is None else pre.bad_word),
+                                       defer=True)
+                            # the trial is queued behind the (persistent) PCG launch and read back
+                            # with its control block: one host synchronisation per trial
+                            trial = trial_tensors(system.backsubstitute(pcg_ws.x))
+                            res, values = pcg_ws.finish(extra=trial[2])
+                            if values is None:  # the PCG needed host-driven steps: redo the trial
+                                trial = trial_tensors(system.backsubstitute(res.solution))
+                                values = trial[2].tolist()
+                            trial = (trial[0], trial[1], values)
                             retained, its, conv = res.solution, res.iterations, res.converged
                             # finiteness of the step is read with the trial terms
                             usable = res.reason in ("residual_tolerance", "max_iterations")
@@ -665,7 +726,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                             summary.linear_residual_checks += res.residual_checks
                             summary.linear_relative_residual_history.append(
                                 res.residual_norm / res.rhs_norm if res.rhs_norm else res.residual_norm)
-                        delta = system.backsubstitute(retained)
+                            delta = None
                     summary.linear_iterations += its
                     summary.linear_iterations_history.append(its)
                     summary.linear_converged_history.append(conv)
@@ -689,18 +750,10 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             except torch.linalg.LinAlgError:
                 usable = False
             if usable:
-                delta = delta.to(torch.float64)
-                if solve_scale is not None:
-                    delta = solve_scale * delta
-                if bplan is None:
-                    proposed = vals.retract(delta, layout)
-                else:
-                    proposed, delta = bplan.retract(vals, delta)
-                with _region("trial_residual", profile):
-                    objective, reduction = problem._evaluate_trial(proposed, lin)
-                pred = -torch.dot(gradient, delta) - 0.5 * original.squared_matvec_norm(delta)
-                proposed_cost, actual, predicted, step_max = torch.stack(
-                    (objective, reduction, pred, reduce(delta, 2))).tolist()
+                if trial is None:
+                    trial = trial_tensors(delta)
+                    trial = (trial[0], trial[1], trial[2].tolist())
+                delta, proposed, (proposed_cost, actual, predicted, step_max) = trial
                 if not math.isfinite(step_max):  # an unusable step: rejected, not a trial
                     usable = False
             if usable:
@@ -729,7 +782,13 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                     fg = lin.gradient
                     if bplan is not None:
                         fg = bplan.projected_gradient(vals, fg)
-                    gnorm, step_norm = torch.stack((reduce(fg, 2), reduce(delta, 1).sqrt())).tolist()
+                    if bplan is None:
+                        checks = [reduce(t, 2) for t in (lin.residual, *lin.jacobian.jacs)]
+                        gnorm, step_norm, fin, cost_next = torch.stack(
+                            (reduce(fg, 2), reduce(delta, 1).sqrt(), torch.stack(checks).max(), lin.cost)).tolist()
+                        cached_head = [fin, gnorm, cost_next]  # the next iteration's opening read
+                    else:
+                        gnorm, step_norm = torch.stack((reduce(fg, 2), reduce(delta, 1).sqrt())).tolist()
                     summary.gradient_norm = gnorm
                     if termination.target_cost is not None and proposed_cost <= termination.target_cost:
                         summary.termination_reason = "target_cost"
