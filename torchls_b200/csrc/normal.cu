@@ -56,6 +56,14 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
   TA xv[DM];
   const TJ* __restrict__ jac = reinterpret_cast<const TJ*>(p.jac);
   const bool live = f < p.n;
+  // factor-major outputs ([N][D] or [N][R]) go through a per-warp shared stage
+  // so the warp stores its contiguous range with coalesced stores
+  constexpr int kStage = (MODE == 1) ? RM : DM;
+  __shared__ TV stage[128 / 32][32 * kStage];
+  const int lane = threadIdx.x & 31;
+  TV* row_stage = stage[threadIdx.x >> 5];
+  const int64_t f0 = f - lane;
+  const int width = (MODE == 1) ? p.R : p.D;
   if (live) {
 #pragma unroll
     for (int c = 0; c < DM; ++c) {
@@ -68,12 +76,19 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
         xv[c] = v;
       }
     }
-    TJ J[RM][DM];
+    // Large blocks are not held in registers (occupancy): J is streamed row by
+    // row for q = J x and read again (L1/L2 hits) for J^T q. Same arithmetic order.
+    constexpr bool kHold = RM * DM <= 36;
+    auto jget = [&](int i, int c) -> TJ {
+      return (i < p.R && c < p.D) ? __ldg(jac + (int64_t)(i * p.D + c) * p.ld + f) : TJ(0);
+    };
+    TJ J[kHold ? RM : 1][kHold ? DM : 1];
+    if constexpr (kHold) {
 #pragma unroll
-    for (int i = 0; i < RM; ++i)
+      for (int i = 0; i < RM; ++i)
 #pragma unroll
-      for (int c = 0; c < DM; ++c)
-        J[i][c] = (i < p.R && c < p.D) ? __ldg(jac + (int64_t)(i * p.D + c) * p.ld + f) : TJ(0);
+        for (int c = 0; c < DM; ++c) J[i][c] = jget(i, c);
+    }
     if constexpr (MODE == 3) {
 #pragma unroll
       for (int i = 0; i < RM; ++i)
@@ -82,20 +97,34 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
 #pragma unroll
       for (int i = 0; i < RM; ++i)
 #pragma unroll
-        for (int c = 0; c < DM; ++c) q[i] += static_cast<TA>(J[i][c]) * xv[c];
+        for (int c = 0; c < DM; ++c) {
+          if constexpr (kHold) q[i] += static_cast<TA>(J[i][c]) * xv[c];
+          else q[i] += static_cast<TA>(jget(i, c)) * xv[c];
+        }
     }
     if constexpr (MODE == 0 || MODE == 3) {
 #pragma unroll
       for (int c = 0; c < DM; ++c) {
         TA y = TA(0);
 #pragma unroll
-        for (int i = 0; i < RM; ++i) y += static_cast<TA>(J[i][c]) * q[i];
-        if (c < p.D) out[f * p.D + c] = static_cast<TV>(y);
+        for (int i = 0; i < RM; ++i) {
+          if constexpr (kHold) y += static_cast<TA>(J[i][c]) * q[i];
+          else y += static_cast<TA>(jget(i, c)) * q[i];
+        }
+        if (c < p.D) row_stage[lane * width + c] = static_cast<TV>(y);
       }
     } else if constexpr (MODE == 1) {
 #pragma unroll
       for (int i = 0; i < RM; ++i)
-        if (i < p.R) out[f * p.R + i] = static_cast<TV>(q[i]);
+        if (i < p.R) row_stage[lane * width + i] = static_cast<TV>(q[i]);
+    }
+  }
+  if constexpr (MODE != 2) {
+    __syncwarp();
+    if (f0 < p.n) {
+      const int nvalid = (p.n - f0) < 32 ? (int)(p.n - f0) : 32;
+      TV* dst = out + f0 * width;
+      for (int k = lane; k < nvalid * width; k += 32) dst[k] = row_stage[k];
     }
   }
   if constexpr (MODE == 2) {
@@ -182,11 +211,23 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
   for (int k = 0; k < WM; ++k) acc[k] = 0.0;
   if (t < seg.count) {
     const int b = seg.ptr[t], e = seg.ptr[t + 1];
-    for (int j = b + lane; j < e; j += L) {
-      const TV* src = contrib + seg.src[j];
+    // two entries per lane in flight per round; accumulated in list order
+    for (int j0 = b + lane; j0 < e; j0 += 2 * L) {
+      TV v[2][WM];
 #pragma unroll
-      for (int k = 0; k < WM; ++k)
-        if (k < d) acc[k] += to_d(src[k]);
+      for (int u = 0; u < 2; ++u) {
+        const int j = j0 + u * L;
+        const TV* src = j < e ? contrib + seg.src[j] : nullptr;
+#pragma unroll
+        for (int k = 0; k < WM; ++k) v[u][k] = (src && k < d) ? src[k] : TV(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (j0 + u * L < e) {
+#pragma unroll
+          for (int k = 0; k < WM; ++k)
+            if (k < d) acc[k] += to_d(v[u][k]);
+        }
     }
   }
   bool writer;
