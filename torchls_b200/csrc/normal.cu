@@ -45,9 +45,9 @@ __host__ FactorPass make_pass(const tls_factor_group& fg, const tls_var_group* v
 
 // MODE 0: contributions J^T J x (per factor)   MODE 1: rows J x   MODE 2: |J x|^2 partial
 // MODE 3: contributions J^T u for factor rows u (x holds u, [N][R])
-template <int RM, int DM, int MODE, typename TJ, typename TV, typename TA, typename TO = TV>
+template <int RM, int DM, int MODE, typename TJ, typename TV, typename TA>
 __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV* __restrict__ x,
-                                                          const TV* __restrict__ scale, TO* __restrict__ out,
+                                                          const TV* __restrict__ scale, TV* __restrict__ out,
                                                           double* __restrict__ partials) {
   const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   TA q[RM];
@@ -59,9 +59,9 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
   // factor-major outputs ([N][D] or [N][R]) go through a per-warp shared stage
   // so the warp stores its contiguous range with coalesced stores
   constexpr int kStage = (MODE == 1) ? RM : DM;
-  __shared__ TO stage[128 / 32][32 * kStage];
+  __shared__ TV stage[128 / 32][32 * kStage];
   const int lane = threadIdx.x & 31;
-  TO* row_stage = stage[threadIdx.x >> 5];
+  TV* row_stage = stage[threadIdx.x >> 5];
   const int64_t f0 = f - lane;
   const int width = (MODE == 1) ? p.R : p.D;
   if (live) {
@@ -111,19 +111,19 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
           if constexpr (kHold) y += static_cast<TA>(J[i][c]) * q[i];
           else y += static_cast<TA>(jget(i, c)) * q[i];
         }
-        if (c < p.D) row_stage[lane * width + c] = static_cast<TO>(y);
+        if (c < p.D) row_stage[lane * width + c] = static_cast<TV>(y);
       }
     } else if constexpr (MODE == 1) {
 #pragma unroll
       for (int i = 0; i < RM; ++i)
-        if (i < p.R) row_stage[lane * width + i] = static_cast<TO>(q[i]);
+        if (i < p.R) row_stage[lane * width + i] = static_cast<TV>(q[i]);
     }
   }
   if constexpr (MODE != 2) {
     __syncwarp();
     if (f0 < p.n) {
       const int nvalid = (p.n - f0) < 32 ? (int)(p.n - f0) : 32;
-      TO* dst = out + f0 * width;
+      TV* dst = out + f0 * width;
       for (int k = lane; k < nvalid * width; k += 32) dst[k] = row_stage[k];
     }
   }
@@ -139,15 +139,15 @@ __global__ void __launch_bounds__(128) factor_pass_kernel(FactorPass p, const TV
   }
 }
 
-template <int MODE, typename TJ, typename TV, typename TA, typename TO = TV>
-static int launch_factor_pass(const FactorPass& p, const TV* x, const TV* scale, TO* out, double* partials,
+template <int MODE, typename TJ, typename TV, typename TA>
+static int launch_factor_pass(const FactorPass& p, const TV* x, const TV* scale, TV* out, double* partials,
                               cudaStream_t st) {
   if (p.n == 0) return TLS_OK;
   const int block = 128;
   const int64_t grid = (p.n + block - 1) / block;
 #define TLS_FP(RM, DM)                                                                                    \
   if (p.R <= RM && p.D <= DM) {                                                                          \
-    factor_pass_kernel<RM, DM, MODE, TJ, TV, TA, TO><<<grid, block, 0, st>>>(p, x, scale, out, partials); \
+    factor_pass_kernel<RM, DM, MODE, TJ, TV, TA><<<grid, block, 0, st>>>(p, x, scale, out, partials); \
     TLS_CHECK_LAUNCH();                                                                                   \
     return TLS_OK;                                                                                        \
   }
@@ -182,8 +182,8 @@ __host__ __device__ __forceinline__ int gather_blocks_for(const tls_segments& se
   return (int)((threads + 255) / 256);
 }
 
-template <int WM, typename TV, typename TC = TV>
-__global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, const TC* __restrict__ contrib,
+template <int WM, typename TV>
+__global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, const TV* __restrict__ contrib,
                                                             const TV* __restrict__ x, const TV* __restrict__ scale,
                                                             double damping, TV* __restrict__ y,
                                                             double* __restrict__ dot_partials, PcgState* pst) {
@@ -213,13 +213,13 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
     const int b = seg.ptr[t], e = seg.ptr[t + 1];
     // two entries per lane in flight per round; accumulated in list order
     for (int j0 = b + lane; j0 < e; j0 += 2 * L) {
-      TC v[2][WM];
+      TV v[2][WM];
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         const int j = j0 + u * L;
-        const TC* src = j < e ? contrib + seg.src[j] : nullptr;
+        const TV* src = j < e ? contrib + seg.src[j] : nullptr;
 #pragma unroll
-        for (int k = 0; k < WM; ++k) v[u][k] = (src && k < d) ? src[k] : TC(0);
+        for (int k = 0; k < WM; ++k) v[u][k] = (src && k < d) ? src[k] : TV(0);
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u)
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(256) normal_gather_kernel(GatherGroups g, cons
 using namespace tls;
 
 int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                      void* pcg_state, cudaStream_t st, int contrib_f32 = 0);
+                      void* pcg_state, cudaStream_t st);
 
 // Number of blocks (and dot partials) of the normal operator's gather kernel.
 int tls_normal_gather_blocks(const tls_normal_args* a) {
@@ -298,21 +298,11 @@ int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* d
                      void* pcg_state, cudaStream_t st) {
   if (a->nfactor_groups > TLS_MAX_FACTOR_GROUPS || a->nvar_groups > TLS_MAX_GROUPS)
     return tls_set_error(TLS_ERR_INVALID, "too many groups");
-  // float32 Jacobians with float64 vectors: each factor's contribution J_f^T J_f x
-  // is computed in float64 and stored in float32 (a product inside one factor
-  // block, like the float32 Jacobian itself); the sums over factors stay float64.
-  // The contribution buffer is half the bytes and stays in L2 between the passes.
-  bool f32c = a->vec_dtype == TLS_F64 && a->nfactor_groups > 0;
-  for (int k = 0; k < a->nfactor_groups; ++k) f32c = f32c && a->fg[k].jac_dtype == TLS_F32;
   for (int k = 0; k < a->nfactor_groups; ++k) {
     const tls_factor_group& fg = a->fg[k];
     FactorPass p = make_pass(fg, a->vg);
     int rc;
-    if (f32c) {
-      float* out = (float*)a->contrib + a->contrib_offset[k];
-      rc = launch_factor_pass<0, float, double, double, float>(p, (const double*)x, (const double*)a->scale, out,
-                                                               nullptr, st);
-    } else if (a->vec_dtype == TLS_F64) {
+    if (a->vec_dtype == TLS_F64) {
       double* out = (double*)a->contrib + a->contrib_offset[k];
       if (fg.jac_dtype == TLS_F64)
         rc = launch_factor_pass<0, double, double, double>(p, (const double*)x, (const double*)a->scale, out, nullptr, st);
@@ -327,11 +317,11 @@ int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* d
     }
     if (rc) return rc;
   }
-  return tls_normal_gather(a, x, y, dot_partials, gather_blocks, pcg_state, st, f32c ? 1 : 0);
+  return tls_normal_gather(a, x, y, dot_partials, gather_blocks, pcg_state, st);
 }
 
 int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
-                      void* pcg_state, cudaStream_t st, int contrib_f32) {
+                      void* pcg_state, cudaStream_t st) {
   PcgState* pst = reinterpret_cast<PcgState*>(pcg_state);
   GatherGroups g{};
   g.ngroups = a->nvar_groups;
@@ -349,11 +339,7 @@ int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* 
   if (blocks == 0) return TLS_OK;
 #define TLS_G(WM)                                                                                        \
   if (wmax <= WM) {                                                                                      \
-    if (a->vec_dtype == TLS_F64 && contrib_f32)                                                          \
-      normal_gather_kernel<WM, double, float><<<blocks, 256, 0, st>>>(g, (const float*)a->contrib,         \
-                                                                      (const double*)x, (const double*)a->scale, \
-                                                                      a->damping, (double*)y, dot_partials, pst); \
-    else if (a->vec_dtype == TLS_F64)                                                                    \
+    if (a->vec_dtype == TLS_F64)                                                                         \
       normal_gather_kernel<WM, double><<<blocks, 256, 0, st>>>(g, (const double*)a->contrib, (const double*)x, \
                                                                (const double*)a->scale, a->damping,     \
                                                                (double*)y, dot_partials, pst);           \
@@ -420,8 +406,8 @@ extern "C" int tls_squared_matvec_norm(const tls_normal_args* a, const double* x
     const int blocks = (int)((fg.count + 127) / 128);
     if (blocks > (1 << 20)) return tls_set_error(TLS_ERR_UNSUPPORTED, "too many factors for one pass");
     int rc = fg.jac_dtype == TLS_F64
-                 ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, (double*)nullptr, partials, st)
-                 : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, (double*)nullptr, partials, st);
+                 ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, nullptr, partials, st)
+                 : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, nullptr, partials, st);
     if (rc) return rc;
     sum_partials_kernel<<<1, 256, 0, st>>>(partials, blocks, out, first ? 0 : 1);
     TLS_CHECK_LAUNCH();
@@ -512,8 +498,8 @@ extern "C" int tls_squared_matvec_norm_static(const tls_normal_args* a, const do
     FactorPass p = make_pass(fg, a->vg);
     const int blocks = (int)((fg.count + 127) / 128);
     rc = fg.jac_dtype == TLS_F64
-             ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, (double*)nullptr, partials, st)
-             : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, (double*)nullptr, partials, st);
+             ? launch_factor_pass<2, double, double, double>(p, x, (const double*)a->scale, nullptr, partials, st)
+             : launch_factor_pass<2, float, double, double>(p, x, (const double*)a->scale, nullptr, partials, st);
     if (rc) return rc;
     sum_partials_kernel<<<1, 256, 0, st>>>(partials, blocks, out, first ? 0 : 1);
     TLS_CHECK_LAUNCH();
