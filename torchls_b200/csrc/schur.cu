@@ -840,14 +840,23 @@ __global__ void schur_factor_kernel(tls_schur_args a) {
 
 // W_e = diag(s_i) E_e diag(s_p) L_p^-T into the slabs; padding entries get 0.
 template <int DR, int DE, typename TW>
-__global__ void schur_whiten_kernel(tls_schur_args a) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= (int64_t)a.nchunks * a.cap) return;
+__global__ void __launch_bounds__(128) schur_whiten_kernel(tls_schur_args a) {
+  // The block's cross blocks ([128][DR][DE] float64, contiguous) are staged in
+  // shared memory with coalesced loads; each thread then whitens its own.
+  constexpr int kW = DR * DE;
+  __shared__ double e_s[128 * kW];
+  const int64_t s0 = (int64_t)blockIdx.x * blockDim.x;
+  const int64_t s = s0 + threadIdx.x;
+  const int64_t nslab = (int64_t)a.nchunks * a.cap;
+  const int nvalid = (int)((nslab - s0) < 128 ? (nslab - s0) : 128);
+  for (int k = threadIdx.x; k < nvalid * kW; k += 128) e_s[k] = a.cross[s0 * kW + k];
+  __syncthreads();
+  if (s >= nslab) return;
   TW* w = reinterpret_cast<TW*>(a.w);
   const int64_t i = a.slab_r[s];
   if (i < 0) {
 #pragma unroll
-    for (int k = 0; k < DR * DE; ++k) w[w_index<DR, DE>(s, k, a.cap)] = TW(0);
+    for (int k = 0; k < kW; ++k) w[w_index<DR, DE>(s, k, a.cap)] = TW(0);
     return;
   }
   const int64_t p = a.slab_e[s];
@@ -857,7 +866,7 @@ __global__ void schur_whiten_kernel(tls_schur_args a) {
 #pragma unroll
   for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
   const double* Li = a.inv_l + p * DE * DE;
-  const double* E = a.cross + s * DR * DE;
+  const double* E = e_s + threadIdx.x * kW;
 #pragma unroll
   for (int r = 0; r < DR; ++r) {
 #pragma unroll
