@@ -35,10 +35,10 @@ sys.path.insert(0, ROOT)
 METRIC = "BA solve s to rel-cost 1e-8 (mixed vs FP64 CUDA); normal-matvec HBM GB/s vs peak"
 TARGET_FILE = os.path.join(ROOT, "tests", "golden", "ba_mid_target.json")
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the persistent
-# Schur-PCG kernel in the roofline measurement (100 iterations + 3 residual checks
-# on the 1M-observation reduced system): 5.713 GB + 0.317 GB
+# Schur-PCG kernel (vector-CTA variant) in the roofline measurement (100 iterations
+# + 3 residual checks on the 1M-observation reduced system): 5.990 GB + 0.327 GB
 # (profiles/schur_pcg_kernel_ba_mid_1M.md).
-NCU_TRAFFIC_BYTES = 6_030_313_488
+NCU_TRAFFIC_BYTES = 6_317_141_248
 
 
 def parse():
@@ -700,7 +700,7 @@ def run_cuda(args, world, rank, local):
         "mixed_speedup_vs_fp64": None if fp64 is None else fp64[0] / mixed_s,
         "normal_matvec": {"gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
                           "bytes": roof["normal_bytes"]},
-        "roofline": {"kernel": "schur_pcg_kernel (persistent Schur-PCG: chunk streaming + gather + vector phase)",
+        "roofline": {"kernel": "schur_pcg_vc_kernel (persistent Schur-PCG: chunk streaming + gather + vector CTA)",
                      "bound": "hbm", "achieved": pcg_gbs, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
                      "frac": pcg_gbs / hbm, "us_per_launch": roof["pcg_s"] * 1e6,
                      "operator_applications_per_launch": roof["pcg_applications"],
