@@ -201,6 +201,19 @@ def time_solves(problem, init, tls, precision, steps, warmup, device, flush, opt
     return times, summ, launches
 
 
+def timed_reps(fn, reps, flush):
+    """Mean device time of fn() over `reps` calls, each after an L2 flush
+    (outside the timed region), with CUDA events on the current stream."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for a, b in evs:
+        flush_l2(flush)
+        a.record()
+        fn()
+        b.record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / 1e3 / reps
+
+
 def kernel_roofline(problem, tls, device):
     """Time the reduced-camera (Schur) matvec and the full normal matvec alone."""
     import ctypes
@@ -217,32 +230,28 @@ def kernel_roofline(problem, tls, device):
     x = torch.randn(plan.dim, device=device, dtype=torch.float64)
     out = torch.empty_like(x)
     stream = L.stream_handle(device)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=device)
     reps = 50
     for _ in range(5):
         L.call("tls_schur_matvec", ctypes.byref(system.args), x.data_ptr(), out.data_ptr(), stream)
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    for _ in range(reps):
-        L.call("tls_schur_matvec", ctypes.byref(system.args), x.data_ptr(), out.data_ptr(), stream)
-    e.record()
-    torch.cuda.synchronize(device)
-    schur_s = s.elapsed_time(e) / 1e3 / reps
+    schur_s = timed_reps(lambda: L.call("tls_schur_matvec", ctypes.byref(system.args), x.data_ptr(),
+                                        out.data_ptr(), stream), reps, flush)
     E = plan.nedges
     # algorithmic bytes: W (18 float32) + 2 int32 edge indices per edge, x and out (float64)
     schur_bytes = E * (plan.dr * plan.de * 4 + 2 * 4) + 2 * plan.dim * 8
-    # full-system normal matvec J^T J x + lambda x: float32 J, float64 vectors
+    # full-system normal matvec J^T J x + lambda x: float32 J, float64 vectors;
+    # the one-pass (tile plan) operator, and the two-pass one for comparison
     J = lin.jacobian
     v = torch.randn(J.shape[1], device=device, dtype=torch.float64)
-    args = J.normal_args(torch.float64, 1e-3)
     y = torch.empty_like(v)
-    for _ in range(5):
-        L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(), y.data_ptr(), stream)
-    s.record()
-    for _ in range(reps):
-        L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(), y.data_ptr(), stream)
-    e.record()
-    torch.cuda.synchronize(device)
-    normal_s = s.elapsed_time(e) / 1e3 / reps
+    normal = {}
+    for tiles in (True, False):
+        args = J.normal_args(torch.float64, 1e-3, tiles=tiles)
+        for _ in range(5):
+            L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(), y.data_ptr(), stream)
+        normal[tiles] = timed_reps(lambda: L.call("tls_normal_matvec", ctypes.byref(args), v.data_ptr(),
+                                                  y.data_ptr(), stream), reps, flush)
+    normal_s, two_pass_s = normal[True], normal[False]
     st = J.structure
     nnz = sum(p.count * st.rdims[k] * st.D[k] for k, p in enumerate(st.plans))
     slots = sum(p.count * len(p.type_indices) for p in st.plans)
@@ -256,6 +265,8 @@ def kernel_roofline(problem, tls, device):
     cfg = ConjugateGradientConfig(rtol=0.0, atol=0.0, max_iterations=100)
     rhs = torch.randn(plan.dim, device=device, dtype=torch.float64)
     ws.run(rhs, cfg, schur_args=system.args, preconditioner=pre, error_word=plan.err)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush_l2(flush)
     s.record()
     res = ws.run(rhs, cfg, schur_args=system.args, preconditioner=pre, error_word=plan.err)
     e.record()
@@ -263,7 +274,7 @@ def kernel_roofline(problem, tls, device):
     pcg_s = s.elapsed_time(e) / 1e3
     applications = res.iterations + res.residual_checks
     return dict(schur_s=schur_s, schur_bytes=schur_bytes, normal_s=normal_s, normal_bytes=normal_bytes,
-                nedges=E, pcg_s=pcg_s, pcg_applications=applications)
+                normal_two_pass_s=two_pass_s, nedges=E, pcg_s=pcg_s, pcg_applications=applications)
 
 
 def e2e_steps(data, tls, device, steps, precision):
@@ -373,18 +384,15 @@ def run_pose(args, world, rank, local):
     J = problem.linearize(jacobian_dtype=torch.float32).jacobian
     v = torch.randn(J.shape[1], device=device, dtype=torch.float64)
     y = torch.empty_like(v)
-    nargs = J.normal_args(torch.float64, 1e-3)
     stream = L.stream_handle(device)
-    for _ in range(5):
-        L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 50
-    ev0.record()
-    for _ in range(reps):
-        L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
-    ev1.record()
-    torch.cuda.synchronize(device)
-    normal_s = ev0.elapsed_time(ev1) / 1e3 / reps
+    normal = {}
+    for tiles in (True, False):
+        nargs = J.normal_args(torch.float64, 1e-3, tiles=tiles)
+        for _ in range(5):
+            L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
+        normal[tiles] = timed_reps(lambda: L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(),
+                                                  y.data_ptr(), stream), 50, flush)
+    normal_s, two_pass_s = normal[True], normal[False]
     st = J.structure
     nnz = sum(p.count * st.rdims[k] * st.D[k] for k, p in enumerate(st.plans))
     slots = sum(p.count * len(p.type_indices) for p in st.plans)
@@ -408,9 +416,10 @@ def run_pose(args, world, rank, local):
         "lm_iterations": summ.iterations, "cg_iterations": summ.linear_iterations_history,
         "lm_iterations_per_s": summ.iterations / mixed_s, "fp64_s": fp64_s, "fp64_final_cost": s64.final_cost,
         "fp64_cg_iterations": s64.linear_iterations_history, "mixed_speedup_vs_fp64": fp64_s / mixed_s,
-        "roofline": {"kernel": "full normal matvec (factor pass + gather)", "bound": "hbm", "achieved": gbs,
-                     "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
-                     "algorithmic_bytes": normal_bytes, "traffic": None},
+        "roofline": {"kernel": "full normal matvec (normal_tile_kernel + tile_gather_kernel)", "bound": "hbm",
+                     "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
+                     "algorithmic_bytes": normal_bytes, "traffic": None, "two_pass_us": two_pass_s * 1e6,
+                     "l2": "flushed before each application"},
         "gpu_launches": launches, "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -698,8 +707,10 @@ def run_cuda(args, world, rank, local):
         "fp64_final_cost": None if fp64 is None else fp64[1].final_cost,
         "fp64_cg_iterations": None if fp64 is None else fp64[1].linear_iterations_history,
         "mixed_speedup_vs_fp64": None if fp64 is None else fp64[0] / mixed_s,
-        "normal_matvec": {"gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
-                          "bytes": roof["normal_bytes"]},
+        "normal_matvec": {"kernels": "normal_tile_kernel + tile_gather_kernel (one-pass tile plan)",
+                          "gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
+                          "bytes": roof["normal_bytes"], "two_pass_us": roof["normal_two_pass_s"] * 1e6,
+                          "l2": "flushed before each application"},
         "roofline": {"kernel": "schur_pcg_vc_kernel (persistent Schur-PCG: chunk streaming + gather + vector CTA)",
                      "bound": "hbm", "achieved": pcg_gbs, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
                      "frac": pcg_gbs / hbm, "us_per_launch": roof["pcg_s"] * 1e6,

@@ -161,6 +161,50 @@ TLS_API int tls_segment_reduce(const tls_segments* seg, const void* contrib, int
  * y = diag(s) J^T J diag(s) x + damping * x, deterministic.
  * `contrib` is a caller workspace of sum_k N_k * D_k elements of vec_dtype.
  */
+
+/* Tile plan of the one-pass normal operator, built once per incidence
+ * structure by the host (torchls_b200/normal_tiles.py). Factor group k is cut
+ * into tiles of tile_factors[k] consecutive factors; CTA c (global numbering)
+ * runs tiles [cta_tile[c], cta_tile[c + 1]). For each tile, the x values of
+ * its distinct target variables are loaded once into a compact shared buffer,
+ * and every factor's per-slot contribution J_s^T J_f x (float64) goes to a
+ * shared-memory stage at the offset in pos[k][s * N_k + f]; the stage is
+ * ordered by target variable,
+ * so each target's contributions in the tile form one contiguous run, summed
+ * in order. A run is final (written to y), added to the CTA's shared
+ * accumulator, or written to a partial slot; at the end the CTA flushes its
+ * accumulator the same way. A last kernel sums each remaining target's
+ * partials in list order. Fixed orders throughout: bitwise reproducible. */
+typedef struct tls_normal_tiles {
+  int32_t ncta;                                /* CTAs over all factor groups */
+  int32_t ntiles;
+  int32_t stage_doubles;                       /* contribution stage per CTA */
+  int32_t acc_doubles;                         /* accumulator per CTA */
+  int32_t ntargets;                            /* targets the gather kernel finishes */
+  int32_t gather_lanes;                        /* lanes per gather target: power of two <= 32 */
+  int32_t xbuf_doubles;                        /* compact per-tile x buffer */
+  int32_t pad_;
+  int32_t tile_factors[TLS_MAX_FACTOR_GROUPS];
+  int32_t tile_base[TLS_MAX_FACTOR_GROUPS];    /* first tile of group k */
+  int32_t cta_base[TLS_MAX_FACTOR_GROUPS + 1]; /* first CTA of group k's launch */
+  const uint32_t* pos[TLS_MAX_FACTOR_GROUPS];  /* [S_k][N_k] stage offset | x-buffer offset << 16 */
+  const int32_t* cta_tile;    /* [ncta + 1] */
+  const int32_t* tile_run;    /* [ntiles + 1] */
+  const int32_t* run_col;     /* first column of the run's target variable */
+  const int32_t* run_meta;    /* stage start | length << 14 | (dim - 1) << 27 */
+  const int32_t* run_dest;    /* >= 0: partial offset; -1: final; <= -2: accumulator offset -2 - dest */
+  const int32_t* run_xoff;    /* offset of the run's x values in the tile's x buffer */
+  const int32_t* cta_flush;   /* [ncta + 1] */
+  const int32_t* flush_col;
+  const int32_t* flush_meta;  /* accumulator offset | (dim - 1) << 16 */
+  const int32_t* flush_dest;  /* >= 0: partial offset; -1: final */
+  const int32_t* target_col;  /* [ntargets] */
+  const int32_t* target_dim;  /* [ntargets] */
+  const int32_t* target_ptr;  /* [ntargets + 1] into target_src */
+  const int32_t* target_src;  /* partial offsets, in summation order */
+  double* partials;           /* workspace of partial slots */
+} tls_normal_tiles;
+
 typedef struct tls_normal_args {
   int32_t nfactor_groups;
   int32_t nvar_groups;
@@ -173,6 +217,10 @@ typedef struct tls_normal_args {
   const void* scale;          /* [n] or NULL */
   void* contrib;
   double damping;
+  /* one-pass plan for this structure, or NULL (two-pass: factor pass into
+   * `contrib`, then a per-variable gather); products other than the normal
+   * operator always take the two-pass route */
+  const tls_normal_tiles* tiles;
 } tls_normal_args;
 
 TLS_API int tls_normal_matvec(const tls_normal_args* args, const void* x, void* y, tls_stream_t stream);

@@ -20,6 +20,7 @@ STRUCTS = {
     "tls_factor_group": L.FactorGroup,
     "tls_segments": L.Segments,
     "tls_linearize_args": L.LinearizeArgs,
+    "tls_normal_tiles": L.NormalTiles,
     "tls_normal_args": L.NormalArgs,
     "tls_block_group": L.BlockGroup,
     "tls_pcg_control": L.PcgControl,

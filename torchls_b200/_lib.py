@@ -57,12 +57,24 @@ class LinearizeArgs(C.Structure):
     ]
 
 
+class NormalTiles(C.Structure):
+    _fields_ = [
+        ("ncta", i32), ("ntiles", i32), ("stage_doubles", i32), ("acc_doubles", i32), ("ntargets", i32),
+        ("gather_lanes", i32), ("xbuf_doubles", i32), ("pad_", i32), ("tile_factors", i32 * MAX_FACTOR_GROUPS),
+        ("tile_base", i32 * MAX_FACTOR_GROUPS), ("cta_base", i32 * (MAX_FACTOR_GROUPS + 1)),
+        ("pos", vp * MAX_FACTOR_GROUPS), ("cta_tile", vp), ("tile_run", vp), ("run_col", vp), ("run_meta", vp),
+        ("run_dest", vp), ("run_xoff", vp), ("cta_flush", vp), ("flush_col", vp),
+        ("flush_meta", vp), ("flush_dest", vp), ("target_col", vp), ("target_dim", vp), ("target_ptr", vp),
+        ("target_src", vp), ("partials", vp),
+    ]
+
+
 class NormalArgs(C.Structure):
     _fields_ = [
         ("nfactor_groups", i32), ("nvar_groups", i32), ("vec_dtype", i32), ("pad_", i32),
         ("fg", FactorGroup * MAX_FACTOR_GROUPS), ("contrib_offset", i64 * MAX_FACTOR_GROUPS),
         ("vg", VarGroup * MAX_GROUPS), ("seg", Segments * MAX_GROUPS), ("scale", vp), ("contrib", vp),
-        ("damping", f64),
+        ("damping", f64), ("tiles", C.POINTER(NormalTiles)),
     ]
 
 

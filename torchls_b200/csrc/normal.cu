@@ -285,19 +285,26 @@ using namespace tls;
 int tls_normal_gather(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
                       void* pcg_state, cudaStream_t st);
 
-// Number of blocks (and dot partials) of the normal operator's gather kernel.
+int tls_normal_tiles_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* nblocks,
+                           void* pcg_state, cudaStream_t st);
+int tls_normal_tiles_blocks(const tls_normal_args* a);
+
+// Number of dot partials the normal operator writes: one per gather block, or
+// with a tile plan one per tile CTA plus one per gather block.
 int tls_normal_gather_blocks(const tls_normal_args* a) {
+  if (a->tiles) return tls_normal_tiles_blocks(a);
   int blocks = 0;
   for (int i = 0; i < a->nvar_groups; ++i) blocks += gather_blocks_for(a->seg[i]);
   return blocks;
 }
 
-// Shared by tls_normal_matvec and the PCG driver. Returns the number of gather
-// blocks (for dot partials) through *gather_blocks.
+// Shared by tls_normal_matvec and the PCG driver. Returns the number of dot
+// partials written through *gather_blocks.
 int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* dot_partials, int* gather_blocks,
                      void* pcg_state, cudaStream_t st) {
   if (a->nfactor_groups > TLS_MAX_FACTOR_GROUPS || a->nvar_groups > TLS_MAX_GROUPS)
     return tls_set_error(TLS_ERR_INVALID, "too many groups");
+  if (a->tiles) return tls_normal_tiles_apply(a, x, y, dot_partials, gather_blocks, pcg_state, st);
   for (int k = 0; k < a->nfactor_groups; ++k) {
     const tls_factor_group& fg = a->fg[k];
     FactorPass p = make_pass(fg, a->vg);

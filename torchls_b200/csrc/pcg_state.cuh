@@ -38,10 +38,11 @@ __device__ __forceinline__ double block_sum_cg(const double* p, int n, double* s
 
 // Called by every block of an operator's final kernel after thread 0 stored
 // the block's dot partial. The last block to finish computes the curvature
-// p.Ap and alpha = r.z / p.Ap for the PCG update (threadfence reduction).
+// p.Ap (the sum of the first `nsum` partials; default: one per block of this
+// kernel) and alpha = r.z / p.Ap for the PCG update (threadfence reduction).
 template <int BLOCK>
 __device__ __forceinline__ void pcg_operator_epilogue(PcgState* st, const double* partials, int nblocks,
-                                                      double* sm) {
+                                                      double* sm, int nsum = -1) {
   __shared__ int last;
   __threadfence();
   __syncthreads();
@@ -49,7 +50,7 @@ __device__ __forceinline__ void pcg_operator_epilogue(PcgState* st, const double
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const double curv = block_sum_cg<BLOCK>(partials, nblocks, sm);
+  const double curv = block_sum_cg<BLOCK>(partials, nsum < 0 ? nblocks : nsum, sm);
   if (threadIdx.x == 0) {
     st->ticket_op = 0;
     tls_pcg_control& c = st->pub;

@@ -18,6 +18,7 @@ Data layout in HBM (per analysed problem, built once per device):
 
 from __future__ import annotations
 
+import ctypes
 from collections.abc import Iterable
 
 import numpy as np
@@ -209,6 +210,7 @@ class Structure:
         for i, e in enumerate(layout):
             self.vgroups[i] = L.VarGroup(e.offset, e.count, e.dim)
         self.plans = problem.plans
+        self._tiles = None
         self.D, self.W, self.slot_col, self.slot_gram, self.index = [], [], [], [], []
         self.grad_base, self.gram_base, self.res_base, self.obs_base = [], [], [], []
         g = gr = rs = ob = 0
@@ -258,6 +260,26 @@ class Structure:
                 self._keep += [p_t, s_t]
                 lst.append(L.Segments(e.count, width, lanes, 0, p_t.data_ptr(), s_t.data_ptr()))
 
+    def normal_tiles(self):
+        """The one-pass normal operator's tile plan on this device (built on
+        first use, kept with the structure), or None when a factor shape does
+        not fit it (the operator then runs in two passes)."""
+        if self._tiles is None:
+            self._tiles = False
+            if self.device.type == "cuda":
+                from .normal_tiles import FactorGroupShape, build_tile_plan
+
+                groups = [FactorGroupShape(plan.count, [(self.layout[t].offset, self.layout[t].dim,
+                                                         plan.indices[s].numpy())
+                                                        for s, t in enumerate(plan.type_indices)], r)
+                          for plan, r in zip(self.plans, self.rdims)]
+                vg = [(e.offset, e.count, e.dim) for e in self.layout]
+                sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+                tp = build_tile_plan(groups, vg, sms)
+                if tp is not None:
+                    self._tiles = _DeviceTiles(tp, self.device)
+        return self._tiles or None
+
     def factor_group(self, k: int, jac: Tensor | None, jac_stride: int = 0, count=None, start: int = 0):
         plan = self.plans[k]
         fg = L.FactorGroup()
@@ -275,6 +297,39 @@ class Structure:
         fg.jac = None if jac is None else jac.data_ptr() + jac.element_size() * start
         fg.jac_stride = jac_stride
         return fg
+
+
+class _DeviceTiles:
+    """A tile plan's arrays on the device and the ``tls_normal_tiles`` that
+    points at them (kept alive together)."""
+
+    def __init__(self, tp, device):
+        self.plan = tp
+        put = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+        self._keep = []
+        t = L.NormalTiles()
+        t.ncta, t.ntiles = tp.ncta, tp.ntiles
+        t.stage_doubles, t.acc_doubles = tp.stage_doubles, tp.acc_doubles
+        t.ntargets, t.gather_lanes, t.xbuf_doubles = len(tp.target_col), tp.gather_lanes, tp.xbuf_doubles
+        for k in range(len(tp.tile_factors)):
+            t.tile_factors[k] = tp.tile_factors[k]
+            t.tile_base[k] = tp.tile_base[k]
+            if tp.pos[k] is not None:
+                pk = put(tp.pos[k].view(np.int32))
+                self._keep.append(pk)
+                t.pos[k] = pk.data_ptr()
+        for k, v in enumerate(tp.cta_base):
+            t.cta_base[k] = v
+        for name in ("cta_tile", "tile_run", "run_col", "run_meta", "run_dest", "run_xoff", "cta_flush", "flush_col",
+                     "flush_meta", "flush_dest", "target_col", "target_dim", "target_ptr", "target_src"):
+            arr = getattr(tp, name)
+            d = put(arr if len(arr) else np.zeros(1, np.int32))
+            self._keep.append(d)
+            setattr(t, name, d.data_ptr())
+        self.partials = torch.empty(max(tp.npartials, 1), dtype=torch.float64, device=device)
+        t.partials = self.partials.data_ptr()
+        self.struct = t
+        self.pointer = ctypes.pointer(t)
 
 
 class Linearization:

@@ -499,10 +499,11 @@ def pcg(matvec: Callable[[Tensor], Tensor], rhs: Tensor, *, preconditioner=None,
     pre_ok = preconditioner is None or isinstance(preconditioner, BlockJacobiPreconditioner)
     op = _operator_of(matvec)
     if op is not None and pre_ok:
-        kind, obj, damping = op
+        kind, obj, damping, tiles = op
         if kind == "normal":
             ws = DevicePCG(rhs.numel(), rhs.dtype, rhs.device)
-            return ws.run(rhs, config, normal_args=obj.normal_args(rhs.dtype, damping), preconditioner=preconditioner)
+            return ws.run(rhs, config, normal_args=obj.normal_args(rhs.dtype, damping, tiles=tiles),
+                          preconditioner=preconditioner)
         if kind == "schur" and rhs.dtype == obj.linear.vec_dtype:
             ws = DevicePCG(rhs.numel(), rhs.dtype, rhs.device)
             return ws.run(rhs, config, schur_args=obj.args, preconditioner=preconditioner, error_word=obj.plan.err)
@@ -511,14 +512,15 @@ def pcg(matvec: Callable[[Tensor], Tensor], rhs: Tensor, *, preconditioner=None,
 
 def _operator_of(matvec):
     if isinstance(matvec, NormalOperator):
-        return "normal", matvec.jacobian, matvec.damping
+        return "normal", matvec.jacobian, matvec.damping, True
     if isinstance(matvec, partial) and getattr(matvec.func, "__func__", None) is BlockJacobian.normal_matvec:
-        return "normal", matvec.func.__self__, float(matvec.keywords.get("damping", 0.0))
+        kw = matvec.keywords
+        return "normal", matvec.func.__self__, float(kw.get("damping", 0.0)), bool(kw.get("tiles", True))
     self_ = getattr(matvec, "__self__", None)
     if isinstance(self_, BlockJacobian) and getattr(matvec, "__func__", None) is BlockJacobian.normal_matvec:
-        return "normal", self_, 0.0
+        return "normal", self_, 0.0, True
     if isinstance(self_, DampedSchurSystem) and getattr(matvec, "__func__", None) is DampedSchurSystem.matvec:
-        return "schur", self_, self_.damping
+        return "schur", self_, self_.damping, True
     return None
 
 

@@ -61,7 +61,10 @@ class BlockJacobian:
             self._scale_cast[dtype] = self.scale.to(dtype).contiguous()
         return self._scale_cast[dtype]
 
-    def normal_args(self, vec_dtype: torch.dtype, damping: float = 0.0) -> L.NormalArgs:
+    def normal_args(self, vec_dtype: torch.dtype, damping: float = 0.0, *, tiles: bool = True) -> L.NormalArgs:
+        """Descriptor of the products on this Jacobian. ``tiles`` attaches the
+        structure's one-pass plan for the normal operator (when it has one);
+        False keeps the two-pass route (factor pass + per-variable gather)."""
         st = self.structure
         a = L.NormalArgs()
         a.nfactor_groups = len(self.jacs)
@@ -79,6 +82,8 @@ class BlockJacobian:
             self._contrib[vec_dtype] = torch.empty(st.grad_size, dtype=vec_dtype, device=self.device)
         a.contrib = self._contrib[vec_dtype].data_ptr()
         a.damping = float(damping)
+        dt = st.normal_tiles() if tiles else None
+        a.tiles = dt.pointer if dt is not None else None
         return a
 
     # ------------------------------------------------------------------ products
@@ -94,7 +99,7 @@ class BlockJacobian:
         self._check_vec(vector, self.shape[1], "matvec")
         v = vector.contiguous()
         out = torch.empty(self.shape[0], dtype=v.dtype, device=v.device)
-        a = self.normal_args(v.dtype)
+        a = self.normal_args(v.dtype, tiles=False)
         L.call("tls_jacobian_matvec", C.byref(a), v.data_ptr(), out.data_ptr(), L.stream_handle(v.device))
         return out
 
@@ -103,16 +108,16 @@ class BlockJacobian:
         self._check_vec(vector, self.shape[0], "rmatvec")
         u = vector.contiguous()
         out = torch.empty(self.shape[1], dtype=u.dtype, device=u.device)
-        a = self.normal_args(u.dtype)
+        a = self.normal_args(u.dtype, tiles=False)
         L.call("tls_jacobian_rmatvec", C.byref(a), u.data_ptr(), out.data_ptr(), L.stream_handle(u.device))
         return out
 
-    def normal_matvec(self, vector: Tensor, damping: float = 0.0) -> Tensor:
+    def normal_matvec(self, vector: Tensor, damping: float = 0.0, *, tiles: bool = True) -> Tensor:
         """diag(s) J^T J diag(s) v + damping * v (sparse.py:83-84)."""
         self._check_vec(vector, self.shape[1], "normal_matvec")
         v = vector.contiguous()
         out = torch.empty_like(v)
-        a = self.normal_args(v.dtype, damping)
+        a = self.normal_args(v.dtype, damping, tiles=tiles)
         L.call("tls_normal_matvec", C.byref(a), v.data_ptr(), out.data_ptr(), L.stream_handle(v.device))
         return out
 
@@ -123,7 +128,7 @@ class BlockJacobian:
         if batch_size < 1:
             raise ValueError("batch_size must be positive")
         v = vector.to(torch.float64).contiguous()
-        a = self.normal_args(torch.float64)
+        a = self.normal_args(torch.float64, tiles=False)
         need = max((n + 127) // 128 for n in (p.count for p in self.structure.plans))
         buf = partials(v.device, max(L.PCG_PARTIALS, need))
         out = torch.empty((), dtype=torch.float64, device=v.device)
