@@ -183,7 +183,7 @@ typedef struct tls_normal_tiles {
   int32_t ntargets;                            /* targets the gather kernel finishes */
   int32_t gather_lanes;                        /* lanes per gather target: power of two <= 32 */
   int32_t xbuf_doubles;                        /* compact per-tile x buffer */
-  int32_t pad_;
+  int32_t nheavy;                              /* the first nheavy targets get a 256-thread block each */
   int32_t tile_factors[TLS_MAX_FACTOR_GROUPS];
   int32_t tile_base[TLS_MAX_FACTOR_GROUPS];    /* first tile of group k */
   int32_t cta_base[TLS_MAX_FACTOR_GROUPS + 1]; /* first CTA of group k's launch */

@@ -60,7 +60,7 @@ class LinearizeArgs(C.Structure):
 class NormalTiles(C.Structure):
     _fields_ = [
         ("ncta", i32), ("ntiles", i32), ("stage_doubles", i32), ("acc_doubles", i32), ("ntargets", i32),
-        ("gather_lanes", i32), ("xbuf_doubles", i32), ("pad_", i32), ("tile_factors", i32 * MAX_FACTOR_GROUPS),
+        ("gather_lanes", i32), ("xbuf_doubles", i32), ("nheavy", i32), ("tile_factors", i32 * MAX_FACTOR_GROUPS),
         ("tile_base", i32 * MAX_FACTOR_GROUPS), ("cta_base", i32 * (MAX_FACTOR_GROUPS + 1)),
         ("pos", vp * MAX_FACTOR_GROUPS), ("cta_tile", vp), ("tile_run", vp), ("run_col", vp), ("run_meta", vp),
         ("run_dest", vp), ("run_xoff", vp), ("cta_flush", vp), ("flush_col", vp),

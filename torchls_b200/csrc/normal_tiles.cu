@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(kTileThreads, (RM * DM <= 18) ? 2 : 1)
                        TV* __restrict__ y, double* __restrict__ dot_partials) {
   extern __shared__ __align__(16) double tile_smem[];
   __shared__ double red[kTileThreads / 32];
+  asm volatile("griddepcontrol.launch_dependents;");
   double* stage = tile_smem;
   double* acc = tile_smem + p.stage_doubles;
   double* xbuf = acc + p.acc_doubles;
@@ -532,6 +533,7 @@ __global__ void __launch_bounds__(kTileThreads, (R * (DA + DB) <= 18) ? 2 : 1)
                         TV* __restrict__ y, double* __restrict__ dot_partials) {
   extern __shared__ __align__(16) double tile_smem[];
   __shared__ double red[kTileThreads / 32];
+  asm volatile("griddepcontrol.launch_dependents;");
   const double dot = tile_cta<R, DA, DB, TJ, TV>(p, blockIdx.x, gridDim.x, tile_smem, x, scale, damping, y);
   if (dot_partials) {
     const double v = block_sum<kTileThreads>(dot, red);
@@ -549,6 +551,7 @@ __global__ void __launch_bounds__(kTileThreads, (R1 * (DA1 + DB1) <= 18 && R2 * 
                             double* __restrict__ dot_partials) {
   extern __shared__ __align__(16) double tile_smem[];
   __shared__ double red[kTileThreads / 32];
+  asm volatile("griddepcontrol.launch_dependents;");
   double dot;
   if ((int)blockIdx.x < g1)
     dot = tile_cta<R1, DA1, DB1, TJ, TV>(p1, blockIdx.x, g1, tile_smem, x, scale, damping, y);
@@ -561,7 +564,7 @@ __global__ void __launch_bounds__(kTileThreads, (R1 * (DA1 + DB1) <= 18 && R2 * 
 }
 
 struct TileGather {
-  int32_t ntargets, lanes;
+  int32_t ntargets, lanes, nheavy, pad_;
   const int32_t* col;
   const int32_t* dim;
   const int32_t* ptr;
@@ -572,48 +575,97 @@ struct TileGather {
 // One aligned lane group per target; lanes stride the target's partials and
 // a fixed butterfly combines them.
 template <int WM, typename TV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     tile_gather_kernel(TileGather g, const TV* __restrict__ x, const TV* __restrict__ scale, double damping,
                        TV* __restrict__ y, double* __restrict__ dot_partials, int dot_base, PcgState* pst) {
   __shared__ double sm[8];
-  const int L = g.lanes;
-  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t t = gt / L;
+  constexpr int B = 4;  // partials per lane in flight
+  // blocks [0, nheavy): a whole block per heavy target; then `lanes` per target
+  __shared__ double hred[256 / 32][WM];
+  const bool heavy = (int)blockIdx.x < g.nheavy;
+  const int L = heavy ? 256 : g.lanes;
+  const int64_t gt = heavy ? (int64_t)threadIdx.x
+                           : (int64_t)(blockIdx.x - g.nheavy) * blockDim.x + threadIdx.x;
+  const int64_t t = heavy ? (int64_t)blockIdx.x : g.nheavy + gt / L;
   const int lane = (int)(gt % L);
+  const bool live = t < g.ntargets;
+  // plan data and x are ready before the tile kernel ends: load them, then
+  // wait for the tile kernel's partials (programmatic dependent launch)
+  int d = 0, b = 0, e = 0;
+  int64_t col = 0;
+  if (live) {
+    d = g.dim[t];
+    b = g.ptr[t];
+    e = g.ptr[t + 1];
+    col = g.col[t];
+  }
+  double xs[WM], sc[WM];
+#pragma unroll
+  for (int c = 0; c < WM; ++c) {
+    xs[c] = 0.0;
+    sc[c] = 1.0;
+    if (live && lane == 0 && c < d) {
+      xs[c] = to_d(x[col + c]);
+      if (scale) sc[c] = to_d(scale[col + c]);
+    }
+  }
+  int off[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) off[q] = b + lane + q * L < e ? __ldg(g.src + b + lane + q * L) : -1;
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   double s[WM];
 #pragma unroll
   for (int c = 0; c < WM; ++c) s[c] = 0.0;
-  int d = 0;
-  if (t < g.ntargets) {
-    d = g.dim[t];
-    const int b = g.ptr[t], e = g.ptr[t + 1];
-    // four partials per lane in flight, added in list order
-    for (int j = b + lane; j < e; j += 4 * L) {
-      int off[4];
+  // B partials per lane in flight, added in list order
+  for (int j = b + lane; j < e; j += B * L) {
+    if (j != b + lane) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) off[q] = j + q * L < e ? __ldg(g.src + j + q * L) : -1;
-      double w[4][WM];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int c = 0; c < WM; ++c) w[q][c] = (off[q] >= 0 && c < d) ? g.partials[off[q] + c] : 0.0;
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (off[q] >= 0) {
-#pragma unroll
-          for (int c = 0; c < WM; ++c)
-            if (c < d) s[c] += w[q][c];
-        }
+      for (int q = 0; q < B; ++q) off[q] = j + q * L < e ? __ldg(g.src + j + q * L) : -1;
     }
-  }
+    double w[B][WM];
 #pragma unroll
-  for (int c = 0; c < WM; ++c) s[c] = group_sum(s[c], L);
+    for (int q = 0; q < B; ++q)
+#pragma unroll
+      for (int c = 0; c < WM; ++c) w[q][c] = (off[q] >= 0 && c < d) ? g.partials[off[q] + c] : 0.0;
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+      if (off[q] >= 0) {
+#pragma unroll
+        for (int c = 0; c < WM; ++c)
+          if (c < d) s[c] += w[q][c];
+      }
+  }
+  if (heavy) {
+    // fixed tree: butterfly within each warp, then the eight warp sums in order
+#pragma unroll
+    for (int c = 0; c < WM; ++c) s[c] = warp_sum(s[c]);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+      for (int c = 0; c < WM; ++c) hred[threadIdx.x >> 5][c] = s[c];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int c = 0; c < WM; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < 256 / 32; ++w) v += hred[w][c];
+        s[c] = v;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < WM; ++c) s[c] = group_sum(s[c], L);
+  }
   double dot = 0.0;
-  if (t < g.ntargets && lane == 0) {
-    const int64_t col = g.col[t];
+  if (live && lane == 0) {
 #pragma unroll
     for (int c = 0; c < WM; ++c)
-      if (c < d) finish_col(col + c, s[c], x, scale, damping, y, dot);
+      if (c < d) {
+        const TV out = static_cast<TV>(s[c] * sc[c] + damping * xs[c]);
+        y[col + c] = out;
+        dot += xs[c] * to_d(out);
+      }
   }
   if (dot_partials) {
     const double v = block_sum<256>(dot, sm);
@@ -622,9 +674,11 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+static int tile_heavy_blocks(const tls_normal_tiles* T) { return T->nheavy; }
+
 static int tile_gather_blocks(const tls_normal_tiles* T) {
-  const int64_t threads = (int64_t)T->ntargets * T->gather_lanes;
-  const int64_t b = (threads + 255) / 256;
+  const int64_t threads = (int64_t)(T->ntargets - T->nheavy) * T->gather_lanes;
+  const int64_t b = tile_heavy_blocks(T) + (threads + 255) / 256;
   return b < 1 ? 1 : (int)b;
 }
 
@@ -750,6 +804,8 @@ static int check_tiles(const tls_normal_args* a) {
     return tls_set_error(TLS_ERR_INVALID, "tile plan: stage, accumulator and x buffer exceed 200 KB of shared memory");
   if (T->gather_lanes < 1 || T->gather_lanes > 32 || (T->gather_lanes & (T->gather_lanes - 1)))
     return tls_set_error(TLS_ERR_INVALID, "tile plan: gather lanes must be a power of two <= 32");
+  if (T->nheavy < 0 || T->nheavy > T->ntargets)
+    return tls_set_error(TLS_ERR_INVALID, "tile plan: heavy targets beyond the target count");
   if (T->cta_base[0] != 0 || T->cta_base[a->nfactor_groups] != T->ncta)
     return tls_set_error(TLS_ERR_INVALID, "tile plan: CTA ranges do not cover the factor groups");
   for (int k = 0; k < a->nfactor_groups; ++k) {
@@ -767,14 +823,31 @@ template <typename TV>
 static int launch_tile_gather(const tls_normal_args* a, const TV* x, const TV* scale, TV* y, double* dot_partials,
                               PcgState* pst, cudaStream_t st) {
   const tls_normal_tiles* T = a->tiles;
-  TileGather g{T->ntargets, T->gather_lanes, T->target_col, T->target_dim, T->target_ptr, T->target_src,
-               T->partials};
+  TileGather g{T->ntargets, T->gather_lanes, T->nheavy, 0, T->target_col, T->target_dim,
+               T->target_ptr, T->target_src, T->partials};
   const int blocks = tile_gather_blocks(T);
   int wmax = 1;
   for (int i = 0; i < a->nvar_groups; ++i) wmax = a->vg[i].dim > wmax ? a->vg[i].dim : wmax;
+  // programmatic dependent launch: the gather's blocks start (and load their
+  // plan data) as the tile kernel's CTAs retire; griddepcontrol.wait orders
+  // their reads of the partials after the whole tile kernel
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const int nbase = T->ncta;
+  const double damping = a->damping;
 #define TLS_TG(WM)                                                                                        \
   if (wmax <= WM) {                                                                                       \
-    tile_gather_kernel<WM, TV><<<blocks, 256, 0, st>>>(g, x, scale, a->damping, y, dot_partials, T->ncta, pst); \
+    cudaError_t err = cudaLaunchKernelEx(&cfg, tile_gather_kernel<WM, TV>, g, x, scale, damping, y,      \
+                                         dot_partials, nbase, pst);                                       \
+    if (err != cudaSuccess) return tls_set_cuda_error(err);                                             \
     TLS_CHECK_LAUNCH();                                                                                   \
     return TLS_OK;                                                                                        \
   }

@@ -37,6 +37,7 @@ MAX_TILE = 1024
 CTAS_PER_SM = 2  # resident CTAs per SM for small factor shapes (r * D <= 18)
 MAX_RUN = (1 << 13) - 1
 MAX_STAGE = 1 << 14
+HEAVY = 32  # partials from which a gather target gets a whole 256-thread block
 
 
 @dataclass
@@ -71,6 +72,7 @@ class TilePlan:
     target_src: np.ndarray
     npartials: int
     gather_lanes: int
+    nheavy: int
     xbuf_doubles: int
     stage_doubles: int = STAGE_DOUBLES
     acc_doubles: int = ACC_DOUBLES
@@ -289,10 +291,20 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
         untouched_d.append(np.full(len(miss), d, np.int64))
     ucols = np.concatenate(untouched_c) if untouched_c else np.zeros(0, np.int64)
     udims = np.concatenate(untouched_d) if untouched_d else np.zeros(0, np.int64)
-    target_col = np.concatenate((tcols, ucols))
-    target_dim = np.concatenate((tdim, udims))
-    target_ptr = np.concatenate(([0], np.cumsum(np.concatenate((counts, np.zeros(len(ucols), np.int64))))))
-    mean = float(counts.mean()) if len(counts) else 1.0
+    # heavy targets (at least HEAVY partials: the cameras) first, a block each;
+    # the rest share `gather_lanes` lanes per target
+    heavy = counts >= HEAVY
+    horder = np.concatenate((np.flatnonzero(heavy), np.flatnonzero(~heavy)))
+    starts = tfirst[horder]
+    counts_o = counts[horder]
+    new_ptr = np.concatenate(([0], np.cumsum(counts_o)))
+    g_src = g_src[np.arange(new_ptr[-1]) - np.repeat(new_ptr[:-1], counts_o) + np.repeat(starts, counts_o)]
+    target_col = np.concatenate((tcols[horder], ucols))
+    target_dim = np.concatenate((tdim[horder], udims))
+    target_ptr = np.concatenate(([0], np.cumsum(np.concatenate((counts_o, np.zeros(len(ucols), np.int64))))))
+    nheavy = int(heavy.sum())
+    light = counts[~heavy]
+    mean = float(light.mean()) if len(light) else 1.0
 
     i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
     run_meta = run_start | (run_len << 14) | ((run_dim - 1) << 27)
@@ -305,5 +317,5 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
                     run_dest=i32(run_dest), run_xoff=i32(run_xoff), xbuf_doubles=xbuf_doubles, cta_flush=cta_flush, flush_col=i32(u_col[fl]),
                     flush_meta=i32(flush_meta), flush_dest=i32(flush_dest), target_col=i32(target_col),
                     target_dim=i32(target_dim), target_ptr=i32(target_ptr), target_src=i32(g_src),
-                    npartials=npartials, gather_lanes=_lanes(mean), stage_doubles=stage_doubles,
+                    npartials=npartials, gather_lanes=_lanes(mean), nheavy=nheavy, stage_doubles=stage_doubles,
                     acc_doubles=acc_doubles, stats=stats)

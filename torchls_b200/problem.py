@@ -311,6 +311,7 @@ class _DeviceTiles:
         t.ncta, t.ntiles = tp.ncta, tp.ntiles
         t.stage_doubles, t.acc_doubles = tp.stage_doubles, tp.acc_doubles
         t.ntargets, t.gather_lanes, t.xbuf_doubles = len(tp.target_col), tp.gather_lanes, tp.xbuf_doubles
+        t.nheavy = tp.nheavy
         for k in range(len(tp.tile_factors)):
             t.tile_factors[k] = tp.tile_factors[k]
             t.tile_base[k] = tp.tile_base[k]
