@@ -124,7 +124,7 @@ def _tile_sizes(groups, budget, stage_doubles, max_tile):
             return (tmax, 0, 0, 1)
         if per is None:
             per = -(-count // (ctas * tmax))
-        T = min(tmax, -(-(-(-count // (ctas * per))) // 32) * 32)
+        T = max(1, min(tmax, -(-count // (ctas * per))))
         nt = -(-count // T)
         return (T, nt, -(-nt // per), per)
 
@@ -312,10 +312,12 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
     stats = dict(ntiles=ntiles, ncta=ncta, nruns=nruns, final_runs=int(final_run.sum()),
                  acc_runs=int(run_acc.sum()), partial_runs=nrp, flushes=len(fl),
                  partial_doubles=npartials, targets=len(target_col))
+    stage_need = max([T * sum(d for _, d, _ in g.slots) for T, g in zip(tile_factors, groups) if g.count] or [0])
+    acc_need = int((acc_off[assigned] + u_dim[assigned]).max()) if assigned.any() else 0
     return TilePlan(tile_factors=tile_factors, tile_base=tile_base, cta_base=cta_base, pos=pos,
                     cta_tile=cta_tile, tile_run=tile_run, run_col=i32(run_col), run_meta=i32(run_meta),
-                    run_dest=i32(run_dest), run_xoff=i32(run_xoff), xbuf_doubles=xbuf_doubles, cta_flush=cta_flush, flush_col=i32(u_col[fl]),
-                    flush_meta=i32(flush_meta), flush_dest=i32(flush_dest), target_col=i32(target_col),
+                    run_dest=i32(run_dest), run_xoff=i32(run_xoff), xbuf_doubles=xbuf_doubles, cta_flush=cta_flush,
+                    flush_col=i32(u_col[fl]),                    flush_meta=i32(flush_meta), flush_dest=i32(flush_dest), target_col=i32(target_col),
                     target_dim=i32(target_dim), target_ptr=i32(target_ptr), target_src=i32(g_src),
-                    npartials=npartials, gather_lanes=_lanes(mean), nheavy=nheavy, stage_doubles=stage_doubles,
-                    acc_doubles=acc_doubles, stats=stats)
+                    npartials=npartials, gather_lanes=_lanes(mean), nheavy=nheavy, stage_doubles=max(stage_need, 1),
+                    acc_doubles=max(acc_need, 1), stats=stats)
