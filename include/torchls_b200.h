@@ -225,6 +225,15 @@ typedef struct tls_normal_args {
 
 TLS_API int tls_normal_matvec(const tls_normal_args* args, const void* x, void* y, tls_stream_t stream);
 
+/* dst[r][p] = src[r][perm[p]] (r < rows, p < ncols; src row stride ld_src,
+ * dst dense): the SoA Jacobian of a factor group in a tile plan's factor
+ * order. A plan may reorder a group's factors (torchls_b200/normal_tiles.py
+ * `perm`) so that a tile's factors share variables; the one-pass operator
+ * then reads that group's J from this copy (fg[k].jac, jac_stride = N_k).
+ * No counterpart in the reference (its operator has no tile plan). */
+TLS_API int tls_permute_columns(const void* src, void* dst, int32_t dtype, int64_t rows, int64_t ncols,
+                                int64_t ld_src, const int32_t* perm, tls_stream_t stream);
+
 /* J diag(s) x per factor row -> out [rows] (factor groups concatenated,
  * factor-major [N][r]); replaces sparse.py:31-41 BlockJacobian.matvec. */
 TLS_API int tls_jacobian_matvec(const tls_normal_args* args, const void* x, void* out_rows, tls_stream_t stream);

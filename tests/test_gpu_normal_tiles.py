@@ -5,8 +5,9 @@ the two-pass operator (factor pass + per-variable gather) and with the
 reference's fixture to 1e-12 relative, for float64 and float32 Jacobians,
 with a column scale and damping, on the small bundle adjustment (two factor
 groups: the fixed camera's observations form a one-slot group) and on a
-pose graph (aliased-slot-free SE(3) between factors plus the edges of the
-fixed first pose). It must be bitwise reproducible, and a PCG driven through
+pose graph (SE(3) between factors plus the edges of the fixed first pose;
+its loop closures come in random order, so the plan reorders the factors
+and the operator reads a tile-ordered copy of J). It must be bitwise reproducible, and a PCG driven through
 it must take the reference's iteration count.
 """
 
@@ -71,7 +72,9 @@ def test_pose_graph(tls):
     data = synthetic.make_pose_graph(400, 1200, seed=4)
     prob = synthetic.build_pose_graph(data, tls, device=DEV)
     J = prob.linearize().jacobian
-    assert J.structure.normal_tiles() is not None
+    tiles = J.structure.normal_tiles()
+    assert tiles is not None
+    assert tiles.perm[0] is not None, "loop closures in random order should be put in tile order"
     gen = torch.Generator().manual_seed(5)
     v = torch.randn(J.shape[1], generator=gen, dtype=torch.float64).to(DEV)
     for damping in (0.0, 1e-2):

@@ -12,7 +12,8 @@ group, an empty group and variables no factor touches; small stages and
 accumulators force multi-tile CTAs and accumulator overflow. They also check
 that no two pairs of a tile share stage space, that each pair's x-buffer
 offset holds its own variable's x, and that every column of y is written
-exactly once.
+exactly once; and that a graph whose edges come in random order is put in
+tile order (a permutation of its factors) with far fewer partials.
 """
 
 from __future__ import annotations
@@ -59,17 +60,18 @@ def _replay(plan, groups, jacs, x, scale, damping):
                 stage = np.full(plan.stage_doubles, np.nan)
                 used = np.zeros(plan.stage_doubles, bool)
                 for f in range(f0, f0 + nt):
+                    fac = f if plan.perm[k] is None else int(plan.perm[k][f])  # tile position -> factor
                     words = [int(plan.pos[k][s * g.count + f]) for s in range(len(g.slots))]
                     xs = np.concatenate([xbuf[(w >> 16):(w >> 16) + d] for w, (_, d, _) in zip(words, g.slots)])
-                    want = np.concatenate([sx[off + int(idx[f]) * d: off + int(idx[f]) * d + d]
+                    want = np.concatenate([sx[off + int(idx[fac]) * d: off + int(idx[fac]) * d + d]
                                            for off, d, idx in g.slots])
                     assert np.array_equal(xs, want), "x buffer offset points at another variable"
-                    q = J[f] @ xs
+                    q = J[fac] @ xs
                     for s, (_, d, _) in enumerate(g.slots):
                         p = words[s] & 0xFFFF
                         assert not used[p:p + d].any(), "two pairs share stage space"
                         used[p:p + d] = True
-                        stage[p:p + d] = J[f][:, cols[s]:cols[s] + d].T @ q
+                        stage[p:p + d] = J[fac][:, cols[s]:cols[s] + d].T @ q
                 for r in range(plan.tile_run[t], plan.tile_run[t + 1]):
                     meta = int(plan.run_meta[r])
                     start, length, d = meta & 0x3FFF, (meta >> 14) & 0x1FFF, ((meta >> 27) & 0xF) + 1
@@ -191,3 +193,22 @@ def test_plan_is_deterministic(sms):
         assert np.array_equal(getattr(a, name), getattr(b, name))
     for pa, pb in zip(a.pos, b.pos):
         assert (pa is None and pb is None) or np.array_equal(pa, pb)
+
+
+def test_random_order_graph_is_reordered_into_local_tiles():
+    # odometry plus near-neighbour loop closures, added in random order
+    rng = np.random.default_rng(11)
+    poses = 400
+    i = np.concatenate((np.arange(poses - 1), rng.integers(0, poses - 4, 800)))
+    j = np.empty_like(i)
+    j[:poses - 1] = np.arange(1, poses)
+    j[poses - 1:] = i[poses - 1:] + rng.integers(2, 4, 800)
+    shuffle = rng.permutation(len(i))
+    g = [FactorGroupShape(len(i), [(0, 6, i[shuffle]), (0, 6, j[shuffle])], 6)]
+    vg = [(0, poses, 6)]
+    kw = dict(num_sms=2, stage_doubles=12 * 128)
+    plan = _check(g, vg, 3, **kw)
+    assert plan.perm[0] is not None and sorted(plan.perm[0].tolist()) == list(range(len(i)))
+    kept = build_tile_plan(g, vg, reorder=False, **kw)
+    assert kept.perm[0] is None
+    assert plan.stats["partial_doubles"] * 5 < kept.stats["partial_doubles"]

@@ -119,6 +119,7 @@ _SIGNATURES = {
     "tls_linearize": [C.POINTER(LinearizeArgs), vp],
     "tls_segment_reduce": [C.POINTER(Segments), vp, i32, i32, i32, vp, i32, vp],
     "tls_normal_matvec": [C.POINTER(NormalArgs), vp, vp, vp],
+    "tls_permute_columns": [vp, vp, i32, i64, i64, i64, vp, vp],
     "tls_jacobian_matvec": [C.POINTER(NormalArgs), vp, vp, vp],
     "tls_squared_matvec_norm": [C.POINTER(NormalArgs), vp, vp, vp, vp],
     "tls_squared_matvec_norm_static": [C.POINTER(NormalArgs), vp, vp, vp],

@@ -960,3 +960,33 @@ int tls_normal_tiles_apply(const tls_normal_args* a, const void* x, void* y, dou
   if (nblocks) *nblocks = tls_normal_tiles_blocks(a);
   return TLS_OK;
 }
+
+// ---------------------------------------------------------------- tile-order copy of J
+namespace tls {
+template <typename T>
+__global__ void __launch_bounds__(256) permute_columns_kernel(const T* __restrict__ src, T* __restrict__ dst,
+                                                              int64_t ncols, int64_t ld, const int32_t* __restrict__ perm) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ncols) return;
+  const int64_t r = blockIdx.y;
+  dst[r * ncols + p] = src[r * ld + __ldg(perm + p)];
+}
+}  // namespace tls
+
+// dst[r][p] = src[r][perm[p]] for r < rows, p < ncols: the columns of an SoA
+// Jacobian [rows][ld] in a tile plan's factor order (coalesced stores).
+extern "C" int tls_permute_columns(const void* src, void* dst, int32_t dtype, int64_t rows, int64_t ncols,
+                                   int64_t ld_src, const int32_t* perm, tls_stream_t stream) {
+  if (rows < 0 || ncols < 0 || ld_src < ncols || rows > 65535 || (dtype != TLS_F32 && dtype != TLS_F64))
+    return tls_set_error(TLS_ERR_INVALID, "tls_permute_columns: bad shape or dtype");
+  if (rows == 0 || ncols == 0) return TLS_OK;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const dim3 grid((unsigned)((ncols + 255) / 256), (unsigned)rows);
+  if (dtype == TLS_F32)
+    permute_columns_kernel<float><<<grid, 256, 0, st>>>((const float*)src, (float*)dst, ncols, ld_src, perm);
+  else
+    permute_columns_kernel<double><<<grid, 256, 0, st>>>((const double*)src, (double*)dst, ncols, ld_src, perm);
+  TLS_CHECK_LAUNCH();
+  return TLS_OK;
+}
+

@@ -55,7 +55,8 @@ class TilePlan:
     tile_factors: list
     tile_base: list
     cta_base: list
-    pos: list  # per group: uint32 [S_k * N_k] (stage offset | x-buffer offset << 16) or None
+    pos: list  # per group: uint32 [S_k * N_k] (stage offset | x-buffer offset << 16), tile order, or None
+    perm: list  # per group: int64 [N_k] factor at each tile position, or None (caller's order)
     cta_tile: np.ndarray
     tile_run: np.ndarray
     run_col: np.ndarray
@@ -144,14 +145,39 @@ def _tile_sizes(groups, budget, stage_doubles, max_tile):
     return out
 
 
+def _tile_order(g: FactorGroupShape, group_count: dict) -> np.ndarray | None:
+    """Factor order for the tiles of one group, or None to keep the caller's.
+
+    Factors are ordered by the smaller (then the larger) index of their slots
+    on the largest variable group (the points of a bundle adjustment, the
+    poses of a pose graph), so that a tile's factors share targets: a pose
+    graph's loop closures, added in random order, then land beside the
+    odometry edges of the same poses. The order is stable; a group already in
+    that order keeps its own (no copy of J is needed then).
+    """
+    if g.count == 0 or not g.slots:
+        return None
+    sizes = [group_count.get(off, 0) for off, _, _ in g.slots]
+    big = max(sizes)
+    keys = [np.asarray(idx, dtype=np.int64) for (_, _, idx), n in zip(g.slots, sizes) if n == big]
+    lo, hi = np.minimum.reduce(keys), np.maximum.reduce(keys)
+    if np.all(lo[1:] >= lo[:-1]):
+        return None  # already ordered by the primary key: keep it
+    return np.lexsort((np.arange(g.count), hi, lo)).astype(np.int64)
+
+
 def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, int, int]], num_sms: int, *,
                     ctas_per_sm: int = CTAS_PER_SM, stage_doubles: int = STAGE_DOUBLES,
-                    acc_doubles: int = ACC_DOUBLES, max_tile: int = MAX_TILE) -> TilePlan | None:
+                    acc_doubles: int = ACC_DOUBLES, max_tile: int = MAX_TILE,
+                    reorder: bool = True) -> TilePlan | None:
     """Plan for factor groups over variable groups ``(offset, count, dim)``.
 
     Returns None when a shape does not fit the one-pass kernel (a variable
     dimension above 16, a tile that cannot hold 32 factors, more than 2^31
-    columns); the operator then takes the two-pass route.
+    columns); the operator then takes the two-pass route. With ``reorder``,
+    a group whose factors are not ordered by their main variable gets a tile
+    order (``perm[k]``: tile position -> factor); the kernels then read J
+    from a copy with its columns in that order (``tls_permute_columns``).
     """
     n = sum(c * d for _, c, d in var_groups)
     if n >= 2**31 or stage_doubles > MAX_STAGE or acc_doubles > 65536:
@@ -163,10 +189,13 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
     if sizes is None:
         return None
     tile_factors, tile_base, cta_base = [], [], [0]
-    cta_tile_parts, pair_parts = [], []
+    cta_tile_parts, pair_parts, perm = [], [], []
+    group_count = {off: c for off, c, _ in var_groups}
     ntiles = 0
     for k, g in enumerate(groups):
         T, nt, G, per = sizes[k]
+        if g.count == 0:
+            perm.append(None)
         tile_factors.append(T)
         tile_base.append(ntiles)
         if G:
@@ -175,8 +204,12 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
         cta_base.append(cta_base[-1] + G)
         if g.count:
             f = np.arange(g.count, dtype=np.int64)
+            order = _tile_order(g, group_count) if reorder else None
+            perm.append(order)
             for s, (off, dim, idx) in enumerate(g.slots):
                 idx = np.asarray(idx, dtype=np.int64)
+                if order is not None:
+                    idx = idx[order]
                 pair_parts.append((ntiles + f // T, off + idx * dim, f % T, np.full(g.count, s, np.int64),
                                    np.full(g.count, dim, np.int64), np.full(g.count, k, np.int64), f))
         ntiles += nt
@@ -314,7 +347,7 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
                  partial_doubles=npartials, targets=len(target_col))
     stage_need = max([T * sum(d for _, d, _ in g.slots) for T, g in zip(tile_factors, groups) if g.count] or [0])
     acc_need = int((acc_off[assigned] + u_dim[assigned]).max()) if assigned.any() else 0
-    return TilePlan(tile_factors=tile_factors, tile_base=tile_base, cta_base=cta_base, pos=pos,
+    return TilePlan(tile_factors=tile_factors, tile_base=tile_base, cta_base=cta_base, pos=pos, perm=perm,
                     cta_tile=cta_tile, tile_run=tile_run, run_col=i32(run_col), run_meta=i32(run_meta),
                     run_dest=i32(run_dest), run_xoff=i32(run_xoff), xbuf_doubles=xbuf_doubles, cta_flush=cta_flush,
                     flush_col=i32(u_col[fl]),                    flush_meta=i32(flush_meta), flush_dest=i32(flush_dest), target_col=i32(target_col),

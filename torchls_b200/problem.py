@@ -327,6 +327,8 @@ class _DeviceTiles:
             d = put(arr if len(arr) else np.zeros(1, np.int32))
             self._keep.append(d)
             setattr(t, name, d.data_ptr())
+        # tile-position -> factor permutations (None: the caller's order)
+        self.perm = [None if q is None else put(q.astype(np.int32)) for q in tp.perm]
         self.partials = torch.empty(max(tp.npartials, 1), dtype=torch.float64, device=device)
         t.partials = self.partials.data_ptr()
         self.struct = t

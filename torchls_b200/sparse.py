@@ -34,9 +34,13 @@ class JacobianGroup:
 
 
 class BlockJacobian:
-    def __init__(self, structure, jacs, gram_contrib, layout, shape, scale: Tensor | None = None):
+    def __init__(self, structure, jacs, gram_contrib, layout, shape, scale: Tensor | None = None,
+                 tile_jacs: dict | None = None):
         self.structure = structure
         self.jacs = jacs
+        # J of reordered factor groups in the tile plan's order, made on first
+        # use and shared by column-scaled views of this Jacobian
+        self._tile_jacs = {} if tile_jacs is None else tile_jacs
         self.gram_contrib = gram_contrib
         self.layout = layout
         self.shape = shape
@@ -84,6 +88,18 @@ class BlockJacobian:
         a.damping = float(damping)
         dt = st.normal_tiles() if tiles else None
         a.tiles = dt.pointer if dt is not None else None
+        if dt is not None:
+            for k, jac in enumerate(self.jacs):
+                if dt.perm[k] is None:
+                    continue
+                j2 = self._tile_jacs.get(k)
+                if j2 is None:
+                    n = st.plans[k].count
+                    j2 = torch.empty_like(jac)
+                    L.call("tls_permute_columns", jac.data_ptr(), j2.data_ptr(), L.dtype_code(jac.dtype),
+                           st.rdims[k] * st.D[k], n, n, dt.perm[k].data_ptr(), L.stream_handle(jac.device))
+                    self._tile_jacs[k] = j2
+                a.fg[k].jac = j2.data_ptr()
         return a
 
     # ------------------------------------------------------------------ products
@@ -143,7 +159,8 @@ class BlockJacobian:
         s = scale.to(torch.float64)
         if self.scale is not None:
             s = self.scale * s
-        return BlockJacobian(self.structure, self.jacs, self.gram_contrib, self.layout, self.shape, s.contiguous())
+        return BlockJacobian(self.structure, self.jacs, self.gram_contrib, self.layout, self.shape, s.contiguous(),
+                             self._tile_jacs)
 
     def diagonal_blocks(self) -> tuple[Tensor, ...]:
         """Exact per-variable J^T J blocks incl. aliased slots (sparse.py:104-121), float64."""
