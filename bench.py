@@ -358,32 +358,14 @@ def pose_opts(tls, precision):
                 termination=tls.TerminationConfig(max_iterations=30), return_summary=True)
 
 
-def run_pose(args, world, rank, local):
-    """SE(3) pose graph: 100,000 poses on a random walk, 99,999 odometry edges
-    and 300,000 loop closures (drawn with replacement among pairs within 3 m),
-    pose 0 fixed; LM with full-system block-Jacobi PCG, 30 iterations."""
+def pose_normal_matvec(problem, init, device, flush):
+    """Full-system normal matvec of the pose graph (float32 J, float64 vectors):
+    seconds per application for the one-pass tile operator and the two-pass
+    one, and the algorithmic bytes."""
     import ctypes
 
-    import torchls_b200 as tls
     from torchls_b200 import _lib as L
-    from torchls_b200 import synthetic
 
-    device = torch.device("cuda", local)
-    torch.cuda.set_device(device)
-    data = synthetic.make_pose_graph(100_000, 300_000, seed=0)
-    problem = synthetic.build_pose_graph(data, tls, device=device)
-    init = {k: v.clone() for k, v in problem.parameters.items()}
-    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=device)
-    target = json.load(open(POSE_TARGET_FILE))["final_cost"] if os.path.exists(POSE_TARGET_FILE) else None
-    barrier(world)
-    with ClockSampler(local) as clocks:
-        times, summ, launches = time_solves(problem, init, tls, "mixed", args.steps, args.warmup, device, flush,
-                                            opts=pose_opts(tls, "mixed"))
-    mixed_s = dist_max(sum(times) / len(times), world, device)
-    t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush,
-                              opts=pose_opts(tls, "native"))
-    fp64_s = dist_max(sum(t64) / len(t64), world, device)
-    # full-system normal matvec on this workload (float32 J, float64 vectors)
     problem.parameters = {k: v.clone() for k, v in init.items()}
     J = problem.linearize(jacobian_dtype=torch.float32).jacobian
     v = torch.randn(J.shape[1], device=device, dtype=torch.float64)
@@ -396,11 +378,41 @@ def run_pose(args, world, rank, local):
             L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(), y.data_ptr(), stream)
         normal[tiles] = timed_reps(lambda: L.call("tls_normal_matvec", ctypes.byref(nargs), v.data_ptr(),
                                                   y.data_ptr(), stream), 50, flush)
-    normal_s, two_pass_s = normal[True], normal[False]
     st = J.structure
     nnz = sum(p.count * st.rdims[k] * st.D[k] for k, p in enumerate(st.plans))
     slots = sum(p.count * len(p.type_indices) for p in st.plans)
-    normal_bytes = nnz * 4 + slots * 4 + 2 * J.shape[1] * 8
+    return normal[True], normal[False], nnz * 4 + slots * 4 + 2 * J.shape[1] * 8
+
+
+def run_pose(args, world, rank, local):
+    """SE(3) pose graph: 100,000 poses on a random walk, 99,999 odometry edges
+    and 300,000 loop closures (drawn with replacement among pairs within 3 m),
+    pose 0 fixed; LM with full-system block-Jacobi PCG, 30 iterations."""
+    import torchls_b200 as tls
+    from torchls_b200 import synthetic
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    data = synthetic.make_pose_graph(100_000, 300_000, seed=0)
+    problem = synthetic.build_pose_graph(data, tls, device=device)
+    init = {k: v.clone() for k, v in problem.parameters.items()}
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    target = json.load(open(POSE_TARGET_FILE))["final_cost"] if os.path.exists(POSE_TARGET_FILE) else None
+    if args.roofline_only:
+        normal_s, two_pass_s, normal_bytes = pose_normal_matvec(problem, init, device, flush)
+        if rank == 0:
+            print(json.dumps({"normal_s": normal_s, "normal_two_pass_s": two_pass_s, "normal_bytes": normal_bytes}),
+                  flush=True)
+        return
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        times, summ, launches = time_solves(problem, init, tls, "mixed", args.steps, args.warmup, device, flush,
+                                            opts=pose_opts(tls, "mixed"))
+    mixed_s = dist_max(sum(times) / len(times), world, device)
+    t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush,
+                              opts=pose_opts(tls, "native"))
+    fp64_s = dist_max(sum(t64) / len(t64), world, device)
+    normal_s, two_pass_s, normal_bytes = pose_normal_matvec(problem, init, device, flush)
     barrier(world)
     if rank != 0:
         return
