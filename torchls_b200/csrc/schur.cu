@@ -428,6 +428,130 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
   }
 }
 
+// Warp per retained variable, for structures whose variables have few run
+// partials each (many small problems merged: a 256-thread block per variable
+// would leave most threads idle and take one block per variable). Lanes take
+// runs lane, lane + 32, ... (four in flight), a fixed butterfly combines them;
+// no dot partials (standalone products only).
+template <int DR, int MODE, typename TV, typename TP>
+__global__ void __launch_bounds__(256) schur_gather_warp_kernel(tls_schur_args a, const TV* __restrict__ x,
+                                                                const double* __restrict__ b,
+                                                                TV* __restrict__ out) {
+  __shared__ double uxs[8][DR * DR];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * 8 + warp;
+  if (i >= a.nretained) return;
+  double* ux = uxs[warp];
+  const TP* part = reinterpret_cast<const TP*>(a.run_partial);
+  if constexpr (MODE == 0) {
+    for (int t = lane; t < DR * DR; t += 32) {
+      const int l = t % DR;
+      const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
+      ux[t] = a.ret_diag[i * DR * DR + t] * (sl * to_d(x[i * DR + l]));
+    }
+  }
+  double acc[DR];
+#pragma unroll
+  for (int k = 0; k < DR; ++k) acc[k] = 0.0;
+  const int rb = __ldg(a.rrun_ptr + i), re = __ldg(a.rrun_ptr + i + 1);
+  for (int j0 = rb + lane; j0 < re; j0 += 128) {
+    TP v[4][DR];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + q * 32;
+#pragma unroll
+      for (int k = 0; k < DR; ++k) v[q][k] = j < re ? part[(int64_t)j * DR + k] : TP(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int k = 0; k < DR; ++k) acc[k] += static_cast<double>(v[q][k]);
+  }
+#pragma unroll
+  for (int k = 0; k < DR; ++k) acc[k] = warp_sum(acc[k]);
+  __syncwarp();
+  if (lane < DR) {
+    const int k = lane;
+    double tot = acc[0];
+#pragma unroll
+    for (int q = 1; q < DR; ++q)
+      if (q == k) tot = acc[q];
+    if constexpr (MODE == 0) {
+      const double xv = to_d(x[i * DR + k]);
+      const double sk = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+      double v = 0.0;
+#pragma unroll
+      for (int l = 0; l < DR; ++l) v += ux[k * DR + l];
+      out[i * DR + k] = static_cast<TV>(sk * v + a.damping * xv - tot);
+    } else {
+      out[i * DR + k] = static_cast<TV>(b[a.retained_offset + i * DR + k] - tot);
+    }
+  }
+}
+
+// Warp per retained variable for the preconditioner blocks: lanes take edges
+// s0 + lane, s0 + lane + 32, ... of each of the variable's cross runs.
+template <int DR, int DE, typename TW>
+__global__ void __launch_bounds__(256) schur_precond_warp_kernel(tls_schur_args a, double* __restrict__ out) {
+  constexpr int NU = DR * (DR + 1) / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * 8 + warp;
+  if (i >= a.nretained) return;
+  double sr[DR];
+#pragma unroll
+  for (int k = 0; k < DR; ++k) sr[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+  double acc[NU];
+#pragma unroll
+  for (int k = 0; k < NU; ++k) acc[k] = 0.0;
+  const int rb = a.rrun_ptr[i], re = a.rrun_ptr[i + 1];
+  for (int j = rb; j < re; ++j) {
+    const int64_t s0 = a.crun_start[j];
+    const int len = a.crun_len[j];
+    for (int64_t s = s0 + lane; s < s0 + len; s += 32) {
+      const int64_t p = a.slab_e[s];
+      double se[DE];
+#pragma unroll
+      for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
+      const double* Li = a.inv_l + p * DE * DE;
+      const double* E = a.cross + s * DR * DE;
+      double wv[DR][DE];
+#pragma unroll
+      for (int r = 0; r < DR; ++r)
+#pragma unroll
+        for (int c = 0; c < DE; ++c) {
+          double v = 0.0;
+#pragma unroll
+          for (int k = 0; k < DE; ++k) v += sr[r] * E[r * DE + k] * se[k] * Li[c * DE + k];
+          wv[r][c] = to_d(static_cast<TW>(v));  // the operator's (stored) precision
+        }
+      int idx = 0;
+#pragma unroll
+      for (int r = 0; r < DR; ++r)
+#pragma unroll
+        for (int q = r; q < DR; ++q) {
+          double v = 0.0;
+#pragma unroll
+          for (int c = 0; c < DE; ++c) v += wv[r][c] * wv[q][c];
+          acc[idx++] += v;
+        }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NU; ++k) acc[k] = warp_sum(acc[k]);
+  if (lane != 0) return;
+  const double* U = a.ret_diag + i * DR * DR;
+  double* o = out + i * DR * DR;
+  int idx = 0;
+#pragma unroll
+  for (int r = 0; r < DR; ++r)
+#pragma unroll
+    for (int q = r; q < DR; ++q) {
+      const double v = sr[r] * U[r * DR + q] * sr[q] - acc[idx++];
+      o[r * DR + q] = v;
+      o[q * DR + r] = v;
+    }
+}
+
 // ---------------------------------------------------------------- persistent Schur-PCG
 // The whole PCG loop on the reduced system in ONE cooperative launch (all
 // CTAs co-resident): per step
@@ -1057,10 +1181,20 @@ struct SchurOps {
     int rc = chunks<0, TW>(a, reinterpret_cast<const double*>(x), s);
     if (rc) return rc;
     if (gblocks) *gblocks = a.nretained;
-    if (a.nretained > 0)
-      schur_gather_kernel<DR, 0, TV, double><<<a.nretained, 256, 0, s>>>(a, x, nullptr, out, dots, pst);
+    if (a.nretained > 0) {
+      if (!dots && !pst && light(a))
+        schur_gather_warp_kernel<DR, 0, TV, double><<<(unsigned)((a.nretained + 7) / 8), 256, 0, s>>>(a, x, nullptr,
+                                                                                                   out);
+      else
+        schur_gather_kernel<DR, 0, TV, double><<<a.nretained, 256, 0, s>>>(a, x, nullptr, out, dots, pst);
+    }
     TLS_CHECK_LAUNCH();
     return TLS_OK;
+  }
+  // many retained variables with few run partials each (merged small
+  // problems): a warp per variable instead of a block
+  static bool light(const tls_schur_args& a) {
+    return a.nretained >= 4096 && (int64_t)a.nruns <= (int64_t)a.nretained * 64;
   }
   template <typename TW, typename TV, typename TA>
   static int rhs(const tls_schur_args& a, const double* b, TV* out, cudaStream_t s) {
@@ -1068,8 +1202,13 @@ struct SchurOps {
     TLS_CHECK_LAUNCH();
     int rc = chunks<1, TW>(a, nullptr, s);
     if (rc) return rc;
-    if (a.nretained > 0)
-      schur_gather_kernel<DR, 1, TV, double><<<a.nretained, 256, 0, s>>>(a, nullptr, b, out, nullptr, nullptr);
+    if (a.nretained > 0) {
+      if (light(a))
+        schur_gather_warp_kernel<DR, 1, TV, double><<<(unsigned)((a.nretained + 7) / 8), 256, 0, s>>>(a, nullptr, b,
+                                                                                                   out);
+      else
+        schur_gather_kernel<DR, 1, TV, double><<<a.nretained, 256, 0, s>>>(a, nullptr, b, out, nullptr, nullptr);
+    }
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }
@@ -1148,7 +1287,12 @@ struct SchurOps {
   }
   template <typename TW>
   static int precond(const tls_schur_args& a, double* out, cudaStream_t s) {
-    if (a.nretained > 0) schur_precond_kernel<DR, DE, TW><<<a.nretained, 256, 0, s>>>(a, out);
+    if (a.nretained > 0) {
+      if (a.nretained >= 4096 && a.nedges <= (int64_t)a.nretained * 1024)
+        schur_precond_warp_kernel<DR, DE, TW><<<(unsigned)((a.nretained + 7) / 8), 256, 0, s>>>(a, out);
+      else
+        schur_precond_kernel<DR, DE, TW><<<a.nretained, 256, 0, s>>>(a, out);
+    }
     TLS_CHECK_LAUNCH();
     return TLS_OK;
   }

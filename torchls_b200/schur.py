@@ -341,7 +341,8 @@ class DampedSchurSystem:
         """(s U s + lambda I) v - W (W^T v) (schur.py:303-328)."""
         v = vector.to(self.linear.vec_dtype).contiguous()
         out = torch.empty_like(v)
-        L.call("tls_schur_matvec", C.byref(self.args), v.data_ptr(), out.data_ptr(), self.stream)
+        # torch's current stream (a CUDA-graph capture stream included)
+        L.call("tls_schur_matvec", C.byref(self.args), v.data_ptr(), out.data_ptr(), L.stream_handle(v.device))
         return out
 
     def preconditioner_blocks(self) -> torch.Tensor:
