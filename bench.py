@@ -39,6 +39,13 @@ TARGET_FILE = os.path.join(ROOT, "tests", "golden", "ba_mid_target.json")
 # + 3 residual checks on the 1M-observation reduced system): 5.990 GB + 0.327 GB
 # (profiles/schur_pcg_kernel_ba_mid_1M.md).
 NCU_TRAFFIC_BYTES = 6_317_141_248
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one full normal matvec
+# through the tile plan (normal_tile_pair_kernel + tile_gather_kernel): the
+# 1M-observation BA (90.04 + 3.78 + 4.83 MB, profiles/normal_tile_ba_mid_1M.md)
+# and the 100k-pose graph (132.67 + 6.00 + 0.38 MB,
+# profiles/normal_tile_pose_graph_100k.md)
+NCU_NORMAL_TRAFFIC_BYTES = 98_648_320
+NCU_POSE_NORMAL_TRAFFIC_BYTES = 139_041_792
 
 
 def parse():
@@ -434,7 +441,8 @@ def run_pose(args, world, rank, local):
         "fp64_cg_iterations": s64.linear_iterations_history, "mixed_speedup_vs_fp64": fp64_s / mixed_s,
         "roofline": {"kernel": "full normal matvec (normal_tile_kernel + tile_gather_kernel)", "bound": "hbm",
                      "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
-                     "algorithmic_bytes": normal_bytes, "traffic": None, "two_pass_us": two_pass_s * 1e6,
+                     "algorithmic_bytes": normal_bytes, "traffic": NCU_POSE_NORMAL_TRAFFIC_BYTES,
+                     "two_pass_us": two_pass_s * 1e6,
                      "l2": "flushed before each application (256 MB write, then read back)"},
         "gpu_launches": launches, "clocks": clocks.summary(),
     }
@@ -725,7 +733,8 @@ def run_cuda(args, world, rank, local):
         "mixed_speedup_vs_fp64": None if fp64 is None else fp64[0] / mixed_s,
         "normal_matvec": {"kernels": "normal_tile_kernel + tile_gather_kernel (one-pass tile plan)",
                           "gbs": normal_gbs, "peak": hbm, "frac": normal_gbs / hbm, "us": roof["normal_s"] * 1e6,
-                          "bytes": roof["normal_bytes"], "two_pass_us": roof["normal_two_pass_s"] * 1e6,
+                          "bytes": roof["normal_bytes"], "traffic": NCU_NORMAL_TRAFFIC_BYTES,
+                          "two_pass_us": roof["normal_two_pass_s"] * 1e6,
                           "l2": "flushed before each application (256 MB write, then read back)"},
         "roofline": {"kernel": "schur_pcg_vc_kernel (persistent Schur-PCG: chunk streaming + gather + vector CTA)",
                      "bound": "hbm", "achieved": pcg_gbs, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",

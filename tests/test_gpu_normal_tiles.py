@@ -8,7 +8,8 @@ groups: the fixed camera's observations form a one-slot group) and on a
 pose graph (SE(3) between factors plus the edges of the fixed first pose;
 its loop closures come in random order, so the plan reorders the factors
 and the operator reads a tile-ordered copy of J). It must be bitwise reproducible, and a PCG driven through
-it must take the reference's iteration count.
+it must take the reference's iteration count. ``tls_permute_columns`` (the
+tile-ordered copy of J) must equal torch's column gather.
 """
 
 from __future__ import annotations
@@ -99,3 +100,16 @@ def test_device_pcg_through_tiles(tls):
                   preconditioner=tls.block_jacobi(J, 1e-3), config=tls.ConjugateGradientConfig())
     assert two.iterations == res.iterations
     close(res.solution, two.solution, 1e-10, what="tiled vs two-pass PCG")
+
+
+def test_permute_columns():
+    from torchls_b200 import _lib as L
+
+    gen = torch.Generator().manual_seed(2)
+    for dtype in (torch.float32, torch.float64):
+        src = torch.randn(7, 1001, generator=gen, dtype=dtype).to(DEV)
+        perm = torch.randperm(1000, generator=gen).to(torch.int32).to(DEV)
+        dst = torch.full((7, 1000), float("nan"), dtype=dtype, device=DEV)
+        L.call("tls_permute_columns", src.data_ptr(), dst.data_ptr(), L.dtype_code(dtype), 7, 1000, 1001,
+               perm.data_ptr(), L.stream_handle(src.device))
+        assert torch.equal(dst, src[:, perm.long()])

@@ -57,6 +57,29 @@ __device__ __forceinline__ double block_sum(double v, double* smem /*[BLOCK/32]*
   return t;  // valid in thread 0
 }
 
+// Three block sums with one exchange: each value takes exactly the tree of
+// block_sum (so the results are bitwise those of three block_sum calls), with
+// two barriers instead of six. Valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ void block_sum3(double& v0, double& v1, double& v2, double (*smem)[BLOCK / 32]) {
+  v0 = warp_sum(v0);
+  v1 = warp_sum(v1);
+  v2 = warp_sum(v2);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smem[0][warp] = v0;
+    smem[1][warp] = v1;
+    smem[2][warp] = v2;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    v0 = warp_sum((lane < BLOCK / 32) ? smem[0][lane] : 0.0);
+    v1 = warp_sum((lane < BLOCK / 32) ? smem[1][lane] : 0.0);
+    v2 = warp_sum((lane < BLOCK / 32) ? smem[2][lane] : 0.0);
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 
 template <typename T>

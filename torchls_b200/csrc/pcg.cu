@@ -224,9 +224,9 @@ __global__ void __launch_bounds__(kSmallThreads) pcg_step_small_kernel(BlockSet 
   if (work)
     pcg_update_blocks<D, TV>(bs, nblocks, threadIdx.x, kSmallThreads, mode, alpha, rhs, x, r, z, p, ap, ztrue, a0,
                              a1, a2);
-  const double t0 = block_sum<kSmallThreads>(a0, sm);
-  const double t1 = block_sum<kSmallThreads>(a1, sm);
-  const double t2 = block_sum<kSmallThreads>(a2, sm);
+  __shared__ double sm3[3][kSmallThreads / 32];
+  block_sum3<kSmallThreads>(a0, a1, a2, sm3);
+  const double t0 = a0, t1 = a1, t2 = a2;
   if (threadIdx.x == 0) {
     pcg_decide(st, t0, t1, t2);
     s_action = st->action;

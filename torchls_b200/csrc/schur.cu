@@ -688,9 +688,9 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
       if (work)
         pcg_update_blocks<D, double, true>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, q.x, q.r, q.z, q.p,
                                            q.ap, q.ztrue, a0, a1, a2);
-      const double t0 = block_sum<kChunkThreads>(a0, smd);
-      const double t1 = block_sum<kChunkThreads>(a1, smd);
-      const double t2 = block_sum<kChunkThreads>(a2, smd);
+      __shared__ double smd3[3][kChunkThreads / 32];
+      block_sum3<kChunkThreads>(a0, a1, a2, smd3);
+      const double t0 = a0, t1 = a1, t2 = a2;
       if (tid == 0) {
         pcg_decide(st, t0, t1, t2);
         s_action = st->action;
@@ -797,9 +797,9 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       if (work)
         pcg_update_blocks<D, double, false>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, x, r, z, p, ap,
                                             q.ztrue, a0, a1, a2);
-      const double t0 = block_sum<kChunkThreads>(a0, smd);
-      const double t1 = block_sum<kChunkThreads>(a1, smd);
-      const double t2 = block_sum<kChunkThreads>(a2, smd);
+      __shared__ double smd3[3][kChunkThreads / 32];
+      block_sum3<kChunkThreads>(a0, a1, a2, smd3);
+      const double t0 = a0, t1 = a1, t2 = a2;
       __shared__ int s_action, s_tofinal;
       __shared__ double s_beta;
       if (tid == 0) {
