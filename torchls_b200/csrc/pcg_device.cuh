@@ -41,20 +41,25 @@ __device__ __forceinline__ void solve_block(const double* __restrict__ L, int di
   for (int i = 0; i < D; ++i)
 #pragma unroll
     for (int k = 0; k <= i; ++k) l[i * (i + 1) / 2 + k] = (i < dim) ? __ldg(L + i * dim + k) : 1.0;
+  // the diagonal's reciprocals first: independent divisions, off the
+  // substitution chains (which then only multiply)
+  double inv[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) inv[i] = (i < dim) ? 1.0 / l[i * (i + 1) / 2 + i] : 0.0;
   double y[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
     double t = r[i];
 #pragma unroll
     for (int k = 0; k < i; ++k) t -= (i < dim) ? l[i * (i + 1) / 2 + k] * y[k] : 0.0;
-    y[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
+    y[i] = (i < dim) ? t * inv[i] : 0.0;
   }
 #pragma unroll
   for (int i = D - 1; i >= 0; --i) {
     double t = y[i];
 #pragma unroll
     for (int k = i + 1; k < D; ++k) t -= (k < dim) ? l[k * (k + 1) / 2 + i] * z[k] : 0.0;
-    z[i] = (i < dim) ? t / l[i * (i + 1) / 2 + i] : 0.0;
+    z[i] = (i < dim) ? t * inv[i] : 0.0;
   }
 }
 
