@@ -34,13 +34,17 @@ __device__ __forceinline__ int find_group(const BlockSet& bs, int64_t b) {
 // The lower triangle is loaded into registers first (independent loads, one
 // memory latency), then the two substitutions run from registers.
 template <int D>
-__device__ __forceinline__ void solve_block(const double* __restrict__ L, int dim, const double (&r)[D],
-                                            double (&z)[D]) {
-  double l[D * (D + 1) / 2];
+__device__ __forceinline__ void load_tri(const double* __restrict__ L, int dim, double (&l)[D * (D + 1) / 2]) {
 #pragma unroll
   for (int i = 0; i < D; ++i)
 #pragma unroll
     for (int k = 0; k <= i; ++k) l[i * (i + 1) / 2 + k] = (i < dim) ? __ldg(L + i * dim + k) : 1.0;
+}
+
+// z = (L L^T)^-1 r with the packed lower triangle l.
+template <int D>
+__device__ __forceinline__ void solve_tri(const double (&l)[D * (D + 1) / 2], int dim, const double (&r)[D],
+                                          double (&z)[D]) {
   // the diagonal's reciprocals first: independent divisions, off the
   // substitution chains (which then only multiply)
   double inv[D];
@@ -61,6 +65,14 @@ __device__ __forceinline__ void solve_block(const double* __restrict__ L, int di
     for (int k = i + 1; k < D; ++k) t -= (k < dim) ? l[k * (k + 1) / 2 + i] * z[k] : 0.0;
     z[i] = (i < dim) ? t * inv[i] : 0.0;
   }
+}
+
+template <int D>
+__device__ __forceinline__ void solve_block(const double* __restrict__ L, int dim, const double (&r)[D],
+                                            double (&z)[D]) {
+  double l[D * (D + 1) / 2];
+  load_tri<D>(L, dim, l);
+  solve_tri<D>(l, dim, r, z);
 }
 
 template <int D>
@@ -184,6 +196,27 @@ __device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nb
     const int dim = g.dim;
     int64_t cols[D];
     block_cols<D>(g, i, cols);
+    // every load of the block before its first store (the stores may alias
+    // the loads' arrays, so the compiler would otherwise order them one by one)
+    const bool solve = mode != M_FINAL && !(bs.identity || g.factor == nullptr);
+    double l[D * (D + 1) / 2];
+    if (solve) load_tri<D>(g.factor + i * dim * dim, dim, l);
+    double v0[D], v1[D], v2[D], v3[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      v0[k] = v1[k] = v2[k] = v3[k] = 0.0;
+      if (k < dim) {
+        const int64_t col = cols[k];
+        if (mode == M_ITER) {
+          v0[k] = to_d(ldv<COH>(x + col));
+          v1[k] = to_d(ldv<COH>(p + col));
+        } else {
+          v0[k] = to_d(rhs[col]);
+        }
+        v2[k] = to_d(ldv<COH>(r + col));
+        v3[k] = to_d(ldv<COH>(ap + col));
+      }
+    }
     double rb[D], zb[D];
     if (mode == M_ITER) {
 #pragma unroll
@@ -191,8 +224,8 @@ __device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nb
         rb[k] = 0.0;
         if (k < dim) {
           const int64_t col = cols[k];
-          x[col] = static_cast<TV>(to_d(ldv<COH>(x + col)) + alpha * to_d(ldv<COH>(p + col)));
-          const TV rn = static_cast<TV>(to_d(ldv<COH>(r + col)) - alpha * to_d(ldv<COH>(ap + col)));
+          x[col] = static_cast<TV>(v0[k] + alpha * v1[k]);
+          const TV rn = static_cast<TV>(v2[k] - alpha * v3[k]);
           r[col] = rn;
           rb[k] = to_d(rn);
         }
@@ -203,22 +236,22 @@ __device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nb
         rb[k] = 0.0;
         if (k < dim) {
           const int64_t col = cols[k];
-          const TV tr = static_cast<TV>(to_d(rhs[col]) - to_d(ldv<COH>(ap + col)));
+          const TV tr = static_cast<TV>(v0[k] - v3[k]);
           ap[col] = tr;
           const double t = to_d(tr);
           rb[k] = t;
           a0 += t * t;
-          const double dr = t - to_d(ldv<COH>(r + col));
+          const double dr = t - v2[k];
           a1 += dr * dr;
         }
       }
     }
     if (mode == M_FINAL) continue;
-    if (bs.identity || g.factor == nullptr) {
+    if (!solve) {
 #pragma unroll
       for (int k = 0; k < D; ++k) zb[k] = rb[k];
     } else {
-      solve_block<D>(g.factor + i * dim * dim, dim, rb, zb);
+      solve_tri<D>(l, dim, rb, zb);
     }
     TV* zdst = (mode == M_ITER) ? z : ztrue;
 #pragma unroll
