@@ -12,8 +12,10 @@ group, an empty group and variables no factor touches; small stages and
 accumulators force multi-tile CTAs and accumulator overflow. They also check
 that no two pairs of a tile share stage space, that each pair's x-buffer
 offset holds its own variable's x, and that every column of y is written
-exactly once; and that a graph whose edges come in random order is put in
-tile order (a permutation of its factors) with far fewer partials.
+exactly once; that a graph whose edges come in random order is put in
+tile order (a permutation of its factors) with far fewer partials; that the
+tiles are spread evenly over the CTAs; and that malformed index arrays are
+rejected.
 """
 
 from __future__ import annotations
@@ -212,3 +214,27 @@ def test_random_order_graph_is_reordered_into_local_tiles():
     kept = build_tile_plan(g, vg, reorder=False, **kw)
     assert kept.perm[0] is None
     assert plan.stats["partial_doubles"] * 5 < kept.stats["partial_doubles"]
+
+
+@pytest.mark.parametrize("count,small", [(995_771, 4_229), (50_000, 0), (1_000, 10)])
+def test_tiles_are_balanced_across_ctas(count, small):
+    # every CTA of the main group carries the same number of tiles (the last
+    # may carry fewer), and the groups together stay within the CTA budget
+    rng = np.random.default_rng(0)
+    pts = max(count // 10, 1)
+    pidx = np.minimum(np.arange(count) // 10, pts - 1)
+    groups = [FactorGroupShape(count, [(0, 6, rng.integers(0, 255, count)), (255 * 6, 3, pidx)], 2)]
+    if small:
+        groups.append(FactorGroupShape(small, [(255 * 6, 3, np.sort(rng.integers(0, pts, small)))], 2))
+    plan = build_tile_plan(groups, [(0, 255, 6), (255 * 6, pts, 3)], num_sms=148)
+    assert plan is not None
+    assert plan.ncta <= 2 * 148
+    per_cta = np.diff(plan.cta_tile[plan.cta_base[0]:plan.cta_base[1] + 1])
+    assert per_cta.max() - per_cta[:-1].min() == 0
+    assert per_cta[-1] <= per_cta[0]
+
+
+def test_plan_rejects_index_arrays_of_the_wrong_length():
+    g = [FactorGroupShape(10, [(0, 6, np.arange(9))])]
+    with pytest.raises(ValueError, match="index"):
+        build_tile_plan(g, [(0, 10, 6)], num_sms=1)

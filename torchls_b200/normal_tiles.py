@@ -179,6 +179,10 @@ def build_tile_plan(groups: list[FactorGroupShape], var_groups: list[tuple[int, 
     order (``perm[k]``: tile position -> factor); the kernels then read J
     from a copy with its columns in that order (``tls_permute_columns``).
     """
+    for k, g in enumerate(groups):
+        for s, (_, _, idx) in enumerate(g.slots):
+            if len(idx) != g.count:
+                raise ValueError(f"factor group {k}, slot {s}: index array of length {len(idx)} for {g.count} factors")
     n = sum(c * d for _, c, d in var_groups)
     if n >= 2**31 or stage_doubles > MAX_STAGE or acc_doubles > 65536:
         return None
