@@ -386,7 +386,10 @@ struct tls_schur_args {
   double* ybuf;                 /* [nelim][de] workspace: L^-1 b_e */
   double damping;
   int32_t* bad;                 /* device: number of non-PD eliminated blocks */
-  int32_t* err;                 /* device: set to 1 if a bounded wait gave up (never expected) */
+  int32_t* err;                 /* device: 1 if a bulk-copy wait gave up, 2 if a grid-barrier wait gave
+                                   up (never expected); cleared (in stream order) by tls_schur_damp, so
+                                   it covers one damped system: its rhs, PCG and back-substitution */
+  int64_t wait_cycles;          /* limit of every bounded wait in SM cycles; <= 0: 2^31 (about a second) */
 };
 
 /* Factor eliminated blocks and whiten every edge (schur.py:263-283). */

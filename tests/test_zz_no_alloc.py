@@ -7,7 +7,8 @@ partials in an array inside the library instead. The test calls it through
 the C ABI twice in a row and compares each result with the buffer-taking
 ``tls_squared_matvec_norm`` (1e-12 relative, the tolerance of the other
 product tests), then checks that an oversized factor group is rejected
-before any work.
+before any work, as are a column scale whose dtype is not float64 and null
+pointers.
 
 The file name makes pytest collect it last, so a run that stops at the first
 failure has already run every other test.
@@ -72,3 +73,25 @@ def test_static_squared_norm_rejects_oversized_groups():
                L.stream_handle(x.device))
     assert L.launch_count() == before
     assert np.isfinite(float(out))
+
+
+def test_static_squared_norm_rejects_bad_arguments():
+    from torchls_b200 import _lib as L
+
+    args = L.NormalArgs()
+    args.nfactor_groups = 0
+    args.vec_dtype = L.dtype_code(torch.float32)
+    scale = torch.ones(8, dtype=torch.float32, device=DEV)
+    args.scale = scale.data_ptr()  # read as float64 by the kernel: must be refused
+    out = torch.zeros((), dtype=torch.float64, device=DEV)
+    x = torch.zeros(8, dtype=torch.float64, device=DEV)
+    before = L.launch_count()
+    with pytest.raises(ValueError, match="float64"):
+        L.call("tls_squared_matvec_norm_static", ctypes.byref(args), x.data_ptr(), out.data_ptr(),
+               L.stream_handle(x.device))
+    with pytest.raises(ValueError, match="null"):
+        L.call("tls_squared_matvec_norm_static", ctypes.byref(args), None, out.data_ptr(),
+               L.stream_handle(x.device))
+    with pytest.raises(ValueError, match="null"):
+        L.call("tls_squared_matvec_norm_static", None, x.data_ptr(), out.data_ptr(), L.stream_handle(x.device))
+    assert L.launch_count() == before

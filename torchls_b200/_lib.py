@@ -102,7 +102,7 @@ class SchurArgs(C.Structure):
         ("retained_offset", i64), ("elim_offset", i64), ("meta", vp), ("slab_r", vp), ("slab_e", vp),
         ("elim_ptr", vp), ("elim_slab", vp), ("rrun_ptr", vp), ("crun_start", vp), ("crun_len", vp),
         ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp), ("w", vp),
-        ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp), ("err", vp),
+        ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp), ("err", vp), ("wait_cycles", i64),
     ]
 
 

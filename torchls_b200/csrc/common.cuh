@@ -4,6 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "torchls_b200.h"
 
 #define TLS_CHECK_LAUNCH()                                   \
@@ -86,6 +90,37 @@ template <typename T>
 __device__ __forceinline__ double to_d(T x) {
   return static_cast<double>(x);
 }
+
+// Launch settings that depend on the device (a function's dynamic shared-memory
+// attribute is set per device; occupancy and SM count are per device): one
+// cache per kernel instantiation, keyed by (current device, key), thread-safe.
+class DeviceGridCache {
+ public:
+  // *out = the cached value for (current device, key); the first call per pair
+  // computes it with compute(device) under the lock (a negative result is a
+  // CUDA failure and is not cached).
+  template <typename F>
+  int get(int key, int* out, F&& compute) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tls_set_cuda_error(e);
+    std::lock_guard<std::mutex> lock(mu_);
+    auto it = values_.find({dev, key});
+    if (it != values_.end()) {
+      *out = it->second;
+      return 0;
+    }
+    const int v = compute(dev);
+    if (v < 0) return tls_set_cuda_error(cudaGetLastError());
+    values_[{dev, key}] = v;
+    *out = v;
+    return 0;
+  }
+
+ private:
+  std::mutex mu_;
+  std::map<std::pair<int, int>, int> values_;
+};
 
 inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
   int64_t g = (n + block - 1) / block;

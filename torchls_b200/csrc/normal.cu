@@ -400,9 +400,22 @@ __global__ void sum_partials_kernel(const double* partials, int count, double* o
   if (threadIdx.x == 0) out[0] = accumulate ? out[0] + s : s;
 }
 
+// Arguments of both |J x|^2 entry points: x and the column scale are read as
+// float64, so a scale of another dtype would be misread.
+static int check_sqnorm_args(const tls_normal_args* a, const double* x, const double* out) {
+  if (!a || !x || !out) return tls_set_error(TLS_ERR_INVALID, "squared_matvec_norm: null args, x or out");
+  if (a->scale && a->vec_dtype != TLS_F64)
+    return tls_set_error(TLS_ERR_INVALID, "squared_matvec_norm: the column scale must be float64 (vec_dtype)");
+  if (a->nfactor_groups < 0 || a->nfactor_groups > TLS_MAX_FACTOR_GROUPS)
+    return tls_set_error(TLS_ERR_INVALID, "squared_matvec_norm: factor group count out of range");
+  return TLS_OK;
+}
+
 extern "C" int tls_squared_matvec_norm(const tls_normal_args* a, const double* x, double* partials, double* out,
                                        tls_stream_t stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (int rc = check_sqnorm_args(a, x, out)) return rc;
+  if (!partials) return tls_set_error(TLS_ERR_INVALID, "squared_matvec_norm: null partials buffer");
   // One launch per factor group; each writes its block partials, then one
   // fixed-order sum accumulates into *out.
   bool first = true;
@@ -489,6 +502,7 @@ int static_scratch(double** out) {
 extern "C" int tls_squared_matvec_norm_static(const tls_normal_args* a, const double* x, double* out,
                                               tls_stream_t stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (int rc = check_sqnorm_args(a, x, out)) return rc;
   for (int k = 0; k < a->nfactor_groups; ++k) {
     if ((a->fg[k].count + 127) / 128 > kStaticSqnormPartials)
       return tls_set_error(TLS_ERR_INVALID,

@@ -76,16 +76,34 @@ __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait on a bulk-copy barrier: gives up after ~2^31 SM cycles (about
-// one second) and flags the error instead of hanging.
-__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
+// Default limit of every bounded wait: 2^31 SM cycles, about one second.
+constexpr long long kWaitCycles = 1LL << 31;
+
+// The wait limit of one launch: a->wait_cycles when positive, else the default.
+__host__ __device__ __forceinline__ long long wait_limit(const tls_schur_args& a) {
+  return a.wait_cycles > 0 ? a.wait_cycles : kWaitCycles;
+}
+
+// Bounded wait on a bulk-copy barrier: gives up after `limit` SM cycles, flags
+// the error and returns false instead of hanging. A caller that sees false
+// must not read the stage (its copy may not have landed).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err,
+                                                  long long limit = kWaitCycles) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 31)) {
+    if (clock64() - t0 > limit) {
       if (err) atomicExch(err, 1);
-      return;
+      return false;
     }
   }
+  return true;
+}
+
+// Wait (with the default limit, whatever the launch's limit) for the bulk
+// copies of consumptions [from, to) that are still in flight into this CTA's
+// shared memory, so that none lands after the CTA has left.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, int from, int to, int32_t* err) {
+  for (int k = from; k < to; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, err);
 }
 
 template <int DR, int DE, int CAP, typename TW, typename TA>
@@ -331,11 +349,17 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     for (int j = tid; j < nx; j += kChunkThreads) x_s[j] = static_cast<TA>(__ldg(x + j));
     __syncthreads();
   }
+  const long long lim = wait_limit(a);
   int it = 0;
   for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x, ++it) {
     const int stg = it & 1;
-    if (tid == 0 && c + (int)gridDim.x < a.nchunks) issue(c + gridDim.x, stg ^ 1);
-    mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+    const bool next = c + (int)gridDim.x < a.nchunks;
+    if (tid == 0 && next) issue(c + gridDim.x, stg ^ 1);
+    const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+    if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
+      if (tid == 0) mbar_drain(bar, it, it + (next ? 2 : 1), a.err);
+      return;
+    }
     const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
     const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
     chunk_compute<DR, DE, CAP, MODE, TW, TA, XS, false>(a, x, x_s, t_s, Ws, Ms, c);
@@ -568,7 +592,7 @@ __global__ void __launch_bounds__(256) schur_precond_warp_kernel(tls_schur_args 
 // runs `tail()` (all its threads) before releasing the others. Waiters poll
 // with a short sleep; false on timeout (about a second).
 template <typename F>
-__device__ __forceinline__ bool grid_barrier(PcgState* st, int32_t* err, F&& tail) {
+__device__ __forceinline__ bool grid_barrier(PcgState* st, int32_t* err, long long limit, F&& tail) {
   __shared__ int ok, last;
   __shared__ uint32_t gen0;
   __syncthreads();
@@ -594,7 +618,7 @@ __device__ __forceinline__ bool grid_barrier(PcgState* st, int32_t* err, F&& tai
     const long long t0 = clock64();
     while (*gen == gen0) {
       __nanosleep(64);
-      if (clock64() - t0 > (1LL << 31)) {
+      if (clock64() - t0 > limit) {
         if (err) atomicExch(err, 2);
         ok = 0;
         break;
@@ -638,7 +662,9 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
   // this CTA's chunks: blockIdx.x + j * gridDim.x, j < kct, cycled every step
   const int kct = (int)blockIdx.x < a.nchunks ? (a.nchunks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * (int)gridDim.x; };
+  const long long lim = wait_limit(a);
   int it = 0;  // chunk consumptions so far; the copy for `it` is always in flight
+  int inflight = 1;  // copies in flight from `it` on when the loop ends
   if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
   for (int step = 0; step < q.steps; ++step) {
     if (tid == 0) {
@@ -648,15 +674,22 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
     __syncthreads();
     if (!s_go) break;
     // ---- A: chunk partials of A p
+    bool failed = false;
     for (int j = 0; j < kct; ++j, ++it) {
       const int stg = it & 1;
       if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
-      mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+      const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+      if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
+        failed = true;
+        inflight = 2;
+        break;
+      }
       const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
       const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
       chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
     }
-    if (!grid_barrier(st, a.err, [] {})) break;
+    if (failed) break;
+    if (!grid_barrier(st, a.err, lim, [] {})) break;
     // ---- B: gather per retained variable
     for (int64_t i = blockIdx.x; i < a.nretained; i += gridDim.x) {
       const double dot = gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
@@ -702,10 +735,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
         pcg_direction_elems<double, true>(q.n, tid, kChunkThreads, s_action, s_beta, s_tofinal != 0, q.x, q.r, q.z,
                                           q.p, q.psave, q.ap, q.ztrue);
     };
-    if (!grid_barrier(st, a.err, phase_c)) break;
+    if (!grid_barrier(st, a.err, lim, phase_c)) break;
   }
-  // drain this CTA's copy in flight before leaving (bounded)
-  if (kct > 0) mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, a.err);
+  // drain this CTA's copies in flight before leaving (bounded)
+  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + inflight, a.err);
   __syncthreads();
 }
 
@@ -763,7 +796,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
         const long long t0 = clock64();
         while (*cnt != (uint32_t)G) {
           __nanosleep(32);
-          if (clock64() - t0 > (1LL << 31)) {
+          if (clock64() - t0 > wait_limit(a)) {
             if (a.err) atomicExch(a.err, 2);
             s_ok = 0;
             break;
@@ -850,7 +883,9 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
   };
   const int kct = (int)blockIdx.x < a.nchunks ? (a.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
   auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * G; };
+  const long long lim = wait_limit(a);
   int it = 0;
+  int inflight = 1;  // copies in flight from `it` on when the loop ends
   if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
   for (int step = 0; step < q.steps; ++step) {
     if (tid == 0) {
@@ -860,14 +895,21 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_go) break;
     // ---- A
+    bool failed = false;
     for (int j = 0; j < kct; ++j, ++it) {
       const int stg = it & 1;
       if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
-      mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err);
+      const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+      if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
+        failed = true;
+        inflight = 2;
+        break;
+      }
       const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
       const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
       chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
     }
+    if (failed) break;
     // ---- barrier over the chunk CTAs
     __syncthreads();
     if (tid == 0) {
@@ -884,7 +926,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
         const long long t0 = clock64();
         while (*gen == gen0) {
           __nanosleep(64);
-          if (clock64() - t0 > (1LL << 31)) {
+          if (clock64() - t0 > lim) {
             if (a.err) atomicExch(a.err, 2);
             s_ok = 0;
             break;
@@ -910,7 +952,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       const long long t0 = clock64();
       while (*gen == gen0) {
         __nanosleep(64);
-        if (clock64() - t0 > (1LL << 31)) {
+        if (clock64() - t0 > lim) {
           if (a.err) atomicExch(a.err, 2);
           s_ok = 0;
           break;
@@ -921,7 +963,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_ok) break;
   }
-  if (kct > 0) mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, a.err);
+  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + inflight, a.err);
   __syncthreads();
 }
 
@@ -1131,17 +1173,18 @@ struct SchurOps {
   template <int MODE, typename TW, int CAP, bool XS>
   static int launch_chunks(const tls_schur_args& a, const double* x, int smem, cudaStream_t s) {
     auto k = schur_chunk_kernel<DR, DE, CAP, MODE, TW, double, XS>;
-    // resident CTAs per SM x SMs for the last shared-memory size, per instantiation
-    static int grid_cap = 0, grid_smem = -1;
-    if (grid_smem != smem) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      int per_sm = 0, dev = 0, sms = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
-      grid_cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-      grid_smem = smem;
-    }
+    // resident CTAs per SM x SMs, per device and shared-memory size, per instantiation
+    static DeviceGridCache cache;
+    int grid_cap = 0;
+    const int rc = cache.get(smem, &grid_cap, [&](int dev) -> int {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      int per_sm = 0, sms = 0;
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
+      if (e != cudaSuccess) return -1;
+      return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    });
+    if (rc) return rc;
     const int grid = a.nchunks < grid_cap ? a.nchunks : grid_cap;
     k<<<grid, kChunkThreads, smem, s>>>(a, x);
     TLS_CHECK_LAUNCH();
@@ -1227,16 +1270,20 @@ struct SchurOps {
     using S = SlabShape<DR, DE, CAP, TW, double>;
     auto k = VC ? schur_pcg_vc_kernel<DR, DE, CAP, TW, D> : schur_pcg_kernel<DR, DE, CAP, TW, D>;
     const int smem = S::kBaseSmem;
-    static int grid = 0;  // co-resident CTAs: per-SM occupancy x SMs, once per instantiation
-    if (grid == 0) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      int per_sm = 0, dev = 0, sms = 0, coop = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
-      grid = (coop && per_sm > 0 && sms > 0) ? per_sm * sms : -1;
-    }
+    // co-resident CTAs (per-SM occupancy x SMs), per device and instantiation;
+    // 0 when the device cannot launch cooperatively
+    static DeviceGridCache cache;
+    int grid = 0;
+    const int rc = cache.get(smem, &grid, [&](int dev) -> int {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      int per_sm = 0, sms = 0, coop = 0;
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
+      if (e != cudaSuccess) return -1;
+      return (coop && per_sm > 0 && sms > 0) ? per_sm * sms : 0;
+    });
+    if (rc) return rc;
     if (grid <= 0) return tls_set_error(TLS_ERR_UNSUPPORTED, "cooperative launch unavailable");
     tls_schur_args aa = a;
     PcgLoop qq = q;
@@ -1271,6 +1318,7 @@ struct SchurOps {
   template <typename TW>
   static int damp(const tls_schur_args& a, cudaStream_t s) {
     cudaMemsetAsync(a.bad, 0, sizeof(int32_t), s);
+    if (a.err) cudaMemsetAsync(a.err, 0, sizeof(int32_t), s);  // the error word describes this system
     if (a.nelim > 0) schur_factor_kernel<DE><<<(a.nelim + 127) / 128, 128, 0, s>>>(a);
     TLS_CHECK_LAUNCH();
     const int64_t nslab = (int64_t)a.nchunks * a.cap;

@@ -89,7 +89,11 @@ class SchurPlan:
         self.global_indices = torch.arange(self.r.offset, self.r.offset + self.r.size, device=device)
         self.layout = (self.r,)
         self.bad = torch.zeros(1, dtype=torch.int32, device=device)
+        # device error word of the bounded waits in the Schur kernels; cleared
+        # in stream order whenever a damped system is built (once per trial)
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        # limit of each bounded device wait in SM cycles (0: about a second)
+        self.wait_cycles = 0
         self._layouts = {}
 
     def chunks_for(self, wdtype) -> ChunkLayout:
@@ -313,6 +317,7 @@ class DampedSchurSystem:
         a.damping = self.damping
         a.bad = p.bad.data_ptr()
         a.err = p.err.data_ptr()
+        a.wait_cycles = int(p.wait_cycles)
         return a
 
     @property

@@ -392,13 +392,15 @@ class DevicePCG:
             ctrl, flags, ev = self._read(words, extra if first else None)
             if first:
                 extra_vals = ev
+            # a wait that ran out left the loop where it was: stop here, not
+            # after further launches
+            if error_word is not None and flags[0] != 0:
+                raise RuntimeError("Schur PCG: a bounded device wait (bulk copy or grid barrier) timed out")
             if ctrl.status != L.PCG_ACTIVE:
                 break
             first = False
             extra_vals = None
             L.call("tls_pcg_run", C.byref(a), pend["batch"], pend["stream"])
-        if error_word is not None and flags[0] != 0:
-            raise RuntimeError("Schur PCG: a bounded device wait (bulk copy or grid barrier) timed out")
         if any(f > 0 for f in flags[1 if error_word is not None else 0 :]):
             raise torch.linalg.LinAlgError("damped block is not positive definite")
         res = PCGResult(self.x.clone(), int(ctrl.iterations), float(ctrl.residual_norm),
