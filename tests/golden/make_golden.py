@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running torchls itself (float64, CPU).
 
-    python tests/golden/make_golden.py /path/to/torchls-checkout
+    python tests/golden/make_golden.py /path/to/torchls-checkout [--only name,name]
 
 Writes ``tests/golden/*.npz`` (arrays) and ``tests/golden/summaries.json``.
 The fixtures pin the numpy oracle (``tests/test_oracle.py``); the CUDA path
@@ -50,9 +50,12 @@ def linearization_record(prefix, lin, out, columns=True):
                 out[f"{prefix}columns{gi}_{si}"] = arr(g.columns[si])
 
 
-def main(reference):
+def main(reference, only=None):
+    """Write every fixture, or (``only``) just the named problems of the
+    second list, merging their summaries into the existing summaries.json."""
     sys.path.insert(0, reference)
     import torchls as tls
+    from torchls.geometry import sim3_exp
     from torchls.schur import SchurLinearization, SchurPlan
 
     import problems as P
@@ -60,9 +63,63 @@ def main(reference):
 
     torch.set_num_threads(8)
     summaries = {}
+    if only:
+        with open(os.path.join(HERE, "summaries.json")) as fh:
+            summaries = json.load(fh)
+
+    # ---------------------------------------------------------------- Sim(3) retraction known answers
+    if not only or "sim3_exp" in only:
+        pose, delta = P.sim3_exp_cases()
+        np.savez_compressed(os.path.join(HERE, "sim3_exp.npz"), pose=arr(pose), delta=arr(delta),
+                            result=arr(pose @ sim3_exp(delta)))
 
     # ---------------------------------------------------------------- small BA (stored inputs)
     data = synthetic.small_bundle_adjustment(0)
+    if only:
+        data = None
+    if data is not None:
+        _small_ba(tls, P, data, summaries, SchurLinearization, SchurPlan)
+
+    # ---------------------------------------------------------------- other problems
+    others = {
+        "ba_tiny": (P.ba_tiny, dict(linear_solver="schur_cg", eliminate="points")),
+        "ba_tiny_gn": (P.ba_tiny, dict(linear_solver="conjugate_gradient", trust_region=None,
+                                       termination=tls.TerminationConfig(max_iterations=8))),
+        "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient",
+                                          termination=tls.TerminationConfig(max_iterations=30))),
+        "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient",
+                                          termination=tls.TerminationConfig(max_iterations=30))),
+        "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
+        "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=tls.TrustRegionConfig(
+            lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
+        "alias_weights": (P.alias_weights, dict()),
+        "alias_cauchy": (lambda api, **k: P.alias_weights(api, loss=P.cauchy_loss(api)), dict()),
+        "alias_softsq": (lambda api, **k: P.alias_weights(api, loss=P.soft_square_loss(api)), dict()),
+        "joint_groups": (P.joint_groups, dict(conjugate_gradient=tls.ConjugateGradientConfig(
+            preconditioner_groups=(("off", "pts"),)))),
+    }
+    for name, (builder, opts) in others.items():
+        if only and name not in only:
+            continue
+        rec = {}
+        p = builder(tls)
+        linearization_record("", p.linearize(), rec)
+        sol, summ = builder(tls).solve(return_summary=True, **opts)
+        for k, val in sol.items():
+            rec[f"solve_{k}"] = arr(val)
+        summaries[name] = summary_dict(summ)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
+        print(name, summ.final_cost, summ.termination_reason, summ.iterations)
+
+    with open(os.path.join(HERE, "summaries.json"), "w") as fh:
+        json.dump(summaries, fh, indent=1, default=float)
+    if "ba_small_schur_cg" in summaries:
+        print("ba_small", summaries["ba_small_schur_cg"]["final_cost"])
+
+
+def _small_ba(tls, P, data, summaries, SchurLinearization, SchurPlan):
+    """The small bundle adjustment with stored inputs: per-kernel products, the
+    Schur system and full solves under several options."""
     out = {
         "cameras_true": arr(data.cameras_true), "points_true": arr(data.points_true),
         "cameras_init": arr(data.cameras_init), "points_init": arr(data.points_init),
@@ -129,38 +186,13 @@ def main(reference):
         summaries[f"ba_small_{name}"] = summary_dict(summ)
     np.savez_compressed(os.path.join(HERE, "ba_small.npz"), **out)
 
-    # ---------------------------------------------------------------- other problems
-    others = {
-        "ba_tiny": (P.ba_tiny, dict(linear_solver="schur_cg", eliminate="points")),
-        "ba_tiny_gn": (P.ba_tiny, dict(linear_solver="conjugate_gradient", trust_region=None,
-                                       termination=tls.TerminationConfig(max_iterations=8))),
-        "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient",
-                                          termination=tls.TerminationConfig(max_iterations=30))),
-        "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
-        "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=tls.TrustRegionConfig(
-            lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
-        "alias_weights": (P.alias_weights, dict()),
-        "alias_cauchy": (lambda api, **k: P.alias_weights(api, loss=P.cauchy_loss(api)), dict()),
-        "alias_softsq": (lambda api, **k: P.alias_weights(api, loss=P.soft_square_loss(api)), dict()),
-        "joint_groups": (P.joint_groups, dict(conjugate_gradient=tls.ConjugateGradientConfig(
-            preconditioner_groups=(("off", "pts"),)))),
-    }
-    for name, (builder, opts) in others.items():
-        rec = {}
-        p = builder(tls)
-        linearization_record("", p.linearize(), rec)
-        sol, summ = builder(tls).solve(return_summary=True, **opts)
-        for k, val in sol.items():
-            rec[f"solve_{k}"] = arr(val)
-        summaries[name] = summary_dict(summ)
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
-        print(name, summ.final_cost, summ.termination_reason, summ.iterations)
-
-    with open(os.path.join(HERE, "summaries.json"), "w") as fh:
-        json.dump(summaries, fh, indent=1, default=float)
-    print("ba_small", summaries["ba_small_schur_cg"]["final_cost"])
-
 
 if __name__ == "__main__":
     sys.path.insert(0, HERE)
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else os.environ.get(
+        "TORCHLS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path to the torchls checkout> "
+                 "(or set TORCHLS_REFERENCE)")
+    only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
+    main(ref, only)

@@ -44,4 +44,8 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TORCHLS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path to the torchls checkout> "
+                 "(or set TORCHLS_REFERENCE)")
+    main(ref)

@@ -82,6 +82,31 @@ def pose_small(api, device="cpu", dtype=torch.float64):
     return synthetic.build_pose_graph(data, api, device=device, dtype=dtype)
 
 
+def sim3_small(api, device="cpu", dtype=torch.float64):
+    """Sim(3) pose graph: 20 poses, 19 odometry + 60 loop edges (sim3_between)."""
+    data = synthetic.make_sim3_pose_graph(20, 60, seed=5)
+    return synthetic.build_pose_graph(data, api, device=device, dtype=dtype, sim3=True)
+
+
+def sim3_exp_cases():
+    """Seeded Sim(3) poses and tangents [t, w, log s] for known-answer tests of
+    the retraction X * Exp(delta): zero, tiny, small and moderate tangents,
+    rotations near pi and large scale changes."""
+    from torchls_b200.geometry import sim3_exp
+
+    g = torch.Generator().manual_seed(29)
+    rnd = lambda n, s: s * torch.randn(n, 7, generator=g, dtype=torch.float64)
+    axis = torch.nn.functional.normalize(torch.randn(4, 3, generator=g, dtype=torch.float64), dim=-1)
+    near_pi = torch.cat((rnd(4, 0.5)[:, :3], axis * 3.1, torch.tensor([[0.3], [-0.2], [0.0], [1e-9]],
+                                                                        dtype=torch.float64)), -1)
+    big_scale = rnd(4, 0.01)
+    big_scale[:, 6] = torch.tensor([1.5, -1.5, 2.5, -2.5], dtype=torch.float64)
+    delta = torch.cat((torch.zeros(1, 7, dtype=torch.float64), rnd(3, 1e-9), rnd(3, 1e-5), rnd(3, 1e-2),
+                       rnd(4, 0.5), near_pi, big_scale, rnd(4, 1.0)))
+    pose = sim3_exp(rnd(len(delta), 0.7))
+    return pose, delta
+
+
 def curve_bounds(api, device="cpu", dtype=torch.float64):
     g = torch.Generator().manual_seed(5)
     x = torch.linspace(0, 4, 60, dtype=torch.float64)

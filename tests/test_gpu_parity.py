@@ -138,6 +138,7 @@ OTHERS = {
     "ba_tiny_gn": (P.ba_tiny, dict(linear_solver="conjugate_gradient", trust_region=None,
                                    termination=dict(max_iterations=8))),
     "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
+    "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
     "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
         lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),

@@ -149,6 +149,7 @@ OTHERS = {
     "ba_tiny_gn": (P.ba_tiny, dict(linear_solver="conjugate_gradient", gauss_newton=True,
                                    termination=dict(max_iterations=8))),
     "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
+    "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
     "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
         lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
@@ -179,3 +180,26 @@ def test_other_problems(name):
     check_summary(s, ref)
     for g, v in zip(prob.groups, vals):
         close(v, fx[f"solve_{g.key}"], 1e-7)
+
+
+def test_sim3_exp_known_answers():
+    """The oracle's and this package's torch Sim(3) exponential against the
+    reference's (torch.matrix_exp) on seeded poses and tangents."""
+    from oracle.geometry import sim3_exp as oracle_exp
+    from torchls_b200.geometry import sim3_exp
+
+    fx = load("sim3_exp")
+    close(fx["pose"] @ oracle_exp(fx["delta"]), fx["result"], 1e-13)
+    close(torch.from_numpy(fx["pose"]) @ sim3_exp(torch.from_numpy(fx["delta"])), fx["result"], 1e-13)
+
+
+def test_sim3_log_inverts_exp():
+    """The torch Sim(3) log (series / closed-form W, adjugate solve) inverts
+    the reference-pinned exponential for rotations below pi."""
+    from torchls_b200.geometry import sim3_exp
+    from torchls_b200.residuals import sim3_log
+
+    fx = load("sim3_exp")
+    delta = torch.from_numpy(fx["delta"])
+    keep = delta[:, 3:6].norm(dim=-1) < 3.0
+    close(sim3_log(sim3_exp(delta[keep])).numpy(), delta[keep].numpy(), 1e-12, 1e-14)

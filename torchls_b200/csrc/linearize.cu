@@ -169,6 +169,43 @@ __device__ __forceinline__ void evaluate(const LinParams& p, int64_t f, double (
         }
       }
     }
+  } else if constexpr (KIND == TLS_RES_SIM3_BETWEEN) {
+    // args: pose_i (4x4 [sR t; 0 1]), pose_j (4x4), measurement Z (4x4)
+    double Si[16], Sj[16], Z[16];
+    const bool vi = p.arg_slot[0] >= 0, vj = p.arg_slot[1] >= 0;
+    const double* pi = vi ? p.arg_data[0] + (int64_t)p.index[p.arg_slot[0]][f] * 16 : p.arg_data[0] + f * p.arg_stride[0];
+    const double* pj = vj ? p.arg_data[1] + (int64_t)p.index[p.arg_slot[1]][f] * 16 : p.arg_data[1] + f * p.arg_stride[1];
+    const double* pz = p.arg_data[2] + f * p.arg_stride[2];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      Si[k] = pi[k];
+      Sj[k] = pj[k];
+      Z[k] = pz[k];
+    }
+    double jr_inv[49], ad[49];
+    sim3_between_residual(Si, Sj, Z, r, p.want_jac ? jr_inv : nullptr, p.want_jac ? ad : nullptr);
+    if (p.want_jac) {
+      const int ci = vi ? p.slot_col[p.arg_slot[0]] : -1;
+      const int cj = vj ? p.slot_col[p.arg_slot[1]] : -1;
+#pragma unroll
+      for (int c = 0; c < DM; ++c) {
+        if (c >= p.D) continue;
+        const bool in_i = ci >= 0 && c >= ci && c < ci + 7;
+        const bool in_j = cj >= 0 && c >= cj && c < cj + 7;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+          double v = 0.0;
+          if (in_j) v += jr_inv[i * 7 + (c - cj)];
+          if (in_i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) acc += jr_inv[i * 7 + k] * ad[k * 7 + (c - ci)];
+            v -= acc;
+          }
+          if (i < RM) J[i][c] = v;
+        }
+      }
+    }
   }
 }
 
@@ -499,6 +536,14 @@ extern "C" int tls_linearize(const tls_linearize_args* a, tls_stream_t stream) {
         return alias ? launch_lin<6, 12, TLS_RES_SE3_BETWEEN, false, false, true>(p, fg.jac_dtype, st)
                      : launch_lin<6, 12, TLS_RES_SE3_BETWEEN, false, false, false>(p, fg.jac_dtype, st);
       return launch_lin<6, 6, TLS_RES_SE3_BETWEEN, false, false, false>(p, fg.jac_dtype, st);
+    }
+    case TLS_RES_SIM3_BETWEEN: {
+      if (fg.rdim != 7) return tls_set_error(TLS_ERR_INVALID, "sim3_between has r = 7");
+      if (fg.total_dim == 14)
+        return alias ? launch_lin<7, 14, TLS_RES_SIM3_BETWEEN, false, false, true>(p, fg.jac_dtype, st)
+                     : launch_lin<7, 14, TLS_RES_SIM3_BETWEEN, false, false, false>(p, fg.jac_dtype, st);
+      if (fg.total_dim != 7) return tls_set_error(TLS_ERR_INVALID, "sim3_between takes Sim(3) slots");
+      return launch_lin<7, 7, TLS_RES_SIM3_BETWEEN, false, false, false>(p, fg.jac_dtype, st);
     }
     default:
       return tls_set_error(TLS_ERR_UNSUPPORTED, "unknown residual kind");

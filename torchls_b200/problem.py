@@ -191,6 +191,10 @@ class CostPlan:
             if any(arg_slot[i] >= 0 and kinds[i] != "se3" for i in range(2)):
                 return None
             return L.RES_SE3_BETWEEN, arg_slot
+        if tag == "sim3_between":
+            if any(arg_slot[i] >= 0 and kinds[i] != "sim3" for i in range(2)):
+                return None
+            return L.RES_SIM3_BETWEEN, arg_slot
         return None
 
 
@@ -436,7 +440,7 @@ class AnalyzedLeastSquaresProblem:
             for plan in self.plans:
                 b = plan.builtin(self.layout)
                 if b is not None:
-                    rdims.append({L.RES_REPROJECTION: 2, L.RES_SE3_BETWEEN: 6}[b[0]])
+                    rdims.append({L.RES_REPROJECTION: 2, L.RES_SE3_BETWEEN: 6, L.RES_SIM3_BETWEEN: 7}[b[0]])
                     continue
                 args = plan.gather(vals, self.layout, device, torch.float64, 0, 1)
                 rdims.append(int(plan.cost.residual_fn(*(a[0] for a in args)).numel()))

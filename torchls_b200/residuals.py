@@ -43,30 +43,70 @@ def sim3_inverse(pose: Tensor) -> Tensor:
     return torch.cat((top, pose[..., 3:4, :]), dim=-2)
 
 
+def sim3_w_coefficients(sigma: Tensor, t2: Tensor):
+    """Coefficients of W(w, sigma) = int_0^1 exp(s (w^ + sigma I)) ds = a0 I + c1 w^ + c2 w^2.
+
+    With z = sigma + i theta (theta^2 = |w|^2 = t2) and F = (e^z - 1) / z:
+    a0 = (e^sigma - 1) / sigma, c1 = Im F / theta, c2 = (a0 - Re F) / theta^2.
+    Where |z| <= 4, or theta^2 < 1e-2 and |sigma| <= 10, the entire series
+    F = sum_k z^k / (k+1)! is summed in (sigma, theta^2) by the recurrences
+    z^k = a_k + i theta b_k, c_k = (sigma^k - a_k) / theta^2 (64 terms); elsewhere
+    the closed forms (theta^2 >= 1e-2 there, so they cancel by at most 100x).
+    Tensor-only, so it works under vmap / jacrev; the CUDA between-factor
+    kernel evaluates the same formulas.
+    """
+    z2 = sigma * sigma + t2
+    series = (z2 <= 16.0) | ((t2 < 1e-2) & (sigma * sigma <= 100.0))
+    # series with inputs kept small where it is not selected (no inf/nan in either branch)
+    ss = torch.where(series, sigma, torch.zeros_like(sigma))
+    st = torch.where(series, t2, torch.zeros_like(t2))
+    a, b, c, sp = torch.ones_like(ss), torch.zeros_like(ss), torch.zeros_like(ss), torch.ones_like(ss)
+    sa, sb, sc = torch.zeros_like(ss), torch.zeros_like(ss), torch.zeros_like(ss)
+    inv = 1.0
+    for k in range(64):
+        inv = inv / (k + 1)
+        sa, sb, sc = sa + inv * sp, sb + inv * b, sc + inv * c
+        a, b, c = ss * a - st * b, a + ss * b, ss * c + b
+        sp = sp * ss
+    # closed forms with inputs kept away from 0 where they are not selected
+    cs_ = torch.where(series, torch.full_like(sigma, 3.0), sigma)
+    ct = torch.where(series, torch.ones_like(t2), t2)
+    th, es = ct.sqrt(), torch.exp(cs_)
+    den = cs_ * cs_ + ct
+    a0c = (es - 1) / cs_
+    ref = (cs_ * (es * torch.cos(th) - 1) + th * es * torch.sin(th)) / den
+    imf = (cs_ * es * torch.sin(th) - th * (es * torch.cos(th) - 1)) / den
+    return (torch.where(series, sa, a0c), torch.where(series, sb, imf / th),
+            torch.where(series, sc, (a0c - ref) / ct))
+
+
+def sim3_left_jacobian(w: Tensor, sigma: Tensor) -> Tensor:
+    """W(w, sigma) = int_0^1 exp(s (w^ + sigma I)) ds, the Sim(3) 'V' matrix."""
+    a0, c1, c2 = sim3_w_coefficients(sigma, (w * w).sum(-1))
+    W = skew(w)
+    eye = torch.eye(3, dtype=w.dtype, device=w.device)
+    return a0[..., None, None] * eye + c1[..., None, None] * W + c2[..., None, None] * (W @ W)
+
+
+def _solve3(M: Tensor, t: Tensor) -> Tensor:
+    """M^-1 t for 3x3 M by the adjugate (tensor-only; no batched LAPACK call)."""
+    c0 = torch.linalg.cross(M[..., 1, :], M[..., 2, :])
+    c1 = torch.linalg.cross(M[..., 2, :], M[..., 0, :])
+    c2 = torch.linalg.cross(M[..., 0, :], M[..., 1, :])
+    det = (M[..., 0, :] * c0).sum(-1)
+    adj = torch.stack((c0, c1, c2), -1)  # columns are the cofactor rows
+    return (adj @ t[..., None]).squeeze(-1) / det[..., None]
+
+
 def sim3_log(pose: Tensor) -> Tensor:
-    """Sim(3) logarithm -> [t(3), w(3), log s], inverse of ``sim3_exp``."""
+    """Sim(3) logarithm -> [t(3), w(3), log s], inverse of ``sim3_exp``:
+    s = sqrt(|sR|_F^2 / 3), w = so3_log(sR / s), t = W(w, log s) u."""
     sr = pose[..., :3, :3]
     s = ((sr * sr).sum((-1, -2)) / 3).sqrt()
     sigma = s.log()
     w = so3_log(sr / s[..., None, None])
-    # Translation part: t = W u, with W = sum_k (A)^k / (k+1)! for the
-    # generator A = w^ + sigma I; solve W u = t via the closed-form W.
-    wmat = sim3_left_jacobian(w, sigma)
-    u = torch.linalg.solve(wmat, pose[..., :3, 3:4]).squeeze(-1)
+    u = _solve3(sim3_left_jacobian(w, sigma), pose[..., :3, 3])
     return torch.cat((u, w, sigma[..., None]), dim=-1)
-
-
-def sim3_left_jacobian(w: Tensor, sigma: Tensor) -> Tensor:
-    """W(w, sigma) = int_0^1 exp(s (w^ + sigma I)) ds, the Sim(3) 'V' matrix.
-
-    Evaluated through ``torch.matrix_exp`` of the 4x4 block generator
-    [[A, I], [0, 0]] whose top-right block equals W (exact for any A).
-    """
-    eye = torch.eye(3, dtype=w.dtype, device=w.device).expand(*w.shape[:-1], 3, 3)
-    a = skew(w) + sigma[..., None, None] * eye
-    zero = torch.zeros_like(a)
-    big = torch.cat((torch.cat((a, eye), -1), torch.cat((zero, zero), -1)), -2)
-    return torch.matrix_exp(big)[..., :3, 3:]
 
 
 def sim3_between(pose_i: Tensor, pose_j: Tensor, measurement: Tensor) -> Tensor:
@@ -90,4 +130,5 @@ def camera_distance_prior(camera: Tensor, reference: Tensor, distance: Tensor) -
 se3_between.cuda_residual = "se3_between"
 sim3_between.cuda_residual = "sim3_between"
 
-__all__ = ["camera_distance_prior", "point_prior", "reprojection", "se3_between", "sim3_between", "sim3_inverse", "sim3_log"]
+__all__ = ["camera_distance_prior", "point_prior", "reprojection", "se3_between", "sim3_between", "sim3_inverse",
+           "sim3_left_jacobian", "sim3_log"]

@@ -23,6 +23,12 @@ Pose graph (``make_pose_graph``)
     with replacement among pose pairs (i, j), j > i + 1, with |p_i - p_j| <= 3.
     Measurements Z = T_i^-1 T_j * se3_exp(noise); initial poses integrate the
     noisy odometry; pose 0 is held fixed (constant data for its edges).
+
+Sim(3) pose graph (``make_sim3_pose_graph``)
+    The same walk and edge rule with a scale drift: pose k stores
+    [s_k R_k, t_k; 0, 1], log s_k a random walk of N(0, scale_sigma^2) steps.
+    Measurements Z = S_i^-1 S_j * sim3_exp([N(0, tn^2)^3, N(0, rn^2)^3,
+    N(0, sn^2)]); initial poses integrate the noisy odometry; pose 0 fixed.
 """
 
 from __future__ import annotations
@@ -33,7 +39,7 @@ from dataclasses import dataclass
 import torch
 from torch import Tensor
 
-from .geometry import se3_exp, se3_inverse
+from .geometry import se3_exp, se3_inverse, sim3_exp
 
 
 @dataclass
@@ -245,6 +251,73 @@ class PoseGraphData:
     measurements: Tensor  # [E, 4, 4]  Z_ij ~ T_i^-1 T_j
 
 
+def _walk(num_poses, g, yaw_sigma):
+    """Unit-step 3D walk: SE(3) poses (yaw only) and positions."""
+    yaw = torch.cumsum(yaw_sigma * torch.randn(num_poses, generator=g, dtype=torch.float64), 0)
+    pitch = 0.05 * torch.randn(num_poses, generator=g, dtype=torch.float64)
+    step = torch.stack((yaw.cos() * pitch.cos(), yaw.sin() * pitch.cos(), pitch.sin()), -1)
+    pos = torch.cat((torch.zeros(1, 3, dtype=torch.float64), torch.cumsum(step[:-1], 0)))
+    rot_vec = torch.zeros(num_poses, 3, dtype=torch.float64)
+    rot_vec[:, 2] = yaw
+    poses = se3_exp(torch.cat((torch.zeros_like(rot_vec), rot_vec), -1))
+    poses[:, :3, 3] = pos
+    return poses, pos
+
+
+def _loop_candidates(pos, loop_radius):
+    """Pose pairs (i, j), j > i + 1, within loop_radius (vectorised in blocks)."""
+    cand_i, cand_j = [], []
+    block = 2048
+    for s in range(0, len(pos), block):
+        d = torch.cdist(pos[s : s + block], pos)
+        ii, jj = (d <= loop_radius).nonzero(as_tuple=True)
+        ii = ii + s
+        keep = jj > ii + 1
+        cand_i.append(ii[keep])
+        cand_j.append(jj[keep])
+    return torch.cat(cand_i), torch.cat(cand_j)
+
+
+def make_sim3_pose_graph(
+    num_poses: int = 60,
+    num_loops: int = 120,
+    *,
+    seed: int = 0,
+    yaw_sigma: float = 0.3,
+    scale_sigma: float = 0.02,
+    rotation_noise: float = 0.01,
+    translation_noise: float = 0.02,
+    scale_noise: float = 0.005,
+    loop_radius: float = 3.0,
+) -> PoseGraphData:
+    from .residuals import sim3_inverse
+
+    g = torch.Generator().manual_seed(seed)
+    poses, pos = _walk(num_poses, g, yaw_sigma)
+    scale = torch.exp(torch.cumsum(scale_sigma * torch.randn(num_poses, generator=g, dtype=torch.float64), 0))
+    poses[:, :3, :3] *= scale[:, None, None]
+    cand_i, cand_j = _loop_candidates(pos, loop_radius)
+    if cand_i.numel() == 0 and num_loops > 0:
+        raise ValueError("no loop-closure candidates")
+    pick = torch.randint(cand_i.numel(), (num_loops,), generator=g)
+    ei = torch.cat((torch.arange(num_poses - 1), cand_i[pick]))
+    ej = torch.cat((torch.arange(1, num_poses), cand_j[pick]))
+    rel = sim3_inverse(poses[ei]) @ poses[ej]
+    noise = torch.cat(
+        (
+            translation_noise * torch.randn(len(ei), 3, generator=g, dtype=torch.float64),
+            rotation_noise * torch.randn(len(ei), 3, generator=g, dtype=torch.float64),
+            scale_noise * torch.randn(len(ei), 1, generator=g, dtype=torch.float64),
+        ),
+        -1,
+    )
+    meas = rel @ sim3_exp(noise)
+    init = [poses[0]]
+    for k in range(num_poses - 1):
+        init.append(init[-1] @ meas[k])
+    return PoseGraphData(poses, torch.stack(init), ei, ej, meas)
+
+
 def make_pose_graph(
     num_poses: int = 1000,
     num_loops: int = 3000,
@@ -256,26 +329,8 @@ def make_pose_graph(
     loop_radius: float = 3.0,
 ) -> PoseGraphData:
     g = torch.Generator().manual_seed(seed)
-    yaw = torch.cumsum(yaw_sigma * torch.randn(num_poses, generator=g, dtype=torch.float64), 0)
-    pitch = 0.05 * torch.randn(num_poses, generator=g, dtype=torch.float64)
-    step = torch.stack((yaw.cos() * pitch.cos(), yaw.sin() * pitch.cos(), pitch.sin()), -1)
-    pos = torch.cat((torch.zeros(1, 3, dtype=torch.float64), torch.cumsum(step[:-1], 0)))
-    rot_vec = torch.zeros(num_poses, 3, dtype=torch.float64)
-    rot_vec[:, 2] = yaw
-    tangent = torch.cat((torch.zeros_like(rot_vec), rot_vec), -1)
-    poses = se3_exp(tangent)
-    poses[:, :3, 3] = pos
-    # Loop candidates: pairs within loop_radius, j > i + 1 (vectorised in blocks).
-    cand_i, cand_j = [], []
-    block = 2048
-    for s in range(0, num_poses, block):
-        d = torch.cdist(pos[s : s + block], pos)
-        ii, jj = (d <= loop_radius).nonzero(as_tuple=True)
-        ii = ii + s
-        keep = jj > ii + 1
-        cand_i.append(ii[keep])
-        cand_j.append(jj[keep])
-    cand_i, cand_j = torch.cat(cand_i), torch.cat(cand_j)
+    poses, pos = _walk(num_poses, g, yaw_sigma)
+    cand_i, cand_j = _loop_candidates(pos, loop_radius)
     if cand_i.numel() == 0 and num_loops > 0:
         raise ValueError("no loop-closure candidates")
     pick = torch.randint(cand_i.numel(), (num_loops,), generator=g)
@@ -297,13 +352,17 @@ def make_pose_graph(
 
 
 def build_pose_graph(data: PoseGraphData, api, *, device="cpu", dtype=torch.float64, loss=None,
-                     residual=None):
-    """``Problem`` over poses 1..N-1; pose 0 is constant data in its edges."""
+                     residual=None, sim3=False):
+    """``Problem`` over poses 1..N-1; pose 0 is constant data in its edges.
+    ``sim3``: Sim(3) poses with the ``sim3_between`` residual."""
     if residual is None:
-        from .residuals import se3_between as residual
+        if sim3:
+            from .residuals import sim3_between as residual
+        else:
+            from .residuals import se3_between as residual
     problem = api.Problem(
         {"poses": data.poses_init[1:].to(device=device, dtype=dtype)},
-        manifolds={"poses": api.SE3Var},
+        manifolds={"poses": api.Sim3Var if sim3 else api.SE3Var},
     )
     free = (data.edge_i > 0) & (data.edge_j > 0)
     problem.add_residual(
