@@ -33,7 +33,7 @@ import torch
 from torch import Tensor
 
 from .problem import _is_ref
-from .variables import EuclideanGroup
+from .variables import euclidean_type
 
 __all__ = ["newton_polish", "objective", "solve_implicit"]
 
@@ -42,7 +42,7 @@ def _groups(problem):
     """(name, values, Var spec, tangent dim, count, offset) per parameter group."""
     out, off = [], 0
     for name, value in problem.parameters.items():
-        spec = problem.manifolds.get(name) or EuclideanGroup(tuple(value.shape[1:]))
+        spec = problem.manifolds.get(name) or euclidean_type(tuple(value.shape[1:]))
         dim = int(spec.tangent_dim)
         count = int(value.shape[0])
         out.append((name, spec, dim, count, off))

@@ -1,10 +1,16 @@
-"""``Cost`` records and the ``Cost.factory`` decorator (torchls cost.py:16-68)."""
+"""Residual batches of the typed API: ``Cost`` and ``Cost.factory``.
+
+The interface (field names, defaults, the decorator and the errors it raises)
+is torchls ``cost.py:16-68``; a ``Cost`` is one batch of single-observation
+residuals over ``Var`` handles (or ``("name", idx)`` bindings made by
+``Problem.add_residual``) and data.
+"""
 
 from __future__ import annotations
 
 from collections.abc import Callable
 from dataclasses import dataclass
-from functools import wraps
+from functools import update_wrapper
 from typing import Literal
 
 from torch import Tensor
@@ -13,15 +19,23 @@ from .batching import AutoBatchSize, BatchSize
 from .losses import Loss
 
 JacMode = Literal["auto", "reverse", "forward"]
+_JAC_MODES = frozenset(("auto", "reverse", "forward"))
+
+
+def _positive_int(x) -> bool:
+    return isinstance(x, int) and not isinstance(x, bool) and x > 0
 
 
 @dataclass(frozen=True)
 class Cost:
-    """One batch of residuals; functions receive local values, not Var handles.
+    """One batch of residuals; ``residual_fn`` sees one observation's values.
 
-    Tensor data defaults to a leading observation axis (length one broadcasts);
-    ``in_dims=None`` marks data shared by every observation. Weights scale each
-    observation's objective after its loss.
+    ``args`` mixes variable handles and data. Data carries a leading
+    observation axis (length one broadcasts) unless its ``in_dims`` entry is
+    None (shared by all observations). ``jacobian_fn`` (optional) returns one
+    raw-residual Jacobian per variable argument; ``loss`` then ``weights``
+    shape each observation's contribution to the objective. ``batch_size``
+    chunks the torch.func linearization of user residuals (None: one chunk).
     """
 
     residual_fn: Callable[..., Tensor]
@@ -34,27 +48,33 @@ class Cost:
     weights: Tensor | float | None = None
 
     def __post_init__(self):
-        if self.loss is not None and not isinstance(self.loss, Loss):
+        problems = []
+        if not (self.loss is None or isinstance(self.loss, Loss)):
             raise TypeError("loss must be a Loss instance such as HuberLoss, or None")
-        if self.jac_mode not in ("auto", "reverse", "forward"):
-            raise ValueError("jac_mode must be auto, reverse or forward")
-        if self.batch_size is not None and not isinstance(self.batch_size, AutoBatchSize):
-            if isinstance(self.batch_size, bool) or not isinstance(self.batch_size, int) or self.batch_size <= 0:
-                raise ValueError("batch_size must be a positive integer, AutoBatchSize, or None")
-        if self.in_dims is not None and (
-            len(self.in_dims) != len(self.args) or any(x not in (0, None) for x in self.in_dims)
-        ):
-            raise ValueError("in_dims must contain one 0 or None per argument")
+        if self.jac_mode not in _JAC_MODES:
+            problems.append("jac_mode must be auto, reverse or forward")
+        if not (self.batch_size is None or isinstance(self.batch_size, AutoBatchSize)
+                or _positive_int(self.batch_size)):
+            problems.append("batch_size must be a positive integer, AutoBatchSize, or None")
+        if self.in_dims is not None:
+            ok = len(self.in_dims) == len(self.args) and all(d is None or d == 0 for d in self.in_dims)
+            if not ok:
+                problems.append("in_dims must contain one 0 or None per argument")
+        if problems:
+            raise ValueError(problems[0])
 
     @staticmethod
     def factory(fn=None, **options):
-        """Decorate a single-observation residual to create batched Costs."""
+        """Turn a single-observation residual into a Cost builder:
+        ``make = Cost.factory(residual, loss=...); make(var_a, var_b, data)``.
+        Usable bare (``@Cost.factory``) or with options (``@Cost.factory(...)``)."""
 
-        def decorate(residual_fn):
-            @wraps(residual_fn)
-            def make(*args):
+        def builder_for(residual_fn):
+            def build(*args):
                 return Cost(residual_fn, args, **options)
 
-            return make
+            return update_wrapper(build, residual_fn)
 
-        return decorate(fn) if fn is not None else decorate
+        if fn is None:
+            return builder_for
+        return builder_for(fn)
