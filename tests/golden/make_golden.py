@@ -73,6 +73,22 @@ def main(reference, only=None):
         np.savez_compressed(os.path.join(HERE, "sim3_exp.npz"), pose=arr(pose), delta=arr(delta),
                             result=arr(pose @ sim3_exp(delta)))
 
+    # ---------------------------------------------------------------- typed API (Cost.factory / VarValues)
+    if not only or "typed_ba" in only:
+        problem, init = P.typed_ba(tls)
+        rec = {"offsets": np.array([e.offset for e in problem.layout]),
+               "dims": np.array([e.dim for e in problem.layout])}
+        for i, e in enumerate(problem.layout):
+            rec[f"ids{i}"] = arr(e.ids)
+        linearization_record("", problem.linearize(init), rec)
+        sol, summ = problem.solve(init, return_summary=True, linear_solver="schur_cg",
+                                  eliminate=problem.layout[0].var_type)
+        for i, e in enumerate(problem.layout):
+            rec[f"solve{i}"] = arr(sol._values[e.var_type])
+        summaries["typed_ba"] = summary_dict(summ)
+        np.savez_compressed(os.path.join(HERE, "typed_ba.npz"), **rec)
+        print("typed_ba", summ.final_cost, summ.termination_reason, summ.iterations)
+
     # ---------------------------------------------------------------- small BA (stored inputs)
     data = synthetic.small_bundle_adjustment(0)
     if only:

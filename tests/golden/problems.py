@@ -88,6 +88,34 @@ def sim3_small(api, device="cpu", dtype=torch.float64):
     return synthetic.build_pose_graph(data, api, device=device, dtype=dtype, sim3=True)
 
 
+def typed_ba(api, device="cpu", dtype=torch.float64):
+    """The tiny bundle adjustment through the typed API (``Cost.factory``,
+    ``Cost``, ``LeastSquaresProblem``, ``VarValues.make``) with sparse, unsorted
+    IDs: free cameras 30, 10, 20 (camera 0 is constant data), points
+    100 + 3 * (39 - p). Returns the analysed problem and the initial values."""
+    data = synthetic.make_bundle_adjustment(4, 40, 3, seed=7)
+
+    class PointVar(api.Var, default_factory=lambda: torch.zeros(3)):
+        """A Euclidean 3-vector (typed API)."""
+
+    cam_ids = torch.tensor([30, 10, 20])
+    pt_ids = 100 + 3 * torch.arange(39, -1, -1)
+    free, fixed = data.split_fixed_camera()
+    to = dict(device=device, dtype=dtype)
+    huber = api.HuberLoss(0.01)
+    observe = api.Cost.factory(reprojection, loss=huber)
+    costs = [
+        observe(api.SE3Var(cam_ids[data.camera_index[free] - 1]), PointVar(pt_ids[data.point_index[free]]),
+                data.uv[free].to(**to)),
+        api.Cost(reprojection, (data.cameras_true[0].to(**to), PointVar(pt_ids[data.point_index[fixed]]),
+                                data.uv[fixed].to(**to)), in_dims=(None, 0, 0), loss=huber),
+    ]
+    problem = api.LeastSquaresProblem(costs, [PointVar(pt_ids), api.SE3Var(cam_ids)]).analyze()
+    init = api.VarValues.make([api.SE3Var(cam_ids).with_value(data.cameras_init[1:].to(**to)),
+                               PointVar(pt_ids).with_value(data.points_init.to(**to))])
+    return problem, init
+
+
 def sim3_exp_cases():
     """Seeded Sim(3) poses and tangents [t, w, log s] for known-answer tests of
     the retraction X * Exp(delta): zero, tiny, small and moderate tangents,

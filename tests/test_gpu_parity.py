@@ -175,3 +175,22 @@ def test_other_problems(tls, name):
     check_summary(s, SUMMARIES[name], cg_slack=2 if name == "pose_small" else 0)
     for key, val in sol.items():
         close(val, fx[f"solve_{key}"], 1e-7, 1e-12, what=key)
+
+
+def test_typed_api_solve(tls):
+    """Cost.factory / LeastSquaresProblem / VarValues with sparse unsorted IDs:
+    linearization and the Schur-CG solve against the reference's fixture."""
+    fx = load("typed_ba")
+    problem, init = P.typed_ba(tls, device=DEV)
+    lin = problem.linearize(init)
+    close(lin.residual, fx["residual"], 1e-11, 1e-15, what="residual")
+    close(lin.gradient, fx["gradient"], 1e-10, 1e-13, what="gradient")
+    for gi, g in enumerate(lin.jacobian.groups):
+        for si, (b, c) in enumerate(zip(g.blocks, g.columns)):
+            close(b, fx[f"block{gi}_{si}"], 1e-10, 1e-13, what=f"block{gi}_{si}")
+            np.testing.assert_array_equal(to_np(c), fx[f"columns{gi}_{si}"])
+    sol, s = problem.solve(init, return_summary=True, linear_solver="schur_cg",
+                           eliminate=problem.layout[0].var_type)
+    check_summary(s, SUMMARIES["typed_ba"])
+    for i, e in enumerate(problem.layout):
+        close(sol._values[e.var_type], fx[f"solve{i}"], 1e-8, what=f"solve{i}")

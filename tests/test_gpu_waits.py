@@ -26,7 +26,9 @@ pytestmark = [pytest.mark.gpu, needs_gpu]
 DEV = "cuda"
 
 
-def _solve(tls, prob):
+def _solve(tls, prob, start):
+    # a solve writes its result back into the problem: start each from the same values
+    prob.parameters.update({k: v.clone() for k, v in start.items()})
     return prob.solve(return_summary=True, linear_solver="schur_cg", eliminate="points",
                       termination=tls.TerminationConfig(max_iterations=30))
 
@@ -36,17 +38,19 @@ def test_expired_wait_raises_and_plan_recovers():
 
     fx = load("ba_small")
     prob = P.ba_small(tls, device=DEV, data=stored_ba(fx))
-    sol0, s0 = _solve(tls, prob)
+    start = {k: v.clone() for k, v in prob.parameters.items()}
+    sol0, s0 = _solve(tls, prob, start)
+    assert s0.linear_iterations > 0
     plans = list(prob._ensure_analyzed().__dict__["_schur_plans"].values())
     assert len(plans) == 1
     plan = plans[0]
     plan.wait_cycles = 200
     with pytest.raises(RuntimeError, match="bounded device wait"):
-        _solve(tls, prob)
+        _solve(tls, prob, start)
     torch.cuda.synchronize()
     assert int(plan.err.item()) != 0  # the kernel returned with its error word set
     plan.wait_cycles = 0
-    sol1, s1 = _solve(tls, prob)
+    sol1, s1 = _solve(tls, prob, start)
     assert int(plan.err.item()) == 0
     assert s1.linear_iterations_history == s0.linear_iterations_history
     close(s1.final_cost, s0.final_cost, 1e-14, what="final cost after recovery")
