@@ -105,6 +105,7 @@ def main(reference, only=None):
                                           termination=tls.TerminationConfig(max_iterations=30))),
         "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient",
                                           termination=tls.TerminationConfig(max_iterations=30))),
+        "se2_custom": (P.se2_custom, dict(linear_solver="conjugate_gradient")),
         "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
         "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=tls.TrustRegionConfig(
             lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),

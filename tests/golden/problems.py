@@ -64,6 +64,19 @@ def soft_square_loss(api):
     return SoftSquareLoss()
 
 
+def se2_between(a, b, z):
+    """SE(2) relative-pose error: b expressed in a's frame minus z, angle wrapped."""
+    c, s = torch.cos(a[2]), torch.sin(a[2])
+    dx, dy = b[0] - a[0], b[1] - a[1]
+    e = torch.stack((c * dx + s * dy - z[0], -s * dx + c * dy - z[1], b[2] - a[2] - z[2]))
+    return torch.stack((e[0], e[1], torch.atan2(torch.sin(e[2]), torch.cos(e[2]))))
+
+
+def se2_odometry(a, b, k, z):
+    """Odometry edge whose measured translation is in units of an unknown scale k."""
+    return se2_between(a, b, torch.stack((k[0] * z[0], k[0] * z[1], z[2])))
+
+
 # ---------------------------------------------------------------- builders
 def ba_small(api, device="cpu", dtype=torch.float64, data=None):
     data = data if data is not None else synthetic.small_bundle_adjustment(0)
@@ -86,6 +99,50 @@ def sim3_small(api, device="cpu", dtype=torch.float64):
     """Sim(3) pose graph: 20 poses, 19 odometry + 60 loop edges (sim3_between)."""
     data = synthetic.make_sim3_pose_graph(20, 60, seed=5)
     return synthetic.build_pose_graph(data, api, device=device, dtype=dtype, sim3=True)
+
+
+def se2_custom(api, device="cpu", dtype=torch.float64):
+    """SE(2) pose graph (``SE2Var``) plus an unknown odometry scale held by a
+    user manifold (``PositiveVar``: a positive scalar updated as x * exp(delta),
+    no CUDA kind, so its retraction runs through torch on the device):
+    16 poses, 15 scaled odometry edges and 24 loop edges; pose 0 is data."""
+
+    class PositiveVar(api.Var, default_factory=lambda: torch.ones(1), tangent_dim=1,
+                      retract_fn=lambda x, d: x * torch.exp(d)):
+        """Positive scalar, multiplicative update."""
+
+    g = torch.Generator().manual_seed(23)
+    n, loops, scale = 16, 24, 1.3
+    th = torch.cumsum(0.3 * torch.randn(n, generator=g, dtype=torch.float64), 0)
+    xy = torch.cat((torch.zeros(1, 2, dtype=torch.float64),
+                    torch.cumsum(torch.stack((th.cos(), th.sin()), -1)[:-1], 0)))
+    truth = torch.cat((xy, th[:, None]), -1)
+
+    def rel(i, j):
+        return torch.stack([se2_between(truth[a], truth[b], torch.zeros(3, dtype=torch.float64)) for a, b in zip(i, j)])
+
+    oi, oj = torch.arange(n - 1), torch.arange(1, n)
+    odo = rel(oi, oj) + 0.01 * torch.randn(n - 1, 3, generator=g, dtype=torch.float64)
+    odo[:, :2] /= scale
+    li = torch.randint(1, n - 2, (loops,), generator=g)
+    lj = torch.minimum(li + torch.randint(2, 6, (loops,), generator=g), torch.tensor(n - 1))
+    loop = rel(li, lj) + 0.01 * torch.randn(loops, 3, generator=g, dtype=torch.float64)
+    init = [truth[0]]
+    for k in range(n - 1):  # integrate odometry at unit scale
+        c, s_ = torch.cos(init[-1][2]), torch.sin(init[-1][2])
+        z = odo[k]
+        init.append(torch.stack((init[-1][0] + c * z[0] - s_ * z[1], init[-1][1] + s_ * z[0] + c * z[1],
+                                 init[-1][2] + z[2])))
+    to = dict(device=device, dtype=dtype)
+    p = api.Problem({"poses": torch.stack(init[1:]).to(**to), "scale": torch.ones(1, 1, **to)},
+                    manifolds={"poses": api.SE2Var, "scale": PositiveVar})
+    zero = lambda m: torch.zeros(m, dtype=torch.long)  # noqa: E731
+    p.add_residual(se2_odometry, ("poses", oi[1:] - 1), ("poses", oj[1:] - 1), ("scale", zero(n - 2)),
+                   odo[1:].to(**to))
+    p.add_residual(se2_odometry, truth[0].to(**to), ("poses", torch.tensor([0])), ("scale", zero(1)),
+                   odo[:1].to(**to), in_dims=(None, 0, 0, 0))
+    p.add_residual(se2_between, ("poses", li - 1), ("poses", lj - 1), loop.to(**to))
+    return p
 
 
 def typed_ba(api, device="cpu", dtype=torch.float64):

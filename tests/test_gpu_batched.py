@@ -54,3 +54,25 @@ def test_batched_single_problem_and_inactive_blocks():
                       termination=tls.TerminationConfig(max_iterations=30))
     assert abs(float(summary.final_cost[0]) - s.final_cost) <= 1e-6 * s.final_cost
     assert torch.isfinite(sols[0]["cams"]).all()
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed"])
+def test_batched_matches_oracle(precision):
+    """Batched final costs against the numpy oracle (the reference's float64
+    LM with Schur-PCG, solved problem by problem on the host) on four problems
+    of the batched generator, in float64 and in mixed precision (float32 J and
+    W storage): 1e-6 relative, the tolerance of the batched-vs-individual test."""
+    import oracle
+    import torchls_b200 as tls
+    from golden import problems as P
+    from torchls_b200 import synthetic
+    from torchls_b200.batched import solve_batched
+
+    datas = synthetic.batched_bundle_adjustment(4, first_seed=200)
+    build = lambda d, api, **k: synthetic.build_bundle_adjustment(d, api, loss=api.HuberLoss(0.01), **k)  # noqa: E731
+    _, summary = solve_batched([build(d, tls, device=DEV) for d in datas], max_iterations=30, precision=precision)
+    for j, d in enumerate(datas):
+        _, ref = oracle.solve(P.oracle_problem(lambda api, d=d: build(d, api)), linear_solver="schur_cg",
+                              eliminate="points", termination=dict(max_iterations=30))
+        got = float(summary.final_cost[j])
+        assert abs(got - ref.final_cost) <= 1e-6 * ref.final_cost + 1e-14, (j, got, ref.final_cost)

@@ -139,6 +139,7 @@ OTHERS = {
                                    termination=dict(max_iterations=8))),
     "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
+    "se2_custom": (P.se2_custom, dict(linear_solver="conjugate_gradient")),
     "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
     "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
         lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),

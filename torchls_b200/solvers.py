@@ -30,7 +30,13 @@ from .kernels import reduce
 from .schur import DampedSchurSystem, SchurLinearization, SchurPlan
 from .sparse import BlockJacobian
 
-_BACKENDS = ("cuda",)
+# Backend names a ConjugateGradientConfig accepts: this package's "cuda" and
+# the reference's "torch" and "warp" (solvers.py:49-52), so that configs written
+# for torchls construct unchanged. All three run this package's CUDA kernels:
+# there is one implementation here, and it computes what the reference's
+# backends compute (same algorithm, same stopping rules, results within the
+# tolerances the parity tests state).
+_BACKENDS = ("cuda", "torch", "warp")
 
 
 def normalize_groups(groups):
@@ -81,9 +87,9 @@ class ConjugateGradientConfig:
                 or self.graph_batch_iterations < 1):
             raise ValueError("graph_batch_iterations must be a positive integer")
         if self.normal_matvec not in _BACKENDS:
-            raise ValueError("normal_matvec must be cuda (this package is the CUDA backend)")
+            raise ValueError("normal_matvec must be cuda, torch or warp (all run the CUDA kernels)")
         if self.backend not in _BACKENDS:
-            raise ValueError("CG backend must be cuda (this package is the CUDA backend)")
+            raise ValueError("CG backend must be cuda, torch or warp (all run the CUDA kernels)")
         if self.rtol < 0 or self.atol < 0 or self.max_iterations < 1:
             raise ValueError("Invalid CG tolerance or iteration limit")
         if self.preconditioner not in ("block_jacobi", None):
@@ -557,8 +563,8 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
         raise ValueError("dense_qr is not a block-sparse inner loop; use conjugate_gradient, schur_cg or schur_dense")
     if linear_solver not in ("conjugate_gradient", "schur_dense", "schur_cg"):
         raise ValueError("Unknown linear solver")
-    if normal_blocks_backend not in ("auto", "cuda"):
-        raise ValueError("normal_blocks_backend must be auto or cuda")
+    if normal_blocks_backend not in ("auto", *_BACKENDS):
+        raise ValueError("normal_blocks_backend must be auto, cuda, torch or warp")
     cg = conjugate_gradient
     is_schur = linear_solver.startswith("schur_")
     if eliminate is not None and not is_schur:
