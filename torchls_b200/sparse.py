@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
+from typing import NamedTuple
 
 import torch
 from torch import Tensor
@@ -213,28 +214,147 @@ class BlockJacobian:
         return dense
 
 
+class _ForeignPlan(NamedTuple):
+    """What the device structure reads of one residual batch."""
+
+    type_indices: tuple
+    indices: tuple  # CPU int64 variable index per slot
+    count: int
+
+
+class _ForeignProblem(NamedTuple):
+    layout: tuple
+    plans: tuple
+
+
+def _is_own(jacobian) -> bool:
+    return isinstance(jacobian, BlockJacobian)
+
+
+def _signature(jacobian):
+    """Incidence structure of a reference-layout Jacobian: per batch the block
+    shapes, type indices and variable indices (compared by value on bind)."""
+    return tuple((tuple(tuple(b.shape) for b in g.blocks), tuple(g.type_indices),
+                  tuple(i for i in g.variable_indices)) for g in jacobian.groups)
+
+
+class _ForeignLayout:
+    """Device structure for a Jacobian in the reference's layout
+    (torchls sparse.py:11-27: per batch, per slot, blocks [N, r, d], global
+    columns [N, d], type indices and variable indices; a layout of
+    (offset, count, dim) groups). Built once per structure; ``pack`` brings one
+    linearization into this package's storage (structure-of-arrays J plus the
+    per-factor Gram contributions of the diagonal blocks) with one launch of
+    the packed linearization kernel per batch."""
+
+    def __init__(self, jacobian):
+        from .problem import Structure
+
+        groups = tuple(jacobian.groups)
+        if not groups:
+            raise ValueError("the Jacobian has no residual batches")
+        proto = groups[0].blocks[0]
+        if proto.device.type != "cuda" or proto.dtype not in (torch.float32, torch.float64):
+            raise ValueError("CUDA products require CUDA float32 or float64 Jacobian blocks")
+        if jacobian.shape[1] > 2**31 - 1:
+            raise ValueError("CUDA products require 32-bit column indices")
+        self.layout = tuple(jacobian.layout)
+        self.shape = tuple(jacobian.shape)
+        self.dtype, self.device = proto.dtype, proto.device
+        plans, rdims = [], []
+        for g in groups:
+            n, r = g.blocks[0].shape[:2]
+            if r > 8 or sum(b.shape[2] for b in g.blocks) > 16:
+                raise ValueError("CUDA products support residual dims <= 8 and slot dims summing to <= 16")
+            for b, c, t, idx in zip(g.blocks, g.columns, g.type_indices, g.variable_indices):
+                e = self.layout[t]
+                if b.shape != (n, r, e.dim) or b.dtype != self.dtype or b.device != self.device:
+                    raise ValueError("Jacobian blocks must share shape [N, r, d_slot], dtype and device")
+                want = idx.to(c.device).long()[:, None] * e.dim + e.offset + torch.arange(e.dim, device=c.device)
+                if c.shape != (n, e.dim) or not torch.equal(c.long(), want):
+                    raise ValueError("Jacobian columns must be variable index * dim + group offset + slot column")
+            plans.append(_ForeignPlan(tuple(g.type_indices), tuple(i.detach().cpu().long() for i in g.variable_indices),
+                                      int(n)))
+            rdims.append(int(r))
+        self.signature = _signature(jacobian)
+        self.structure = Structure(_ForeignProblem(self.layout, tuple(plans)), self.device, rdims)
+
+    def check(self, jacobian, what):
+        sig = _signature(jacobian)
+        same = len(sig) == len(self.signature) and all(
+            a[0] == b[0] and a[1] == b[1] and all(x is y or torch.equal(x, y) for x, y in zip(a[2], b[2]))
+            for a, b in zip(sig, self.signature))
+        if not same or tuple(jacobian.shape) != self.shape:
+            raise ValueError(f"CUDA {what} plan requires unchanged incidence structure")
+        proto = jacobian.groups[0].blocks[0]
+        if proto.dtype != self.dtype or proto.device != self.device:
+            raise ValueError(f"CUDA {what} plan requires unchanged block shapes, dtype and device")
+
+    def pack(self, jacobian) -> BlockJacobian:
+        st = self.structure
+        gram = torch.empty(st.gram_size, dtype=torch.float64, device=self.device)
+        jacs, keep = [], []
+        stream = L.stream_handle(self.device)
+        for k, g in enumerate(jacobian.groups):
+            n, r = st.plans[k].count, st.rdims[k]
+            jac = torch.empty(r * st.D[k] * n, dtype=self.dtype, device=self.device)
+            blocks = [b.detach().to(torch.float64).contiguous() for b in g.blocks]
+            zero = torch.zeros(n * r, dtype=torch.float64, device=self.device)
+            keep += [blocks, zero]
+            la = L.LinearizeArgs()
+            la.fg = st.factor_group(k, jac, jac_stride=n)
+            la.residual_kind, la.loss_kind, la.has_loss, la.want_jacobian = L.RES_PACKED, L.LOSS_NONE, 0, 1
+            la.packed_residual = zero.data_ptr()
+            for si, b in enumerate(blocks):
+                la.packed_blocks[si] = b.data_ptr()
+            la.gram_contrib = gram.data_ptr() + 8 * st.gram_base[k]
+            L.call("tls_linearize", C.byref(la), stream)
+            jacs.append(jac)
+        return BlockJacobian(st, tuple(jacs), gram, self.layout, self.shape)
+
+
 class CudaNormalPlan:
     """Fixed incidence structure for repeated normal products.
 
-    Mirrors torchls ``WarpNormalPlan(J, max_packed_bytes=...)`` /
-    ``.bind(J)`` / ``.normal_matvec(v, damping)`` (warp_normal.py:125-294).
-    ``max_packed_bytes`` is accepted for interface parity; the Jacobian is
-    always stored structure-of-arrays, so no extra packed copy exists.
+    The interface of torchls ``WarpNormalPlan(J, max_packed_bytes=...)``,
+    ``.bind(J)`` and ``.normal_matvec(v, damping)`` (warp_normal.py:125-294).
+    ``J`` is either this package's ``BlockJacobian`` (already stored
+    structure-of-arrays: ``bind`` checks it and returns it) or any Jacobian in
+    the reference's layout (``groups`` of per-slot blocks [N, r, d] with global
+    columns, ``layout``, ``shape``), such as the reference's own
+    ``BlockJacobian``: the plan builds the device structure (index maps, the
+    one-pass tile plan) once, and each ``bind`` packs that linearization's
+    blocks into structure-of-arrays storage on the device. ``max_packed_bytes``
+    is validated for interface parity; the packed copy is the only storage the
+    kernels read.
     """
 
-    def __init__(self, jacobian: BlockJacobian, *, max_packed_bytes: int = 256 * 1024**2):
-        if not isinstance(jacobian, BlockJacobian) or jacobian.device.type != "cuda":
-            raise ValueError("CUDA normal matvec requires a CUDA BlockJacobian")
+    def __init__(self, jacobian, *, max_packed_bytes: int = 256 * 1024**2):
         if isinstance(max_packed_bytes, bool) or not isinstance(max_packed_bytes, int) or max_packed_bytes < 0:
             raise ValueError("max_packed_bytes must be a nonnegative integer")
-        if jacobian.shape[1] > 2**31 - 1:
-            raise ValueError("CUDA normal matvec requires 32-bit column indices")
-        self.structure = jacobian.structure
+        if _is_own(jacobian):
+            if jacobian.device.type != "cuda":
+                raise ValueError("CUDA normal matvec requires a CUDA BlockJacobian")
+            if jacobian.shape[1] > 2**31 - 1:
+                raise ValueError("CUDA normal matvec requires 32-bit column indices")
+            self._foreign = None
+            self.structure = jacobian.structure
+            self.dtype, self.device = jacobian.dtype, jacobian.device
+        else:
+            self._foreign = _ForeignLayout(jacobian)
+            self.structure = self._foreign.structure
+            self.dtype, self.device = self._foreign.dtype, self._foreign.device
         self.size = jacobian.shape[1]
-        self.dtype, self.device = jacobian.dtype, jacobian.device
 
-    def bind(self, jacobian: BlockJacobian) -> BlockJacobian:
-        if jacobian.structure is not self.structure or jacobian.shape[1] != self.size:
+    def bind(self, jacobian) -> BlockJacobian:
+        """The linearization to multiply with; raises ValueError when its
+        structure, block shapes, dtype or device differ from the plan's."""
+        if self._foreign is not None:
+            if _is_own(jacobian):
+                raise ValueError("CUDA normal plan requires unchanged incidence structure")
+            self._foreign.check(jacobian, "normal")
+            return self._foreign.pack(jacobian)
+        if not _is_own(jacobian) or jacobian.structure is not self.structure or jacobian.shape[1] != self.size:
             raise ValueError("CUDA normal plan requires unchanged incidence structure")
         if jacobian.dtype != self.dtype or jacobian.device != self.device:
             raise ValueError("CUDA normal plan requires unchanged block shapes, dtype and device")
@@ -242,14 +362,28 @@ class CudaNormalPlan:
 
 
 class CudaDiagonalPlan:
-    """Mirrors torchls ``WarpDiagonalPlan(J).diagonal_blocks(J)`` (warp_diagonal.py:69-179)."""
+    """The interface of torchls ``WarpDiagonalPlan(J).diagonal_blocks(J)``
+    (warp_diagonal.py:69-179): exact per-variable J^T J blocks, aliased slots
+    included, one [count, d, d] tensor per layout entry, float64, deterministic.
+    Accepts this package's ``BlockJacobian`` or the reference's layout (see
+    ``CudaNormalPlan``)."""
 
-    def __init__(self, jacobian: BlockJacobian):
-        if not isinstance(jacobian, BlockJacobian) or jacobian.device.type != "cuda":
-            raise ValueError("CUDA diagonal blocks require a CUDA BlockJacobian")
-        self.structure = jacobian.structure
+    def __init__(self, jacobian):
+        if _is_own(jacobian):
+            if jacobian.device.type != "cuda":
+                raise ValueError("CUDA diagonal blocks require a CUDA BlockJacobian")
+            self._foreign = None
+            self.structure = jacobian.structure
+        else:
+            self._foreign = _ForeignLayout(jacobian)
+            self.structure = self._foreign.structure
 
-    def diagonal_blocks(self, jacobian: BlockJacobian):
-        if jacobian.structure is not self.structure:
+    def diagonal_blocks(self, jacobian):
+        if self._foreign is not None:
+            if _is_own(jacobian):
+                raise ValueError("CUDA diagonal plan requires unchanged incidence structure, shapes and dtype")
+            self._foreign.check(jacobian, "diagonal")
+            return self._foreign.pack(jacobian).diagonal_blocks()
+        if not _is_own(jacobian) or jacobian.structure is not self.structure:
             raise ValueError("CUDA diagonal plan requires unchanged incidence structure, shapes and dtype")
         return jacobian.diagonal_blocks()
