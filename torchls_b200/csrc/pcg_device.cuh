@@ -180,95 +180,120 @@ __device__ __forceinline__ void pcg_decide(PcgState* st, double s0, double s1, d
   c.mode = M_DONE;
 }
 
-// One PCG step's vector work on blocks [b0, nblocks) with stride `step`:
+// One block's PCG vector work (block b of the set; `l` holds its packed
+// factor when `have_l`, else it is loaded here):
 // ITER: x += alpha p, r -= alpha Ap, z = M r; sums r.r, r.z.
 // CHECK/FINAL: ap holds A x; true residual tr = rhs - A x (into ap), ztrue = M tr;
 // sums tr.tr, (tr - r).(tr - r), tr.ztrue.
+template <int D, typename TV, bool COH = false>
+__device__ __forceinline__ void pcg_update_block(const BlockSet& bs, int64_t b, int mode, double alpha,
+                                                 const TV* __restrict__ rhs, TV* x, TV* r, TV* z, const TV* p,
+                                                 TV* ap, TV* ztrue, double (&l)[D * (D + 1) / 2], bool have_l,
+                                                 double& a0, double& a1, double& a2) {
+  const int gi = find_group(bs, b);
+  const int64_t i = b - bs.block_begin[gi];
+  const tls_block_group& g = bs.g[gi];
+  const int dim = g.dim;
+  int64_t cols[D];
+  block_cols<D>(g, i, cols);
+  // every load of the block before its first store (the stores may alias
+  // the loads' arrays, so the compiler would otherwise order them one by one)
+  const bool solve = mode != M_FINAL && !(bs.identity || g.factor == nullptr);
+  if (solve && !have_l) load_tri<D>(g.factor + i * dim * dim, dim, l);
+  double v0[D], v1[D], v2[D], v3[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    v0[k] = v1[k] = v2[k] = v3[k] = 0.0;
+    if (k < dim) {
+      const int64_t col = cols[k];
+      if (mode == M_ITER) {
+        v0[k] = to_d(ldv<COH>(x + col));
+        v1[k] = to_d(ldv<COH>(p + col));
+      } else {
+        v0[k] = to_d(rhs[col]);
+      }
+      v2[k] = to_d(ldv<COH>(r + col));
+      v3[k] = to_d(ldv<COH>(ap + col));
+    }
+  }
+  double rb[D], zb[D];
+  if (mode == M_ITER) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      rb[k] = 0.0;
+      if (k < dim) {
+        const int64_t col = cols[k];
+        x[col] = static_cast<TV>(v0[k] + alpha * v1[k]);
+        const TV rn = static_cast<TV>(v2[k] - alpha * v3[k]);
+        r[col] = rn;
+        rb[k] = to_d(rn);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      rb[k] = 0.0;
+      if (k < dim) {
+        const int64_t col = cols[k];
+        const TV tr = static_cast<TV>(v0[k] - v3[k]);
+        ap[col] = tr;
+        const double t = to_d(tr);
+        rb[k] = t;
+        a0 += t * t;
+        const double dr = t - v2[k];
+        a1 += dr * dr;
+      }
+    }
+  }
+  if (mode == M_FINAL) return;
+  if (!solve) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) zb[k] = rb[k];
+  } else {
+    solve_tri<D>(l, dim, rb, zb);
+  }
+  TV* zdst = (mode == M_ITER) ? z : ztrue;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    if (k < dim) {
+      const TV zk = static_cast<TV>(zb[k]);
+      zdst[cols[k]] = zk;
+      const double zd = to_d(zk);
+      if (mode == M_ITER) {
+        a0 += rb[k] * rb[k];
+        a1 += rb[k] * zd;
+      } else {
+        a2 += rb[k] * zd;
+      }
+    }
+  }
+}
+
+// The PCG vector work of blocks [b0, nblocks) with stride `step` (see
+// pcg_update_block).
 template <int D, typename TV, bool COH = false>
 __device__ __forceinline__ void pcg_update_blocks(const BlockSet& bs, int64_t nblocks, int64_t b0, int64_t step,
                                                   int mode, double alpha, const TV* __restrict__ rhs, TV* x, TV* r,
                                                   TV* z, const TV* p, TV* ap, TV* ztrue, double& a0, double& a1,
                                                   double& a2) {
   for (int64_t b = b0; b < nblocks; b += step) {
-    const int gi = find_group(bs, b);
-    const int64_t i = b - bs.block_begin[gi];
-    const tls_block_group& g = bs.g[gi];
-    const int dim = g.dim;
-    int64_t cols[D];
-    block_cols<D>(g, i, cols);
-    // every load of the block before its first store (the stores may alias
-    // the loads' arrays, so the compiler would otherwise order them one by one)
-    const bool solve = mode != M_FINAL && !(bs.identity || g.factor == nullptr);
     double l[D * (D + 1) / 2];
-    if (solve) load_tri<D>(g.factor + i * dim * dim, dim, l);
-    double v0[D], v1[D], v2[D], v3[D];
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      v0[k] = v1[k] = v2[k] = v3[k] = 0.0;
-      if (k < dim) {
-        const int64_t col = cols[k];
-        if (mode == M_ITER) {
-          v0[k] = to_d(ldv<COH>(x + col));
-          v1[k] = to_d(ldv<COH>(p + col));
-        } else {
-          v0[k] = to_d(rhs[col]);
-        }
-        v2[k] = to_d(ldv<COH>(r + col));
-        v3[k] = to_d(ldv<COH>(ap + col));
-      }
-    }
-    double rb[D], zb[D];
-    if (mode == M_ITER) {
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        rb[k] = 0.0;
-        if (k < dim) {
-          const int64_t col = cols[k];
-          x[col] = static_cast<TV>(v0[k] + alpha * v1[k]);
-          const TV rn = static_cast<TV>(v2[k] - alpha * v3[k]);
-          r[col] = rn;
-          rb[k] = to_d(rn);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        rb[k] = 0.0;
-        if (k < dim) {
-          const int64_t col = cols[k];
-          const TV tr = static_cast<TV>(v0[k] - v3[k]);
-          ap[col] = tr;
-          const double t = to_d(tr);
-          rb[k] = t;
-          a0 += t * t;
-          const double dr = t - v2[k];
-          a1 += dr * dr;
-        }
-      }
-    }
-    if (mode == M_FINAL) continue;
-    if (!solve) {
-#pragma unroll
-      for (int k = 0; k < D; ++k) zb[k] = rb[k];
-    } else {
-      solve_tri<D>(l, dim, rb, zb);
-    }
-    TV* zdst = (mode == M_ITER) ? z : ztrue;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      if (k < dim) {
-        const TV zk = static_cast<TV>(zb[k]);
-        zdst[cols[k]] = zk;
-        const double zd = to_d(zk);
-        if (mode == M_ITER) {
-          a0 += rb[k] * rb[k];
-          a1 += rb[k] * zd;
-        } else {
-          a2 += rb[k] * zd;
-        }
-      }
-    }
+    pcg_update_block<D, TV, COH>(bs, b, mode, alpha, rhs, x, r, z, p, ap, ztrue, l, false, a0, a1, a2);
   }
+}
+
+// Load block b's packed factor into `l` ahead of its update (false when the
+// step's mode solves no block or the set has no factors).
+template <int D>
+__device__ __forceinline__ bool pcg_prefetch_factor(const BlockSet& bs, int64_t b, int mode,
+                                                    double (&l)[D * (D + 1) / 2]) {
+  if (mode == M_FINAL || bs.identity) return false;
+  const int gi = find_group(bs, b);
+  const tls_block_group& g = bs.g[gi];
+  if (g.factor == nullptr) return false;
+  const int64_t i = b - bs.block_begin[gi];
+  load_tri<D>(g.factor + i * g.dim * g.dim, g.dim, l);
+  return true;
 }
 
 // Direction / restart / swap for elements [i0, n) with stride `step`.

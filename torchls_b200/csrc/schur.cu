@@ -195,7 +195,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
 #pragma unroll
           for (int k = 0; k < DR; ++k) {
             if constexpr (XS) xr[k] = x_s[i * DR + k];
-            else if constexpr (COH) xr[k] = static_cast<TA>(x[(int64_t)i * DR + k]);  // written by this kernel: no .nc path
+            else if constexpr (COH) xr[k] = static_cast<TA>(__ldcg(x + (int64_t)i * DR + k));  // rewritten by this kernel: L2
             else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
           }
           TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
@@ -370,7 +370,8 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
 // finish its rows, with 256 threads:
 // MODE 0: out = s U s x + lambda x - sum; returns x_i . out_i to thread 0
 // MODE 1: out = b_retained - sum
-// COH: x is rewritten by this kernel (persistent loop): plain loads, not .nc.
+// COH: x and the run partials are rewritten by this kernel (persistent loop):
+// L2 loads (__ldcg), so no CTA reads a stale L1 line from an earlier step.
 template <int DR, int MODE, typename TV, typename TP, bool COH>
 __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* __restrict__ x,
                                              const double* __restrict__ b, TV* __restrict__ out, int64_t i,
@@ -381,7 +382,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
     if (tid < DR * DR) {
       const int l = tid % DR;
       const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
-      const double xl = to_d(x[i * DR + l]);
+      const double xl = to_d(COH ? __ldcg(x + i * DR + l) : x[i * DR + l]);
       ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * xl);
     }
   }
@@ -396,7 +397,10 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
     for (int q = 0; q < 4; ++q) {
       const int j = j0 + q * 256;
 #pragma unroll
-      for (int k = 0; k < DR; ++k) v[q][k] = j < re ? part[(int64_t)j * DR + k] : TP(0);
+      for (int k = 0; k < DR; ++k) {
+        const TP* src = part + (int64_t)j * DR + k;
+        v[q][k] = j < re ? (COH ? __ldcg(src) : *src) : TP(0);
+      }
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -417,7 +421,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
 #pragma unroll
       for (int q = 0; q < 8; ++q) tot += sm[q][k];
       if constexpr (MODE == 0) {
-        const double xv = to_d(x[i * DR + k]);
+        const double xv = to_d(COH ? __ldcg(x + i * DR + k) : x[i * DR + k]);
         const double sk = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
         double v = 0.0;
 #pragma unroll
@@ -777,6 +781,11 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     double* p = z + n;
     double* psave = p + n;
     double* ap = psave + n;
+    // The control block lives in this CTA's shared memory during the solve;
+    // status and mode are published to global memory every step (the chunk
+    // CTAs read them), the rest when the loop ends.
+    __shared__ PcgState sst;
+    if (tid == 0) sst = *st;
     for (int64_t i = tid; i < n; i += kChunkThreads) {
       x[i] = q.x[i];
       r[i] = q.r[i];
@@ -785,10 +794,18 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       psave[i] = q.psave[i];
     }
     __syncthreads();
+    // one preconditioner block per thread when they fit: its factor is loaded
+    // while the chunk CTAs still stream, ahead of the update
+    const bool one_block = q.nb <= kChunkThreads;
+    constexpr int LD = D * (D + 1) / 2;
     for (int step = 0; step < q.steps; ++step) {
-      if (tid == 0) s_go = st->pub.status == TLS_PCG_ACTIVE && st->pub.mode != M_DONE;
+      if (tid == 0) s_go = sst.pub.status == TLS_PCG_ACTIVE && sst.pub.mode != M_DONE;
       __syncthreads();
       if (!s_go) break;
+      const int mode = sst.pub.mode;
+      double lpre[LD];
+      bool have = false;
+      if (one_block && tid < q.nb) have = pcg_prefetch_factor<D>(q.bs, tid, mode, lpre);
       // wait until every chunk CTA has gathered its variables
       if (tid == 0) {
         s_ok = 1;
@@ -806,40 +823,52 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       }
       __syncthreads();
       if (!s_ok) break;
-      for (int64_t i = tid; i < n; i += kChunkThreads) ap[i] = __ldcg(q.ap + i);
-      tls_pcg_control& c = st->pub;
-      const int mode = c.mode;
-      if (c.status == TLS_PCG_ACTIVE && mode == M_ITER) {
-        const double curv = block_sum_cg<kChunkThreads>(q.dots, a.nretained, smd);
-        if (tid == 0) {
-          const double rz = c.rz;
-          c.curvature = curv;
-          const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
-          st->alpha_ok = ok;
-          c.alpha = ok ? rz / curv : 0.0;
-        }
+      // Ap into shared memory, and the curvature p.Ap in the same pass
+      double part = 0.0;
+      for (int64_t i = tid; i < n; i += kChunkThreads) {
+        const double v = __ldcg(q.ap + i);
+        ap[i] = v;
+        part += p[i] * v;
+      }
+      const double curv = block_sum<kChunkThreads>(part, smd);
+      tls_pcg_control& c = sst.pub;
+      if (tid == 0 && c.status == TLS_PCG_ACTIVE && mode == M_ITER) {
+        const double rz = c.rz;
+        c.curvature = curv;
+        const bool ok = isfinite(curv) && isfinite(rz) && curv > 0.0 && rz > 0.0;
+        sst.alpha_ok = ok;
+        c.alpha = ok ? rz / curv : 0.0;
       }
       __syncthreads();
       double a0 = 0.0, a1 = 0.0, a2 = 0.0;
       bool work = c.status == TLS_PCG_ACTIVE && mode != M_DONE;
       double alpha = 0.0;
       if (work && mode == M_ITER) {
-        if (!st->alpha_ok) work = false;
+        if (!sst.alpha_ok) work = false;
         else alpha = c.alpha;
       }
-      if (work)
-        pcg_update_blocks<D, double, false>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, x, r, z, p, ap,
-                                            q.ztrue, a0, a1, a2);
+      if (work) {
+        if (one_block) {
+          if (tid < q.nb)
+            pcg_update_block<D, double, false>(q.bs, tid, mode, alpha, q.rhs, x, r, z, p, ap, q.ztrue, lpre, have,
+                                               a0, a1, a2);
+        } else {
+          pcg_update_blocks<D, double, false>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, x, r, z, p, ap,
+                                              q.ztrue, a0, a1, a2);
+        }
+      }
       __shared__ double smd3[3][kChunkThreads / 32];
       block_sum3<kChunkThreads>(a0, a1, a2, smd3);
       const double t0 = a0, t1 = a1, t2 = a2;
       __shared__ int s_action, s_tofinal;
       __shared__ double s_beta;
       if (tid == 0) {
-        pcg_decide(st, t0, t1, t2);
-        s_action = st->action;
-        s_beta = st->pub.beta;
-        s_tofinal = st->pub.mode == M_FINAL && st->action != A_SWAP_TO_X;
+        pcg_decide(&sst, t0, t1, t2);
+        s_action = sst.action;
+        s_beta = sst.pub.beta;
+        s_tofinal = sst.pub.mode == M_FINAL && sst.action != A_SWAP_TO_X;
+        st->pub.status = sst.pub.status;  // read by the chunk CTAs at their next step
+        st->pub.mode = sst.pub.mode;
       }
       __syncthreads();
       if (s_action != A_NONE)
@@ -855,6 +884,15 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       }
     }
     __syncthreads();
+    if (tid == 0) {  // the control block back to global memory (not the barrier words)
+      st->pub = sst.pub;
+      st->action = sst.action;
+      st->pending = sst.pending;
+      st->rec = sst.rec;
+      st->rec_hit = sst.rec_hit;
+      st->periodic_hit = sst.periodic_hit;
+      st->alpha_ok = sst.alpha_ok;
+    }
     for (int64_t i = tid; i < n; i += kChunkThreads) {
       q.x[i] = x[i];
       q.r[i] = r[i];
@@ -937,11 +975,8 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     }
     __syncthreads();
     if (!s_ok) break;
-    // ---- B
-    for (int64_t i = blockIdx.x; i < a.nretained; i += G) {
-      const double dot = gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
-      if (tid == 0) q.dots[i] = dot;
-    }
+    // ---- B (the vector CTA forms p.Ap itself)
+    for (int64_t i = blockIdx.x; i < a.nretained; i += G) gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
     // ---- arrive at the vector CTA, wait for its release
     __syncthreads();
     if (tid == 0) {
