@@ -195,7 +195,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
 #pragma unroll
           for (int k = 0; k < DR; ++k) {
             if constexpr (XS) xr[k] = x_s[i * DR + k];
-            else if constexpr (COH) xr[k] = static_cast<TA>(__ldcg(x + (int64_t)i * DR + k));  // rewritten by this kernel: L2
+            else if constexpr (COH) xr[k] = static_cast<TA>(x[(int64_t)i * DR + k]);  // see gather_one: COH  // rewritten by this kernel: L2
             else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
           }
           TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
@@ -371,7 +371,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
 // MODE 0: out = s U s x + lambda x - sum; returns x_i . out_i to thread 0
 // MODE 1: out = b_retained - sum
 // COH: x and the run partials are rewritten by this kernel (persistent loop):
-// L2 loads (__ldcg), so no CTA reads a stale L1 line from an earlier step.
+// plain loads, not the read-only (.nc) path. They observe this step's values:
+// the writers release them through a GPU-scope fence and an atomic before the
+// grid barrier, and this CTA acquires them (a fence after the barrier wait,
+// then a block barrier) before it reads.
 template <int DR, int MODE, typename TV, typename TP, bool COH>
 __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* __restrict__ x,
                                              const double* __restrict__ b, TV* __restrict__ out, int64_t i,
@@ -382,7 +385,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
     if (tid < DR * DR) {
       const int l = tid % DR;
       const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
-      const double xl = to_d(COH ? __ldcg(x + i * DR + l) : x[i * DR + l]);
+      const double xl = to_d(x[i * DR + l]);
       ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * xl);
     }
   }
@@ -399,7 +402,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
         const TP* src = part + (int64_t)j * DR + k;
-        v[q][k] = j < re ? (COH ? __ldcg(src) : *src) : TP(0);
+        v[q][k] = j < re ? *src : TP(0);
       }
     }
 #pragma unroll
@@ -421,7 +424,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
 #pragma unroll
       for (int q = 0; q < 8; ++q) tot += sm[q][k];
       if constexpr (MODE == 0) {
-        const double xv = to_d(COH ? __ldcg(x + i * DR + k) : x[i * DR + k]);
+        const double xv = to_d(x[i * DR + k]);
         const double sk = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
         double v = 0.0;
 #pragma unroll
