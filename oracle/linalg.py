@@ -10,7 +10,17 @@ import math
 from dataclasses import dataclass
 
 import numpy as np
+import torch
 from scipy.linalg import solve_triangular
+
+
+def add_rows(out, rows, vals):
+    """out[rows[k]] += vals[k], repeated rows summed in input order (what
+    np.add.at does), through torch's CPU index_add_ on views of the arrays."""
+    k = int(np.prod(out.shape[1:], dtype=np.int64))
+    target = torch.from_numpy(out.reshape(out.shape[0], k))  # a view: updates `out` in place
+    src = torch.from_numpy(np.ascontiguousarray(vals, dtype=np.float64).reshape(-1, k))
+    target.index_add_(0, torch.from_numpy(np.asarray(rows, dtype=np.int64).reshape(-1)), src)
 
 
 class LinAlgError(Exception):
@@ -39,7 +49,7 @@ class BlockJacobian:
             n, r, _ = g["blocks"][0].shape
             local = u[off : off + n * r].reshape(n, r)
             for b, c in zip(g["blocks"], g["columns"]):
-                np.add.at(out, c.reshape(-1), np.einsum("nrd,nr->nd", b, local).reshape(-1))
+                add_rows(out, c.reshape(-1), np.einsum("nrd,nr->nd", b, local).reshape(-1))
             off += n * r
         return out
 
@@ -69,7 +79,7 @@ class BlockJacobian:
                         cross = np.einsum("nri,nrj->nij", b, g["blocks"][o])
                         mask = (rows == g["rows"][o])[:, None, None]
                         gram = gram + (cross + np.swapaxes(cross, -1, -2)) * mask
-                np.add.at(diag[t], rows, gram)
+                add_rows(diag[t], rows, gram)
         return diag
 
     def to_dense(self):

@@ -4,8 +4,9 @@ from __future__ import annotations
 
 import numpy as np
 import scipy.sparse as sp
+import torch
 
-from .linalg import BlockJacobian, JointBlocks, block_apply, cholesky
+from .linalg import BlockJacobian, JointBlocks, add_rows, block_apply, cholesky
 
 
 class RetainedEntry:
@@ -89,6 +90,13 @@ class SchurPlan:
         self.row_ptr = np.concatenate(([0], np.cumsum(cnt))).astype(np.int64)
         self.columns = np.concatenate(csr_cols).astype(np.int64)
         self.value_order = np.concatenate(orders)
+        # W^T's CSR pattern and the permutation from W's values to W^T's, built
+        # once (a damped system then only permutes its values)
+        ncols = self.e.count * self.e.dim
+        probe = sp.csr_matrix((np.arange(len(self.columns), dtype=np.float64), self.columns, self.row_ptr),
+                              shape=(self.dim, ncols)).T.tocsr()
+        self.t_ptr, self.t_cols = probe.indptr.astype(np.int64), probe.indices.astype(np.int64)
+        self.t_perm = probe.data.astype(np.int64)
         self.joint = JointBlocks(self.layout, preconditioner_groups) if preconditioner_groups else None
         self.pre_edges = []
         if self.joint is not None:
@@ -123,7 +131,7 @@ class SchurLinearization:
             for gi, s, es, eids in recs:
                 blocks = jac.groups[gi]["blocks"]
                 eb = sum(blocks[k] for k in es)
-                np.add.at(vals, eids, np.einsum("nri,nrj->nij", blocks[s], eb))
+                add_rows(vals, eids, np.einsum("nri,nrj->nij", blocks[s], eb))
             self.cross.append(vals)
         self.base = None
         if dense:
@@ -141,6 +149,23 @@ class SchurLinearization:
         return DampedSchurSystem(self, damping)
 
 
+class _Csr:
+    """CSR matrix times a numpy vector through torch's (multithreaded) CPU SpMV;
+    the products are those of ``scipy.sparse`` up to summation order."""
+
+    def __init__(self, ptr, cols, values, shape):
+        self.shape = shape
+        self.t = torch.sparse_csr_tensor(torch.from_numpy(ptr), torch.from_numpy(cols), torch.from_numpy(values),
+                                         size=shape, check_invariants=False)
+        self.ptr, self.cols, self.values = ptr, cols, values
+
+    def __matmul__(self, v):
+        return (self.t @ torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))).numpy()
+
+    def scipy(self):
+        return sp.csr_matrix((self.values, self.cols, self.ptr), shape=self.shape)
+
+
 class DampedSchurSystem:
     """schur.py:263-397."""
 
@@ -153,8 +178,9 @@ class DampedSchurSystem:
         self.whitened = [blk @ np.swapaxes(self.inverse_l[ei], -1, -2) for blk, (_, ei) in zip(lin.cross, self.plan.edges)]
         values = np.concatenate([w.reshape(-1) for w in self.whitened])[self.plan.value_order]
         e = self.plan.e
-        self.w = sp.csr_matrix((values, self.plan.columns, self.plan.row_ptr), shape=(self.plan.dim, e.count * e.dim))
-        self.wt = self.w.T.tocsr()
+        shape = (self.plan.dim, e.count * e.dim)
+        self.w = _Csr(self.plan.row_ptr, self.plan.columns, values, shape)
+        self.wt = _Csr(self.plan.t_ptr, self.plan.t_cols, values[self.plan.t_perm], shape[::-1])
 
     def reduced_rhs(self, rhs):
         e = self.plan.e
@@ -201,13 +227,13 @@ class DampedSchurSystem:
                         wh[m, start : start + d] = self.whitened[i]
                         start += d
                 out = base.copy()
-                np.add.at(out, rows, -(wh @ np.swapaxes(wh, -1, -2)))
+                add_rows(out, rows, -(wh @ np.swapaxes(wh, -1, -2)))
                 diags.append(out)
             return self.plan.joint.factor(diags, self.damping)
         factors = []
         for i, ent, wh, (ri, _) in zip(self.plan.retained, self.plan.layout, self.whitened, self.plan.edges):
             d = self.lin.diag[i].copy()
-            np.add.at(d, ri, -(wh @ np.swapaxes(wh, -1, -2)))
+            add_rows(d, ri, -(wh @ np.swapaxes(wh, -1, -2)))
             factors.append(cholesky(d + self.damping * np.eye(ent.dim)))
 
         def apply(v):
@@ -222,5 +248,5 @@ class DampedSchurSystem:
         if self.lin.base is None:
             raise ValueError("Dense Schur matrix was not requested")
         m = self.lin.base + self.damping * np.eye(self.plan.dim)
-        m = m - (self.w @ self.wt).toarray()
+        m = m - (self.w.scipy() @ self.wt.scipy()).toarray()
         return 0.5 * (m + m.T)
