@@ -309,11 +309,12 @@ typedef struct tls_pcg_control {
 } tls_pcg_control;
 
 typedef struct tls_schur_args tls_schur_args;
+typedef struct tls_schur_general_args tls_schur_general_args;
 
 typedef struct tls_pcg_args {
   int64_t n;
   int32_t vec_dtype;
-  int32_t op_kind;               /* 0: normal operator, 1: Schur reduced operator */
+  int32_t op_kind;               /* 0: normal operator, 1: Schur reduced operator, 2: general Schur */
   const tls_normal_args* normal; /* op_kind 0 */
   const tls_schur_args* schur;   /* op_kind 1 */
   const tls_block_group* pre;    /* preconditioner blocks, or NULL (identity) */
@@ -323,6 +324,7 @@ typedef struct tls_pcg_args {
   void *x, *r, *z, *p, *ap, *ztrue, *psave;   /* [n] workspaces of vec_dtype */
   double* partials;              /* >= 65536 + 3 * 1024 doubles */
   tls_pcg_control* control;      /* device buffer of tls_pcg_state_bytes() bytes */
+  const tls_schur_general_args* schur_general; /* op_kind 2 */
 } tls_pcg_args;
 
 /* Initialise: x = 0, r = rhs, norms, threshold = max(atol, rtol |rhs|),
@@ -391,6 +393,74 @@ struct tls_schur_args {
                                    it covers one damped system: its rhs, PCG and back-substitution */
   int64_t wait_cycles;          /* limit of every bounded wait in SM cycles; <= 0: 2^31 (about a second) */
 };
+
+/* ---------------------------------------------------------------- general Schur complement
+ * Replaces: schur.py:17-397 where the one-group path above does not apply:
+ * several retained groups (e.g. cameras and intrinsics), residuals that couple
+ * retained variables (camera priors, odometry between cameras; schur.py:41-56,
+ * 303-328) and joint preconditioner groups (schur.py:163-189, 330-352).
+ * Retained variables are numbered in reduced order (groups in layout order,
+ * IDs ascending); each one's edges are contiguous, in the reference's edge
+ * order (sorted key r * E + e, schur.py:80, 93). Every sum runs in a fixed
+ * order: results are deterministic. Reduced vectors are float64.
+ */
+struct tls_schur_general_args {
+  int32_t de;                   /* eliminated block dim (<= 4) */
+  int32_t nelim;                /* eliminated variables */
+  int32_t nretained;            /* retained variables over all groups */
+  int32_t wdtype;               /* TLS_F32 / TLS_F64 storage of the whitened blocks */
+  int64_t nedges;
+  int64_t reduced_dim;
+  int64_t full_dim;             /* length of the full tangent vector */
+  int64_t elim_offset;          /* tangent offset of the eliminated group (full vector) */
+  const int32_t* var_dim;       /* [nretained] tangent dim (<= max_dim) */
+  const int64_t* var_row;       /* [nretained] offset in the reduced vector */
+  const int64_t* var_full;      /* [nretained] offset in the full tangent vector */
+  const int64_t* var_diag;      /* [nretained] element offset of its dim x dim block in ret_diag / outputs */
+  const int32_t* var_ptr;       /* [nretained + 1] edges of variable v: [var_ptr[v], var_ptr[v+1]) */
+  const int32_t* edge_var;      /* [nedges] retained variable of each edge */
+  const int32_t* edge_elim;     /* [nedges] eliminated variable of each edge */
+  const int64_t* edge_w;        /* [nedges] element offset of its dim x de block in cross and w */
+  const int32_t* elim_ptr;      /* [nelim + 1] CSR over the edges of each eliminated variable */
+  const int32_t* elim_edge;     /* [nnz] edge ids, in (retained variable, edge) order */
+  const double* cross;          /* J_r^T J_e per edge (unscaled) */
+  const double* elim_diag;      /* [nelim][de][de] eliminated diagonal blocks (unscaled) */
+  const double* ret_diag;       /* retained diagonal blocks at var_diag (unscaled) */
+  const double* scale;          /* [n_full] column scale or NULL */
+  double* inv_l;                /* [nelim][de][de] L^-1, L = chol(s C s + lambda I) */
+  void* w;                      /* whitened blocks (wdtype) at edge_w */
+  double* tbuf;                 /* [nelim][de] workspace */
+  double* ybuf;                 /* [nelim][de] workspace: L^-1 b_e */
+  /* retained couplings: the normal operator of the (column-scaled) full
+   * Jacobian with this system's damping, and two full-length float64
+   * workspaces; NULL: the base term is the block-diagonal s U s + lambda I */
+  const tls_normal_args* normal;
+  double* xfull;
+  double* yfull;
+  double damping;
+  int32_t* bad;                 /* device: number of non-PD eliminated blocks */
+  int32_t max_dim;              /* largest retained dim (<= 16) */
+};
+
+/* Factor eliminated blocks and whiten every edge (schur.py:263-283). */
+TLS_API int tls_schur_general_damp(const tls_schur_general_args* a, tls_stream_t stream);
+/* out = base(x) - W W^T x (schur.py:303-328). */
+TLS_API int tls_schur_general_matvec(const tls_schur_general_args* a, const double* x, double* out,
+                                     tls_stream_t stream);
+/* rhs = b_r - W (L^-1 b_e), y_e = L^-1 b_e kept in ybuf; b full, scaled (schur.py:285-290). */
+TLS_API int tls_schur_general_reduced_rhs(const tls_schur_general_args* a, const double* b, double* out,
+                                          tls_stream_t stream);
+/* delta_e = L^-T (y_e - W^T x); writes the full tangent step (schur.py:292-301). */
+TLS_API int tls_schur_general_backsubstitute(const tls_schur_general_args* a, const double* x, double* delta_full,
+                                             tls_stream_t stream);
+/* out (at var_diag) = s U s - sum_e W_e W_e^T per retained variable, W in float64 (schur.py:353-378). */
+TLS_API int tls_schur_general_preconditioner_blocks(const tls_schur_general_args* a, double* out,
+                                                    tls_stream_t stream);
+/* out[i] (da x db) = sum_k W_{edge_a[k]} W_{edge_b[k]}^T over k in [ptr[i], ptr[i+1]): the Schur
+ * cross terms between two members of a joint preconditioner group (schur.py:330-352). */
+TLS_API int tls_schur_general_pair_blocks(const tls_schur_general_args* a, int32_t count, const int32_t* ptr,
+                                          const int32_t* edge_a, const int32_t* edge_b, int32_t da, int32_t db,
+                                          double* out, tls_stream_t stream);
 
 /* Factor eliminated blocks and whiten every edge (schur.py:263-283). */
 TLS_API int tls_schur_damp(const tls_schur_args* a, tls_stream_t stream);

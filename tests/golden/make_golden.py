@@ -89,6 +89,28 @@ def main(reference, only=None):
         np.savez_compressed(os.path.join(HERE, "typed_ba.npz"), **rec)
         print("typed_ba", summ.final_cost, summ.termination_reason, summ.iterations)
 
+    # ---------------------------------------------------------------- general Schur system products
+    if not only or "schur_general" in only:
+        rec = {}
+        g = torch.Generator().manual_seed(31)
+        for tag, builder, groups in (("intr", P.ba_intrinsics, ()), ("joint", P.ba_intrinsics, (("cams", "focal"),)),
+                                     ("priors", P.ba_priors, ()), ("two", P.ba_two_groups, ())):
+            p = builder(tls)
+            an = p._ensure_analyzed()
+            lin = p.linearize()
+            J = lin.jacobian
+            plan = SchurPlan(an, "points", torch.device("cpu"), preconditioner_groups=groups)
+            slin = SchurLinearization(J, J.diagonal_blocks(), plan, dense=True)
+            system = slin.damped(1e-3)
+            vc = torch.randn(plan.dim, generator=g, dtype=torch.float64)
+            rec[f"{tag}_vc"] = arr(vc)
+            rec[f"{tag}_reduced_rhs"] = arr(system.reduced_rhs(-lin.gradient))
+            rec[f"{tag}_matvec"] = arr(system.matvec(vc))
+            rec[f"{tag}_preconditioner"] = arr(system.preconditioner()(vc))
+            rec[f"{tag}_backsubstitute"] = arr(system.backsubstitute(vc))
+            rec[f"{tag}_dense"] = arr(system.dense_matrix())
+        np.savez_compressed(os.path.join(HERE, "schur_general.npz"), **rec)
+
     # ---------------------------------------------------------------- small BA (stored inputs)
     data = synthetic.small_bundle_adjustment(0)
     if only:
@@ -106,6 +128,13 @@ def main(reference, only=None):
         "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient",
                                           termination=tls.TerminationConfig(max_iterations=30))),
         "se2_custom": (P.se2_custom, dict(linear_solver="conjugate_gradient")),
+        "ba_two_groups": (P.ba_two_groups, dict(linear_solver="schur_cg", eliminate="points")),
+        "ba_priors": (P.ba_priors, dict(linear_solver="schur_cg", eliminate="points")),
+        "ba_priors_dense": (P.ba_priors, dict(linear_solver="schur_dense", eliminate="points")),
+        "ba_intrinsics": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points")),
+        "ba_intrinsics_joint": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points",
+                                                      conjugate_gradient=tls.ConjugateGradientConfig(
+                                                          preconditioner_groups=(("cams", "focal"),)))),
         "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
         "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=tls.TrustRegionConfig(
             lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),

@@ -77,6 +77,21 @@ def se2_odometry(a, b, k, z):
     return se2_between(a, b, torch.stack((k[0] * z[0], k[0] * z[1], z[2])))
 
 
+def focal_reprojection(camera, focal, point, observation):
+    """Reprojection with a per-camera focal scale (a second retained group that
+    shares residuals with the camera poses)."""
+    xyz = camera[:3, :3] @ point + camera[:3, 3]
+    valid = xyz[2] > 1e-6
+    z = torch.where(valid, xyz[2], torch.ones_like(xyz[2]))
+    err = focal[0] * xyz[:2] / z - observation
+    return torch.where(valid, err, torch.zeros_like(err))
+
+
+def camera_link(cam_a, cam_b, target):
+    """Relative position prior between two cameras' translations (couples them)."""
+    return cam_a[:3, 3] - cam_b[:3, 3] - target
+
+
 # ---------------------------------------------------------------- builders
 def ba_small(api, device="cpu", dtype=torch.float64, data=None):
     data = data if data is not None else synthetic.small_bundle_adjustment(0)
@@ -142,6 +157,61 @@ def se2_custom(api, device="cpu", dtype=torch.float64):
     p.add_residual(se2_odometry, truth[0].to(**to), ("poses", torch.tensor([0])), ("scale", zero(1)),
                    odo[:1].to(**to), in_dims=(None, 0, 0, 0))
     p.add_residual(se2_between, ("poses", li - 1), ("poses", lj - 1), loop.to(**to))
+    return p
+
+
+def _tiny_data():
+    return synthetic.make_bundle_adjustment(4, 40, 3, seed=7)
+
+
+def ba_two_groups(api, device="cpu", dtype=torch.float64):
+    """The tiny BA with its free cameras split into two retained groups
+    ("cams_a": cameras 1-2, "cams_b": camera 3); no residual couples them."""
+    d = _tiny_data()
+    to = dict(device=device, dtype=dtype)
+    p = api.Problem({"cams_a": d.cameras_init[1:3].to(**to), "cams_b": d.cameras_init[3:4].to(**to),
+                     "points": d.points_init.to(**to)}, manifolds={"cams_a": api.SE3Var, "cams_b": api.SE3Var})
+    huber = api.HuberLoss(0.01)
+    for name, sel, base in (("cams_a", (d.camera_index >= 1) & (d.camera_index <= 2), 1),
+                            ("cams_b", d.camera_index == 3, 3)):
+        p.add_residual(reprojection, (name, d.camera_index[sel] - base), ("points", d.point_index[sel]),
+                       d.uv[sel].to(**to), loss=huber)
+    fixed = d.camera_index == 0
+    p.add_residual(reprojection, d.cameras_true[0].to(**to), ("points", d.point_index[fixed]), d.uv[fixed].to(**to),
+                   in_dims=(None, 0, 0), loss=huber)
+    return p
+
+
+def ba_priors(api, device="cpu", dtype=torch.float64):
+    """The tiny BA plus relative-position priors between consecutive free
+    cameras: residuals that couple two retained variables."""
+    p = ba_tiny(api, device=device, dtype=dtype)
+    d = _tiny_data()
+    a, b = torch.tensor([0, 1]), torch.tensor([1, 2])
+    target = (d.cameras_true[1 + a, :3, 3] - d.cameras_true[1 + b, :3, 3]).to(device=device, dtype=dtype)
+    p.add_residual(camera_link, ("cams", a), ("cams", b), target,
+                   weights=torch.full((2,), 0.5, dtype=dtype, device=device))
+    return p
+
+
+def ba_intrinsics(api, device="cpu", dtype=torch.float64):
+    """The tiny BA with a per-camera focal scale ("focal", 1-dim, cameras 1-3)
+    entering the reprojection of the free cameras (two retained groups coupled
+    in every residual) and a weak prior holding each focal near 1."""
+    d = _tiny_data()
+    to = dict(device=device, dtype=dtype)
+    true_f = torch.tensor([1.0, 1.05, 0.97, 1.02], dtype=torch.float64)
+    uv = d.uv * true_f[d.camera_index][:, None]
+    p = api.Problem({"cams": d.cameras_init[1:].to(**to), "focal": torch.ones(3, 1, **to),
+                     "points": d.points_init.to(**to)}, manifolds={"cams": api.SE3Var})
+    huber = api.HuberLoss(0.01)
+    free = d.camera_index > 0
+    p.add_residual(focal_reprojection, ("cams", d.camera_index[free] - 1), ("focal", d.camera_index[free] - 1),
+                   ("points", d.point_index[free]), uv[free].to(**to), loss=huber)
+    p.add_residual(reprojection, d.cameras_true[0].to(**to), ("points", d.point_index[~free]), uv[~free].to(**to),
+                   in_dims=(None, 0, 0), loss=huber)
+    p.add_residual(point_prior, ("focal", torch.arange(3)), torch.ones(3, 1, **to),
+                   weights=torch.full((3,), 1e-2, dtype=dtype, device=device))
     return p
 
 

@@ -26,6 +26,7 @@ STRUCTS = {
     "tls_pcg_control": L.PcgControl,
     "tls_schur_args": L.SchurArgs,
     "tls_pcg_args": L.PcgArgs,
+    "tls_schur_general_args": L.SchurGeneralArgs,
 }
 
 

@@ -140,6 +140,12 @@ OTHERS = {
     "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "se2_custom": (P.se2_custom, dict(linear_solver="conjugate_gradient")),
+    "ba_two_groups": (P.ba_two_groups, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_priors": (P.ba_priors, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_priors_dense": (P.ba_priors, dict(linear_solver="schur_dense", eliminate="points")),
+    "ba_intrinsics": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_intrinsics_joint": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points",
+                                                  conjugate_gradient=dict(preconditioner_groups=(("cams", "focal"),)))),
     "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
     "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
         lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
@@ -195,3 +201,35 @@ def test_typed_api_solve(tls):
     check_summary(s, SUMMARIES["typed_ba"])
     for i, e in enumerate(problem.layout):
         close(sol._values[e.var_type], fx[f"solve{i}"], 1e-8, what=f"solve{i}")
+
+
+GENERAL_SCHUR = {"intr": (P.ba_intrinsics, ()), "joint": (P.ba_intrinsics, (("cams", "focal"),)),
+                 "priors": (P.ba_priors, ()), "two": (P.ba_two_groups, ())}
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed"])
+@pytest.mark.parametrize("tag", list(GENERAL_SCHUR))
+def test_general_schur_system(tls, tag, precision):
+    """Several retained groups, retained couplings, joint groups (the general
+    Schur kernels) against torchls's own Schur system (schur.py:17-397). Mixed
+    precision stores W in float32: products within 1e-6 there."""
+    from torchls_b200.schur import SchurLinearization, SchurPlan
+
+    builder, groups = GENERAL_SCHUR[tag]
+    fx = load("schur_general")
+    prob = builder(tls, device=DEV)
+    an = prob._ensure_analyzed()
+    plan = SchurPlan(an, "points", torch.device(DEV), preconditioner_groups=groups)
+    assert plan.general
+    wdt = torch.float64 if precision == "native" else torch.float32
+    lin = prob.linearize(jacobian_dtype=wdt, schur=plan)
+    slin = SchurLinearization(plan, lin, lin.jacobian.diagonal_blocks(), None, wdtype=wdt, vec_dtype=torch.float64,
+                              dense=True)
+    system = slin.damped(1e-3)
+    tol = 1e-11 if precision == "native" else 1e-6
+    vc = torch.from_numpy(fx[f"{tag}_vc"]).to(DEV)
+    close(system.reduced_rhs(-lin.gradient), fx[f"{tag}_reduced_rhs"], tol, what="reduced_rhs")
+    close(system.matvec(vc), fx[f"{tag}_matvec"], tol, what="matvec")
+    close(system.preconditioner()(vc), fx[f"{tag}_preconditioner"], max(tol, 1e-10), what="preconditioner")
+    close(system.backsubstitute(vc), fx[f"{tag}_backsubstitute"], tol, what="backsubstitute")
+    close(system.dense_matrix(), fx[f"{tag}_dense"], tol, what="dense")

@@ -150,6 +150,12 @@ OTHERS = {
                                    termination=dict(max_iterations=8))),
     "pose_small": (P.pose_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
     "sim3_small": (P.sim3_small, dict(linear_solver="conjugate_gradient", termination=dict(max_iterations=30))),
+    "ba_two_groups": (P.ba_two_groups, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_priors": (P.ba_priors, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_priors_dense": (P.ba_priors, dict(linear_solver="schur_dense", eliminate="points")),
+    "ba_intrinsics": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points")),
+    "ba_intrinsics_joint": (P.ba_intrinsics, dict(linear_solver="schur_cg", eliminate="points",
+                                                  cg=dict(preconditioner_groups=(("cams", "focal"),)))),
     "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
     "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=dict(
         lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
@@ -203,3 +209,25 @@ def test_sim3_log_inverts_exp():
     delta = torch.from_numpy(fx["delta"])
     keep = delta[:, 3:6].norm(dim=-1) < 3.0
     close(sim3_log(sim3_exp(delta[keep])).numpy(), delta[keep].numpy(), 1e-12, 1e-14)
+
+
+GENERAL_SCHUR = {"intr": (P.ba_intrinsics, ()), "joint": (P.ba_intrinsics, (("cams", "focal"),)),
+                 "priors": (P.ba_priors, ()), "two": (P.ba_two_groups, ())}
+
+
+@pytest.mark.parametrize("tag", list(GENERAL_SCHUR))
+def test_general_schur_system(tag):
+    """Several retained groups, retained couplings and joint groups: the
+    oracle's Schur system against torchls's own (schur.py:17-397)."""
+    builder, groups = GENERAL_SCHUR[tag]
+    fx = load("schur_general")
+    prob = builder(P.OracleAPI).inner
+    lin = prob.linearize(prob.values())
+    plan = SchurPlan(prob, "points", preconditioner_groups=groups)
+    system = SchurLinearization(lin.jacobian, lin.jacobian.diagonal_blocks(), plan, dense=True).damped(1e-3)
+    vc = fx[f"{tag}_vc"]
+    close(system.reduced_rhs(-lin.gradient), fx[f"{tag}_reduced_rhs"], 1e-11)
+    close(system.matvec(vc), fx[f"{tag}_matvec"], 1e-11)
+    close(system.preconditioner()(vc), fx[f"{tag}_preconditioner"], 1e-10)
+    close(system.backsubstitute(vc), fx[f"{tag}_backsubstitute"], 1e-11)
+    close(system.dense_matrix(), fx[f"{tag}_dense"], 1e-11)

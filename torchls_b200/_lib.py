@@ -111,7 +111,18 @@ class PcgArgs(C.Structure):
         ("n", i64), ("vec_dtype", i32), ("op_kind", i32), ("normal", C.POINTER(NormalArgs)),
         ("schur", C.POINTER(SchurArgs)), ("pre", C.POINTER(BlockGroup)), ("npre", i32), ("pad_", i32),
         ("rhs", vp), ("x", vp), ("r", vp), ("z", vp), ("p", vp), ("ap", vp), ("ztrue", vp), ("psave", vp),
-        ("partials", vp), ("control", vp),
+        ("partials", vp), ("control", vp), ("schur_general", vp),
+    ]
+
+
+class SchurGeneralArgs(C.Structure):
+    _fields_ = [
+        ("de", i32), ("nelim", i32), ("nretained", i32), ("wdtype", i32), ("nedges", i64), ("reduced_dim", i64),
+        ("full_dim", i64), ("elim_offset", i64), ("var_dim", vp), ("var_row", vp), ("var_full", vp),
+        ("var_diag", vp), ("var_ptr", vp), ("edge_var", vp), ("edge_elim", vp), ("edge_w", vp), ("elim_ptr", vp),
+        ("elim_edge", vp), ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp),
+        ("w", vp), ("tbuf", vp), ("ybuf", vp), ("normal", C.POINTER(NormalArgs)), ("xfull", vp), ("yfull", vp),
+        ("damping", f64), ("bad", vp), ("max_dim", i32),
     ]
 
 
@@ -134,6 +145,12 @@ _SIGNATURES = {
     "tls_schur_reduced_rhs": [C.POINTER(SchurArgs), vp, vp, vp],
     "tls_schur_backsubstitute": [C.POINTER(SchurArgs), vp, vp, vp],
     "tls_schur_preconditioner_blocks": [C.POINTER(SchurArgs), vp, vp],
+    "tls_schur_general_damp": [C.POINTER(SchurGeneralArgs), vp],
+    "tls_schur_general_matvec": [C.POINTER(SchurGeneralArgs), vp, vp, vp],
+    "tls_schur_general_reduced_rhs": [C.POINTER(SchurGeneralArgs), vp, vp, vp],
+    "tls_schur_general_backsubstitute": [C.POINTER(SchurGeneralArgs), vp, vp, vp],
+    "tls_schur_general_preconditioner_blocks": [C.POINTER(SchurGeneralArgs), vp, vp],
+    "tls_schur_general_pair_blocks": [C.POINTER(SchurGeneralArgs), i32, vp, vp, vp, i32, i32, vp, vp],
     "tls_retract": [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp],
     "tls_reduce": [vp, i32, i64, i32, vp, vp, vp],
     "tls_trial_terms": [i64, i32, vp, vp, i32, f64, vp, vp, vp, i32, vp, vp, vp],

@@ -46,6 +46,35 @@ __device__ __forceinline__ void cholesky_solve_block(const double* L, int dim, c
   }
 }
 
+// Eliminated block of the Schur complement: L = chol(s C s + damping I) of the
+// unscaled block C (row-major DE x DE) and column scales s; writes L^-1
+// (forward substitution on unit vectors). False when a pivot fails.
+template <int DE>
+__device__ __forceinline__ bool eliminated_factor(const double* C_in, const double (&s)[DE], double damping,
+                                                  double* inv_out) {
+  double C[DE * DE], L[DE * DE];
+#pragma unroll
+  for (int i = 0; i < DE; ++i)
+#pragma unroll
+    for (int j = 0; j < DE; ++j) C[i * DE + j] = s[i] * C_in[i * DE + j] * s[j];
+  const bool ok = cholesky_block(C, L, DE, damping);
+  double Li[DE * DE];
+#pragma unroll
+  for (int col = 0; col < DE; ++col) {
+#pragma unroll
+    for (int i = 0; i < DE; ++i) {
+      double t = (i == col) ? 1.0 : 0.0;
+#pragma unroll
+      for (int k = 0; k < DE; ++k)
+        if (k < i) t -= L[i * DE + k] * Li[k * DE + col];
+      Li[i * DE + col] = t / L[i * DE + i];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < DE * DE; ++k) inv_out[k] = Li[k];
+  return ok;
+}
+
 // Column of element k of block i in a (possibly joint) block group.
 __device__ __forceinline__ int64_t block_column(const tls_block_group& g, int64_t i, int k) {
   int start = 0;

@@ -27,6 +27,9 @@ int tls_normal_apply(const tls_normal_args* a, const void* x, void* y, double* d
 int tls_schur_apply(const tls_schur_args* a, const void* x, void* out, double* dot_partials, int* gather_blocks,
                     void* pcg_state, cudaStream_t st);
 int tls_normal_gather_blocks(const tls_normal_args* a);
+int tls_schur_general_apply(const tls_schur_general_args* a, const double* x, double* out, double* dots,
+                            int* gblocks, void* pcg_state, cudaStream_t s);
+int tls_schur_general_ret_blocks(const tls_schur_general_args* a);
 
 namespace tls {
 
@@ -318,6 +321,7 @@ __global__ void set_block_counts_kernel(PcgState* st, int op_blocks, int upd_blo
 // Number of dot partials the operator's final kernel writes (one per block).
 static int operator_blocks(const tls_pcg_args* a) {
   if (a->op_kind == 0) return tls_normal_gather_blocks(a->normal);
+  if (a->op_kind == 2) return tls_schur_general_ret_blocks(a->schur_general);
   return a->schur->nretained;  // one gather block per retained variable
 }
 
@@ -362,10 +366,15 @@ static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
     for (int k = 0; k < steps; ++k) {
       int launched = 0;
       int rc;
-      if (a->op_kind == 0)
+      if (a->op_kind == 0) {
         rc = tls_normal_apply(a->normal, a->p, a->ap, a->partials, &launched, st, s);
-      else
+      } else if (a->op_kind == 2) {
+        if (a->vec_dtype != TLS_F64) return tls_set_error(TLS_ERR_UNSUPPORTED, "general Schur vectors are float64");
+        rc = tls_schur_general_apply(a->schur_general, (const double*)a->p, (double*)a->ap, a->partials, &launched,
+                                     st, s);
+      } else {
         rc = tls_schur_apply(a->schur, a->p, a->ap, a->partials, &launched, st, s);
+      }
       if (rc) return rc;
       if (launched != op_blocks) return tls_set_error(TLS_ERR_INVALID, "operator block count changed");
       if (nb <= kSmallMaxBlocks) {

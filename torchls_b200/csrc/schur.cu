@@ -1016,30 +1016,10 @@ template <int DE>
 __global__ void schur_factor_kernel(tls_schur_args a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.nelim) return;
-  double C[DE * DE], L[DE * DE], s[DE];
+  double s[DE];
 #pragma unroll
   for (int k = 0; k < DE; ++k) s[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
-#pragma unroll
-  for (int i = 0; i < DE; ++i)
-#pragma unroll
-    for (int j = 0; j < DE; ++j) C[i * DE + j] = s[i] * a.elim_diag[p * DE * DE + i * DE + j] * s[j];
-  const bool ok = cholesky_block(C, L, DE, a.damping);
-  if (!ok) atomicAdd(a.bad, 1);
-  // inverse of the lower-triangular L by forward substitution on unit vectors
-  double Li[DE * DE];
-#pragma unroll
-  for (int col = 0; col < DE; ++col) {
-#pragma unroll
-    for (int i = 0; i < DE; ++i) {
-      double t = (i == col) ? 1.0 : 0.0;
-#pragma unroll
-      for (int k = 0; k < DE; ++k)
-        if (k < i) t -= L[i * DE + k] * Li[k * DE + col];
-      Li[i * DE + col] = t / L[i * DE + i];
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < DE * DE; ++k) a.inv_l[p * DE * DE + k] = Li[k];
+  if (!eliminated_factor<DE>(a.elim_diag + p * DE * DE, s, a.damping, a.inv_l + p * DE * DE)) atomicAdd(a.bad, 1);
 }
 
 // W_e = diag(s_i) E_e diag(s_p) L_p^-T into the slabs; padding entries get 0.

@@ -25,7 +25,47 @@ from . import _lib as L
 from .kernels import segment_reduce
 
 
+# (retained dim, eliminated dim) pairs the one-group kernels are built for
+FAST_DIMS = frozenset({(6, 3), (3, 3), (7, 3), (6, 1), (3, 1), (1, 1), (2, 2), (3, 2), (2, 1), (1, 3)})
+
+
+def _one_group_fits(problem, eliminate, preconditioner_groups) -> bool:
+    """Whether the one-group kernels take this system: one retained group of a
+    built shape, no residual with two retained slots, no joint preconditioner
+    groups, every eliminated variable with at most 256 retained neighbours."""
+    layout = problem.layout
+    matches = [i for i, e in enumerate(layout) if e.key == eliminate]
+    if len(matches) != 1 or len(layout) != 2 or preconditioner_groups:
+        return False
+    elim = matches[0]
+    ret = 1 - elim
+    if (layout[ret].dim, layout[elim].dim) not in FAST_DIMS:
+        return False
+    deg = np.zeros(layout[elim].count, np.int64)
+    for plan in problem.plans:
+        rs = [s for s, t in enumerate(plan.type_indices) if t != elim]
+        es = [s for s, t in enumerate(plan.type_indices) if t == elim]
+        if len(rs) > 1:
+            return False
+        if rs and es:
+            np.add.at(deg, plan.indices[es[0]].numpy(), 1)
+    return int(deg.max(initial=0)) <= 256
+
+
 class SchurPlan:
+    """Symbolic Schur structure. Systems the one-group kernels do not take
+    (several retained groups, retained couplings, joint preconditioner groups,
+    other block shapes) get a ``schur_general.GeneralSchurPlan`` instead."""
+
+    general = False
+
+    def __new__(cls, problem, eliminate, device, *, preconditioner_groups=()):
+        if cls is SchurPlan and not _one_group_fits(problem, eliminate, preconditioner_groups):
+            from .schur_general import GeneralSchurPlan
+
+            return GeneralSchurPlan(problem, eliminate, device, preconditioner_groups=preconditioner_groups)
+        return super().__new__(cls)
+
     def __init__(self, problem, eliminate, device, *, preconditioner_groups=()):
         layout = problem.layout
         matches = [i for i, e in enumerate(layout) if e.key == eliminate]
@@ -36,10 +76,6 @@ class SchurPlan:
         self.retained = tuple(i for i in range(len(layout)) if i != self.eliminated)
         if not self.retained:
             raise ValueError("Schur elimination needs a retained parameter group")
-        if len(self.retained) != 1:
-            raise NotImplementedError("the CUDA Schur path supports exactly one retained variable group")
-        if preconditioner_groups:
-            raise NotImplementedError("joint preconditioner groups are not supported with the CUDA Schur path")
         self.device = torch.device(device)
         self.r = layout[self.retained[0]]
         self.dim = self.r.size
@@ -55,9 +91,6 @@ class SchurPlan:
             if eslots and any(not torch.equal(plan.indices[s], plan.indices[eslots[0]]) for s in eslots[1:]):
                 raise ValueError(
                     "Eliminated variables must be independent: a residual connects distinct eliminated indices")
-            if len(rslots) > 1:
-                raise NotImplementedError(
-                    "the CUDA Schur path does not support residuals coupling several retained variables")
             info = dict(eslots=eslots, rslots=rslots, width=0, slot_cross=[-1] * L.MAX_SLOTS, base=0)
             if eslots and rslots:
                 off = 0
@@ -258,6 +291,13 @@ class ChunkLayout:
 
 class SchurLinearization:
     """Cross blocks E_e = J_r^T J_e per edge (schur.py:192-257), in chunk order, float64."""
+
+    def __new__(cls, plan, *args, **kwargs):
+        if cls is SchurLinearization and getattr(plan, "general", False):
+            from .schur_general import GeneralSchurLinearization
+
+            return GeneralSchurLinearization(plan, *args, **kwargs)
+        return super().__new__(cls)
 
     def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
         self.plan = plan

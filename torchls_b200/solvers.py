@@ -354,6 +354,10 @@ class DevicePCG:
             a.op_kind = 0
             keep.append(normal_args)
             a.normal = C.pointer(normal_args)
+        elif isinstance(schur_args, L.SchurGeneralArgs):
+            a.op_kind = 2
+            keep.append(schur_args)
+            a.schur_general = C.addressof(schur_args)
         else:
             a.op_kind = 1
             keep.append(schur_args)
@@ -512,7 +516,7 @@ def pcg(matvec: Callable[[Tensor], Tensor], rhs: Tensor, *, preconditioner=None,
             ws = DevicePCG(rhs.numel(), rhs.dtype, rhs.device)
             return ws.run(rhs, config, normal_args=obj.normal_args(rhs.dtype, damping, tiles=tiles),
                           preconditioner=preconditioner)
-        if kind == "schur" and rhs.dtype == obj.linear.vec_dtype:
+        if kind == "schur" and rhs.dtype == torch.float64:
             ws = DevicePCG(rhs.numel(), rhs.dtype, rhs.device)
             return ws.run(rhs, config, schur_args=obj.args, preconditioner=preconditioner, error_word=obj.plan.err)
     return _generic_pcg(matvec, rhs, preconditioner, config)
@@ -528,6 +532,11 @@ def _operator_of(matvec):
     if isinstance(self_, BlockJacobian) and getattr(matvec, "__func__", None) is BlockJacobian.normal_matvec:
         return "normal", self_, 0.0, True
     if isinstance(self_, DampedSchurSystem) and getattr(matvec, "__func__", None) is DampedSchurSystem.matvec:
+        return "schur", self_, self_.damping, True
+    from .schur_general import GeneralDampedSchurSystem
+
+    if (isinstance(self_, GeneralDampedSchurSystem)
+            and getattr(matvec, "__func__", None) is GeneralDampedSchurSystem.matvec):
         return "schur", self_, self_.damping, True
     return None
 
