@@ -75,35 +75,3 @@ def test_full_system_pcg_matches_generic(points):
     matvec = partial(J.normal_matvec, damping=1e-3)
     res = _compare(tls, lambda v: J.normal_matvec(v, 1e-3), -lin.gradient, pre, device_matvec=matvec)
     assert res.iterations > 5
-
-
-def test_warp_tiles_match_cta_chunks():
-    """Float32 W in 64-edge warp tiles (each warp streams and reduces its own
-    tiles) against the 512-edge CTA chunks on the same system: the reduced
-    rhs, the operator and the persistent PCG agree to rounding."""
-    import torchls_b200 as tls
-    from torchls_b200 import synthetic
-    from torchls_b200.schur import SchurLinearization, SchurPlan
-
-    data = synthetic.make_bundle_adjustment(40, 3000, 6, seed=21)
-    prob = synthetic.build_bundle_adjustment(data, tls, device=DEV, loss=tls.HuberLoss(0.01))
-    an = prob._ensure_analyzed()
-    out = {}
-    for name, max_dim in (("tiles", SchurPlan.TILE_MAX_DIM), ("chunks", 0)):
-        plan = SchurPlan(an, "points", torch.device(DEV))
-        plan.TILE_MAX_DIM = max_dim
-        lin = prob.linearize(jacobian_dtype=torch.float32, schur=plan)
-        slin = SchurLinearization(plan, lin, lin.jacobian.diagonal_blocks(), None, wdtype=torch.float32,
-                                  vec_dtype=torch.float64)
-        assert slin.layout.cap == (64 if name == "tiles" else 512)
-        system = slin.damped(1e-3)
-        rhs = system.reduced_rhs(-lin.gradient)
-        v = torch.linspace(-1.0, 1.0, plan.dim, dtype=torch.float64, device=DEV)
-        res = tls.pcg(system.matvec, rhs, preconditioner=system.preconditioner(),
-                      config=tls.ConjugateGradientConfig(rtol=1e-8, max_iterations=400))
-        out[name] = (rhs, system.matvec(v), res)
-        assert int(plan.err.item()) == 0
-    close(out["tiles"][0], out["chunks"][0], 1e-12, what="reduced rhs")
-    close(out["tiles"][1], out["chunks"][1], 1e-12, what="matvec")
-    assert abs(out["tiles"][2].iterations - out["chunks"][2].iterations) <= 1
-    close(out["tiles"][2].solution, out["chunks"][2].solution, 1e-7, what="pcg solution")

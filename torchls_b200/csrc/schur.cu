@@ -34,7 +34,6 @@
 namespace tls {
 
 constexpr int kChunkThreads = 256;
-constexpr int kTileCap = 64;  // edges per warp tile (float32 W, one warp per tile)
 constexpr int kMetaHead = 4;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -107,9 +106,7 @@ __device__ __forceinline__ void mbar_drain(uint64_t* bar, int from, int to, int3
   for (int k = from; k < to; ++k) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, err);
 }
 
-// A chunk slab of CAP edges processed by NT threads (a CTA of 256, or one
-// warp for the 64-edge warp tiles).
-template <int DR, int DE, int CAP, typename TW, typename TA, int NT = kChunkThreads>
+template <int DR, int DE, int CAP, typename TW, typename TA>
 struct SlabShape {
   static constexpr int kWBytes = DR * DE * CAP * (int)sizeof(TW);
   static constexpr int kMetaInts = 5 * CAP + 8;
@@ -117,7 +114,7 @@ struct SlabShape {
   static constexpr int kStageBytes = kWBytes + kMetaBytes;
   static constexpr int kTBytes = CAP * 4 * (int)sizeof(TA);  // [CAP][4] per-edge / per-variable 3-vectors
   static constexpr int kBaseSmem = 2 * kStageBytes + kTBytes;
-  static constexpr int kEpt = CAP / NT;  // consecutive edges per thread
+  static constexpr int kEpt = CAP / kChunkThreads;  // consecutive edges per thread
   static_assert(kWBytes % 16 == 0 && kMetaBytes % 16 == 0, "slabs must be 16-byte multiples");
   static_assert(kEpt == 1 || kEpt == 2 || kEpt == 4, "edges per thread");
   static_assert(DE <= 4, "eliminated blocks up to 4 wide");
@@ -172,16 +169,11 @@ __device__ __forceinline__ void sts4(TA* p, const TA (&v)[4]) {
 // XS: x was staged in shared memory (as TA). COH: x is rewritten by this
 // kernel between matvecs (persistent loop): plain coherent loads after the
 // grid barrier instead of the read-only (.nc) path.
-template <int DR, int DE, int CAP, int MODE, typename TW, typename TA, bool XS, bool COH, int NT = kChunkThreads>
+template <int DR, int DE, int CAP, int MODE, typename TW, typename TA, bool XS, bool COH>
 __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const double* __restrict__ x, const TA* x_s,
                                               TA* t_s, const TW* Ws, const int32_t* Ms, int c) {
-  constexpr int EPT = CAP / NT;
-  // NT threads share the chunk: the CTA (block barriers) or one warp (warp syncs)
-  auto sync = [] {
-    if constexpr (NT == 32) __syncwarp();
-    else __syncthreads();
-  };
-  const int tid = threadIdx.x % NT, lane = threadIdx.x & 31;
+  constexpr int EPT = CAP / kChunkThreads;
+  const int tid = threadIdx.x, lane = tid & 31;
   const int ne = Ms[0], np = Ms[1];
   const int32_t* er = Ms + kMetaHead;
   const uint32_t* meta = reinterpret_cast<const uint32_t*>(Ms + kMetaHead + CAP);
@@ -216,14 +208,14 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
         }
       }
     }
-    sync();
+    __syncthreads();
   }
   // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges), then overwrite t_s
-  constexpr int PPT = CAP / NT;
+  constexpr int PPT = CAP / kChunkThreads;
   double yreg[PPT][DE];
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
-    const int pl = tid + q * NT;
+    const int pl = tid + q * kChunkThreads;
 #pragma unroll
     for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
     if (pl < np) {
@@ -250,10 +242,10 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       }
     }
   }
-  sync();
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
-    const int pl = tid + q * NT;
+    const int pl = tid + q * kChunkThreads;
     if (pl < np) {
       TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
 #pragma unroll
@@ -261,7 +253,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       sts4(t_s + pl * 4, y);
     }
   }
-  sync();
+  __syncthreads();
   // ---- phase 2: u_e = W_e y_p; segmented sums over runs of equal retained
   // variable (runs never cross a window of 32 * EPT edges): sequential within
   // the thread, then a warp-segmented inclusive scan of the carries over as
@@ -323,7 +315,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       }
     }
   }
-  sync();
+  __syncthreads();
 }
 
 // MODE 0: S x partials; MODE 1: reduced rhs. Persistent over chunks: thread 0
@@ -371,55 +363,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
     const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
     const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
     chunk_compute<DR, DE, CAP, MODE, TW, TA, XS, false>(a, x, x_s, t_s, Ws, Ms, c);
-  }
-}
-
-// The same for 64-edge warp tiles: every warp streams its own tiles
-// (warp w of CTA b: tiles b * 8 + w + j * 8 gridDim.x) through two stages of
-// its own and reduces each with warp syncs only.
-template <int DR, int DE, int CAP, int MODE, typename TW, typename TA>
-__global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_warp_kernel(tls_schur_args a,
-                                                                           const double* __restrict__ x) {
-  using S = SlabShape<DR, DE, CAP, TW, TA, 32>;
-  constexpr int kWarps = kChunkThreads / 32;
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[2 * kWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* unit = smem + warp * S::kBaseSmem;
-  uint64_t* ubar = bar + 2 * warp;
-  TA* t_s = reinterpret_cast<TA*>(unit + 2 * S::kStageBytes);
-  const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
-  const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
-  if (lane == 0) {
-    mbar_init(&ubar[0], 1);
-    mbar_init(&ubar[1], 1);
-    fence_mbar_init();
-  }
-  __syncwarp();
-  auto issue = [&](int c, int stg) {
-    unsigned char* base = unit + stg * S::kStageBytes;
-    fence_proxy_async();
-    mbar_expect_tx(&ubar[stg], S::kStageBytes);
-    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &ubar[stg]);
-    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &ubar[stg]);
-  };
-  const int U = (int)gridDim.x * kWarps;
-  const int u = (int)blockIdx.x * kWarps + warp;
-  if (lane == 0 && u < a.nchunks) issue(u, 0);
-  const long long lim = wait_limit(a);
-  int it = 0;
-  for (int c = u; c < a.nchunks; c += U, ++it) {
-    const int stg = it & 1;
-    const bool next = c + U < a.nchunks;
-    if (lane == 0 && next) issue(c + U, stg ^ 1);
-    const bool ok = mbar_wait_bounded(&ubar[stg], (it >> 1) & 1, a.err, lim);
-    if (__any_sync(0xffffffffu, !ok)) {  // this stage may be incomplete: leave without reading it
-      if (lane == 0) mbar_drain(ubar, it, it + (next ? 2 : 1), a.err);
-      return;
-    }
-    const TW* Ws = reinterpret_cast<const TW*>(unit + stg * S::kStageBytes);
-    const int32_t* Ms = reinterpret_cast<const int32_t*>(unit + stg * S::kStageBytes + S::kWBytes);
-    chunk_compute<DR, DE, CAP, MODE, TW, TA, false, false, 32>(a, x, nullptr, t_s, Ws, Ms, c);
   }
 }
 
@@ -817,19 +760,12 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
 //      the control block, then releases the chunk CTAs.
 // The arithmetic (and its order) is that of schur_pcg_kernel. Every wait is
 // bounded; on timeout the kernel flags a.err and every CTA leaves.
-//
-// NT = 32 (warp tiles, CAP = 64): each warp of a chunk CTA streams its own
-// tiles (warp w of CTA b takes tiles b * 8 + w + j * 8G) through its own two
-// shared-memory stages and mbarriers and reduces them with warp syncs only;
-// the CTA joins its warps once per step, before the barrier. NT = 256: the
-// CTA streams chunks of 512 (float32 W) or 256 (float64 W) edges together.
-template <int DR, int DE, int CAP, typename TW, int D, int NT = kChunkThreads>
+template <int DR, int DE, int CAP, typename TW, int D>
 __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schur_args a, PcgLoop q) {
   using TA = double;
-  using S = SlabShape<DR, DE, CAP, TW, TA, NT>;
-  constexpr int kWarps = kChunkThreads / 32;
+  using S = SlabShape<DR, DE, CAP, TW, TA>;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[NT == 32 ? 2 * kWarps : 2];
+  __shared__ __align__(8) uint64_t bar[2];
   __shared__ double sm[8][DR];
   __shared__ double ux[DR * DR];
   __shared__ double smd[kChunkThreads / 32];
@@ -970,39 +906,28 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     return;
   }
   // ---------------- chunk CTAs
-  // Stages: NT = 256: [stage 0 | stage 1 | t scratch] for the CTA;
-  // NT = 32: per warp [stage 0 | stage 1 | t scratch], warp w at w * kBaseSmem.
-  const int warp = tid >> 5, wl = tid & 31;
-  const int owner = NT == 32 ? wl : tid;  // the thread that issues and drains this unit's copies
-  unsigned char* unit = smem + (NT == 32 ? warp * S::kBaseSmem : 0);
-  uint64_t* ubar = bar + (NT == 32 ? 2 * warp : 0);
-  TA* t_s = reinterpret_cast<TA*>(unit + 2 * S::kStageBytes);
+  TA* t_s = reinterpret_cast<TA*>(smem + 2 * S::kStageBytes);
   const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
   const unsigned char* msrc = reinterpret_cast<const unsigned char*>(a.meta);
-  if (owner == 0) {
-    mbar_init(&ubar[0], 1);
-    mbar_init(&ubar[1], 1);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
   auto issue = [&](int c, int stg) {
-    unsigned char* base = unit + stg * S::kStageBytes;
+    unsigned char* base = smem + stg * S::kStageBytes;
     fence_proxy_async();
-    mbar_expect_tx(&ubar[stg], S::kStageBytes);
-    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &ubar[stg]);
-    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &ubar[stg]);
+    mbar_expect_tx(&bar[stg], S::kStageBytes);
+    bulk_load(base, wsrc + (size_t)c * S::kWBytes, S::kWBytes, &bar[stg]);
+    bulk_load(base + S::kWBytes, msrc + (size_t)c * S::kMetaBytes, S::kMetaBytes, &bar[stg]);
   };
-  // this unit's chunks: u + j * U (u = its index, U = units over the grid), cycled every step
-  const int U = NT == 32 ? G * kWarps : G;
-  const int u = NT == 32 ? (int)blockIdx.x * kWarps + warp : (int)blockIdx.x;
-  const int kct = u < a.nchunks ? (a.nchunks - 1 - u) / U + 1 : 0;
-  auto chunk_of = [&](int j) { return u + (j % kct) * U; };
+  const int kct = (int)blockIdx.x < a.nchunks ? (a.nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+  auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * G; };
   const long long lim = wait_limit(a);
-  __shared__ int s_fail;
-  if (tid == 0) s_fail = 0;
   int it = 0;
   int inflight = 1;  // copies in flight from `it` on when the loop ends
-  if (owner == 0 && kct > 0) issue(chunk_of(0), 0);
+  if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
   for (int step = 0; step < q.steps; ++step) {
     if (tid == 0) {
       const int status = __ldcg(&st->pub.status), mode = __ldcg(&st->pub.mode);
@@ -1011,24 +936,21 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_go) break;
     // ---- A
+    bool failed = false;
     for (int j = 0; j < kct; ++j, ++it) {
       const int stg = it & 1;
-      if (owner == 0) issue(chunk_of(it + 1), stg ^ 1);
-      const bool ok = mbar_wait_bounded(&ubar[stg], (it >> 1) & 1, a.err, lim);
-      bool bad;
-      if constexpr (NT == 32) bad = __any_sync(0xffffffffu, !ok);
-      else bad = __syncthreads_or(!ok);
-      if (bad) {  // this stage may be incomplete: stop without reading it
-        if (owner == 0) atomicExch(&s_fail, 1);
+      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
+      const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+      if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
+        failed = true;
         inflight = 2;
         break;
       }
-      const TW* Ws = reinterpret_cast<const TW*>(unit + stg * S::kStageBytes);
-      const int32_t* Ms = reinterpret_cast<const int32_t*>(unit + stg * S::kStageBytes + S::kWBytes);
-      chunk_compute<DR, DE, CAP, 0, TW, TA, false, true, NT>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
+      const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
+      const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
+      chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
     }
-    __syncthreads();
-    if (s_fail) break;
+    if (failed) break;
     // ---- barrier over the chunk CTAs
     __syncthreads();
     if (tid == 0) {
@@ -1079,7 +1001,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_ok) break;
   }
-  if (kct > 0 && owner == 0) mbar_drain(ubar, it, it + inflight, a.err);
+  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + inflight, a.err);
   __syncthreads();
 }
 
@@ -1303,36 +1225,10 @@ struct SchurOps {
     return launch_chunks<MODE, TW, CAP, false>(a, x, S::kBaseSmem, s);
   }
   template <int MODE, typename TW>
-  static int chunks_warp(const tls_schur_args& a, const double* x, cudaStream_t s) {
-    using S = SlabShape<DR, DE, kTileCap, TW, double, 32>;
-    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
-    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
-      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
-    auto k = schur_chunk_warp_kernel<DR, DE, kTileCap, MODE, TW, double>;
-    const int smem = (kChunkThreads / 32) * S::kBaseSmem;
-    static DeviceGridCache cache;
-    int grid_cap = 0;
-    const int rc = cache.get(smem, &grid_cap, [&](int dev) -> int {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      int per_sm = 0, sms = 0;
-      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kChunkThreads, smem);
-      if (e != cudaSuccess) return -1;
-      return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-    });
-    if (rc) return rc;
-    const int units = (a.nchunks + kChunkThreads / 32 - 1) / (kChunkThreads / 32);
-    const int grid = units < grid_cap ? units : grid_cap;
-    k<<<grid, kChunkThreads, smem, s>>>(a, x);
-    TLS_CHECK_LAUNCH();
-    return TLS_OK;
-  }
-  template <int MODE, typename TW>
   static int chunks(const tls_schur_args& a, const double* x, cudaStream_t s) {
     if (a.nchunks == 0) return TLS_OK;
     if constexpr (sizeof(TW) == 4) {
-      if (a.cap == kTileCap) return chunks_warp<MODE, TW>(a, x, s);
-      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs or 64-edge tiles");
+      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs");
       return chunks_cap<MODE, TW, 512>(a, x, s);
     } else {
       if (a.cap != 256) return tls_set_error(TLS_ERR_INVALID, "float64 W uses 256-edge chunk slabs");
@@ -1387,27 +1283,11 @@ struct SchurOps {
     if (q.n * 6 * (int64_t)sizeof(double) <= S::kBaseSmem) return pcg_launch<TW, CAP, D, true>(a, q, s);
     return pcg_launch<TW, CAP, D, false>(a, q, s);
   }
-  // warp tiles (64-edge slabs): only the vector-CTA kernel; its vectors must
-  // fit in the CTA's shared memory (8 warp units)
-  template <typename TW, int D>
-  static int pcg_tiles(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
-    using S = SlabShape<DR, DE, kTileCap, TW, double, 32>;
-    if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
-    if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
-      return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
-    constexpr int kSmem = (kChunkThreads / 32) * S::kBaseSmem;
-    if (q.n * 6 * (int64_t)sizeof(double) > kSmem)
-      return tls_set_error(TLS_ERR_UNSUPPORTED, "reduced system too large for the warp-tile kernel");
-    return pcg_launch<TW, kTileCap, D, true, 32>(a, q, s);
-  }
-  template <typename TW, int CAP, int D, bool VC, int NT = kChunkThreads>
+  template <typename TW, int CAP, int D, bool VC>
   static int pcg_launch(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
-    using S = SlabShape<DR, DE, CAP, TW, double, NT>;
-    auto k = [] {
-      if constexpr (VC) return schur_pcg_vc_kernel<DR, DE, CAP, TW, D, NT>;
-      else return schur_pcg_kernel<DR, DE, CAP, TW, D>;
-    }();
-    const int smem = (NT == 32 ? kChunkThreads / 32 : 1) * S::kBaseSmem;
+    using S = SlabShape<DR, DE, CAP, TW, double>;
+    auto k = VC ? schur_pcg_vc_kernel<DR, DE, CAP, TW, D> : schur_pcg_kernel<DR, DE, CAP, TW, D>;
+    const int smem = S::kBaseSmem;
     // co-resident CTAs (per-SM occupancy x SMs), per device and instantiation;
     // 0 when the device cannot launch cooperatively
     static DeviceGridCache cache;
@@ -1439,8 +1319,7 @@ struct SchurOps {
   template <typename TW, int D>
   static int pcg_cap(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
     if constexpr (sizeof(TW) == 4) {
-      if (a.cap == kTileCap) return pcg_tiles<TW, D>(a, q, s);
-      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs or 64-edge tiles");
+      if (a.cap != 512) return tls_set_error(TLS_ERR_INVALID, "float32 W uses 512-edge chunk slabs");
       return pcg_go<TW, 512, D>(a, q, s);
     } else {
       if (a.cap != 256) return tls_set_error(TLS_ERR_INVALID, "float64 W uses 256-edge chunk slabs");

@@ -129,26 +129,13 @@ class SchurPlan:
         self.wait_cycles = 0
         self._layouts = {}
 
-    # warp tiles: largest reduced system whose six PCG vectors fit the vector
-    # CTA's shared memory (8 warp units of 13,888 bytes), largest point degree
-    TILE_MAX_DIM = 2304
-    TILE_MAX_DEGREE = 64
-
     def chunks_for(self, wdtype) -> ChunkLayout:
-        """Slab layout for W stored as ``wdtype``: float32 W in 64-edge warp
-        tiles when every eliminated variable has at most 64 edges and the
-        reduced system is small enough for the vector-CTA kernel, else 512-edge
-        chunks; float64 W in 256-edge chunks (36 KB of W per chunk)."""
-        key = (512, 256)
-        if wdtype == torch.float32:
-            deg = np.bincount(self._ei, minlength=self.E_count)
-            if int(deg.max(initial=0)) <= self.TILE_MAX_DEGREE and self.dim <= self.TILE_MAX_DIM:
-                key = (64, 32)
-        else:
-            key = (256, 256)
-        if key not in self._layouts:
-            self._layouts[key] = ChunkLayout(self, *key)
-        return self._layouts[key]
+        """Slab layout for W stored as ``wdtype`` (512 edges per chunk for
+        float32, 256 for float64: 36 KB of W per chunk either way)."""
+        cap = 512 if wdtype == torch.float32 else 256
+        if cap not in self._layouts:
+            self._layouts[cap] = ChunkLayout(self, cap)
+        return self._layouts[cap]
 
     @property
     def chunks(self) -> ChunkLayout:
@@ -188,12 +175,12 @@ class ChunkLayout:
     (``rrun_ptr``), so each retained variable sums a contiguous range.
     """
 
-    def __init__(self, plan: SchurPlan, cap: int, threads: int = 256):
-        """``threads``: the threads that reduce one chunk (256: a CTA; 32: a
-        warp, for 64-edge warp tiles packed greedily with whole points)."""
+    THREADS = 256
+
+    def __init__(self, plan: SchurPlan, cap: int):
         ri, ei, E, P = plan._ri, plan._ei, plan.nedges, plan.E_count
         device = plan.device
-        self.cap, self.threads = cap, threads
+        self.cap = cap
         deg = np.bincount(ei, minlength=P)
         max_deg = int(deg.max()) if E else 0
         if max_deg > cap:
@@ -207,16 +194,7 @@ class ChunkLayout:
         rank[point_order] = np.arange(P)
         deg_o = deg[point_order]
         start = np.cumsum(deg_o) - deg_o
-        if threads == 32:
-            # greedy: each tile takes whole points while their edges fit
-            ends = np.cumsum(deg_o)
-            bounds, b = [0], 0
-            while b < P:
-                b = max(int(np.searchsorted(ends, start[b] + cap, side="right")), b + 1)
-                bounds.append(b)
-            chunk_of_rank = np.repeat(np.arange(len(bounds) - 1), np.diff(bounds))
-        else:
-            chunk_of_rank = start // max(1, cap - max_deg + 1)
+        chunk_of_rank = start // max(1, cap - max_deg + 1)
         ch = chunk_of_rank[rank[ei]]
         order = np.lexsort((ei, ri, ch))
         c_r, c_e, c_raw = ri[order], ei[order], ch[order]
@@ -229,7 +207,7 @@ class ChunkLayout:
         local = np.arange(E) - chunk_ptr[cid] if E else np.zeros(0, np.int64)
         sidx = cid * cap + local
         # runs: equal retained variable, split at warp windows
-        win = 32 * max(1, cap // threads)
+        win = 32 * max(1, cap // self.THREADS)
         self.window = win
         newrun = newchunk.copy()
         newrun[1:] |= c_r[1:] != c_r[:-1]
