@@ -44,7 +44,10 @@ def test_adjoint_matches_unrolled_reference_gradients():
     grads = torch.autograd.grad(loss, uv)
     close(sol["points"], fx["points"], 1e-8, what="points")
     close(sol["cams"], fx["cams"], 1e-8, what="cams")
-    close(loss.detach(), fx["loss"], 1e-8, what="loss")
+    # the loss sums squares of (solved - true) point and camera differences of
+    # about 1e-3: parameters pinned to 1e-8 relative move it by up to ~1e-7
+    # relative (6e-13 absolute on 4.9e-5 in one run), so it is checked there
+    close(loss.detach(), fx["loss"], 1e-7, what="loss")
     close(grads[0], fx["grad_uv_free"], 1e-6, what="d loss / d uv (free cameras)")
     close(grads[1], fx["grad_uv_fixed"], 1e-6, what="d loss / d uv (fixed camera)")
     assert solve_implicit.last["refinement_history"][-1] <= 1e-12
