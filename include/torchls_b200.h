@@ -462,6 +462,14 @@ TLS_API int tls_schur_general_pair_blocks(const tls_schur_general_args* a, int32
                                           const int32_t* edge_a, const int32_t* edge_b, int32_t da, int32_t db,
                                           double* out, tls_stream_t stream);
 
+/* Dense reduced matrix S = s U s + lambda I - W W^T (n = nretained * dr, row-major,
+ * symmetric) from the slabs (schur.py:380-397): per lower block (target_r[t],
+ * target_c[t]) the pairs [ptr[t], ptr[t+1]) of slab entries (pair_a, pair_b) of a
+ * shared eliminated variable, summed in list order. */
+TLS_API int tls_schur_dense_matrix(const tls_schur_args* a, int64_t ntargets, const int32_t* target_r,
+                                   const int32_t* target_c, const int32_t* ptr, const int32_t* pair_a,
+                                   const int32_t* pair_b, double* S, tls_stream_t stream);
+
 /* Factor eliminated blocks and whiten every edge (schur.py:263-283). */
 TLS_API int tls_schur_damp(const tls_schur_args* a, tls_stream_t stream);
 /* out = (s U s + lambda I) x - W W^T x on the reduced vector (schur.py:303-328). */
@@ -475,6 +483,19 @@ TLS_API int tls_schur_backsubstitute(const tls_schur_args* a, const void* x_c, d
 /* Preconditioner blocks s U s - sum_e W_e W_e^T -> out [nretained][dr][dr]
  * (schur.py:353-363); the damping is added by tls_block_cholesky. */
 TLS_API int tls_schur_preconditioner_blocks(const tls_schur_args* a, double* out, tls_stream_t stream);
+
+/* ---------------------------------------------------------------- dense Cholesky
+ * Replaces: torch.linalg.cholesky / cholesky_solve at the reference's dense
+ * sites (solvers.py:517-518 schur_dense, schur.py:380-397, linear_system.py:61-98).
+ * Row-major float64, lower triangle. Blocked right-looking (64-column panels)
+ * with the trailing updates on the FP64 tensor cores; deterministic. */
+/* In place: A (n x n, leading dimension lda) <- L with zeros above the diagonal;
+ * *info (device) = 0, or the 1-based index of the first pivot that is not
+ * positive (then L is not usable). */
+TLS_API int tls_dense_cholesky(int64_t n, double* A, int64_t lda, int32_t* info, tls_stream_t stream);
+/* In place: B (n x nrhs, leading dimension ldb) <- (L L^T)^-1 B; n <= 29,056. */
+TLS_API int tls_dense_cholesky_solve(int64_t n, const double* L, int64_t lda, int64_t nrhs, double* B, int64_t ldb,
+                                     tls_stream_t stream);
 
 /* ---------------------------------------------------------------- retraction
  * Replaces: variables.py:153-160 / 242-249 with geometry.py:40-160 retractions.

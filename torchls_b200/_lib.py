@@ -151,6 +151,9 @@ _SIGNATURES = {
     "tls_schur_general_backsubstitute": [C.POINTER(SchurGeneralArgs), vp, vp, vp],
     "tls_schur_general_preconditioner_blocks": [C.POINTER(SchurGeneralArgs), vp, vp],
     "tls_schur_general_pair_blocks": [C.POINTER(SchurGeneralArgs), i32, vp, vp, vp, i32, i32, vp, vp],
+    "tls_schur_dense_matrix": [C.POINTER(SchurArgs), i64, vp, vp, vp, vp, vp, vp, vp],
+    "tls_dense_cholesky": [i64, vp, i64, vp, vp],
+    "tls_dense_cholesky_solve": [i64, vp, i64, i64, vp, i64, vp],
     "tls_retract": [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp],
     "tls_reduce": [vp, i32, i64, i32, vp, vp, vp],
     "tls_trial_terms": [i64, i32, vp, vp, i32, f64, vp, vp, vp, i32, vp, vp, vp],

@@ -33,6 +33,7 @@ import torch
 from torch import Tensor
 
 from .problem import _is_ref
+from . import dense
 from .variables import euclidean_type
 
 __all__ = ["newton_polish", "objective", "solve_implicit"]
@@ -135,7 +136,7 @@ class _Operators:
         raw = lin.jacobian.diagonal_blocks()
         slin = SchurLinearization(plan, lin, raw, None, wdtype=torch.float64, vec_dtype=torch.float64, dense=True)
         system = slin.damped(0.0)
-        fac, info = torch.linalg.cholesky_ex(system.dense_matrix())
+        fac, info = dense.cholesky_ex(system.dense_matrix())
         if int(info) > 0:
             raise torch.linalg.LinAlgError(
                 "Gauss-Newton reduced matrix is singular at the solution: fix the gauge (priors or fixed variables)")
@@ -146,7 +147,7 @@ class _Operators:
         kind, lin, system, fac = self._gauss_newton()
         if kind == "schur":
             rc = system.reduced_rhs(b)
-            xc = torch.cholesky_solve(rc.double()[:, None], fac).reshape(-1)
+            xc = dense.cholesky_solve(rc.double(), fac)
             return system.backsubstitute(xc)
         from functools import partial
 

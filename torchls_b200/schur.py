@@ -257,6 +257,8 @@ class ChunkLayout:
             rank_in_chunk = np.arange(E) - chunk_ptr[cid[po]]
             M[cid[po], off_pe + rank_in_chunk] = local[po]
         self.nchunks, self.nruns, self.nedges = nchunks, nruns, E
+        self._host = (c_r, c_e, sidx, plan.r.count, P)
+        self._dense_pairs = None
         self.order, self.pos_of_edge = order, np.empty(E, np.int64)
         self.pos_of_edge[order] = np.arange(E)
         self.slab_of_edge = np.empty(E, np.int64)
@@ -287,6 +289,35 @@ class ChunkLayout:
         )
         self.cross_seg = L.Segments(nslab, plan.dr * plan.de, 1, 0, self.dev["cross_ptr"].data_ptr(),
                                     self.dev["cross_src"].data_ptr())
+
+
+def _dense_pairs(layout: ChunkLayout):
+    """Per lower block (i, j), i >= j, of the reduced matrix: the pairs of slab
+    entries (a, b), retained variables i and j, of each eliminated variable
+    they share, in eliminated-variable order (device int32 arrays, built once)."""
+    if layout._dense_pairs is None:
+        c_r, c_e, sidx, nret, P = layout._host
+        order = np.lexsort((c_r, c_e))  # by eliminated variable, then retained
+        r_s, s_s = c_r[order], sidx[order]
+        deg = np.bincount(c_e, minlength=P)
+        start = np.cumsum(deg) - deg
+        pa, pb = [], []
+        for d in np.unique(deg[deg > 0]):
+            base = start[deg == d]
+            ti, tj = np.tril_indices(int(d))
+            pa.append((base[:, None] + ti[None, :]).reshape(-1))
+            pb.append((base[:, None] + tj[None, :]).reshape(-1))
+        pa = np.concatenate(pa) if pa else np.zeros(0, np.int64)
+        pb = np.concatenate(pb) if pb else np.zeros(0, np.int64)
+        key = r_s[pa] * nret + r_s[pb]
+        o = np.lexsort((pb, pa, key))
+        key, pa, pb = key[o], pa[o], pb[o]
+        uniq, first = np.unique(key, return_index=True)
+        ptr = np.concatenate((first, [len(key)]))
+        dev = layout.dev["meta"].device
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device=dev, dtype=torch.int32)  # noqa: E731
+        layout._dense_pairs = (t(uniq // nret), t(uniq % nret), t(ptr), t(s_s[pa]), t(s_s[pb]))
+    return layout._dense_pairs
 
 
 class SchurLinearization:
@@ -406,41 +437,13 @@ class DampedSchurSystem:
                                                      None, p.dim, check=check)
 
     def dense_matrix(self) -> torch.Tensor:
-        """Dense reduced matrix (s U s + lambda I) - W W^T, symmetrised (schur.py:380-397)."""
+        """Dense reduced matrix (s U s + lambda I) - W W^T (schur.py:380-397),
+        assembled from the slabs by ``tls_schur_dense_matrix``: one warp per
+        camera-pair block sums the products of their shared eliminated
+        variables in a fixed order; the result is exactly symmetric."""
         p = self.plan
-        E = p.nedges
-        n = p.dim
-        S = torch.zeros((n, n), dtype=torch.float64, device=p.device)
-        # base blocks
-        U = self.linear.ret_diag
-        if self.linear.scale is not None:
-            s = self.linear.scale[p.r.offset : p.r.offset + p.r.size].view(p.r.count, p.dr)
-            U = U * s[:, :, None] * s[:, None, :]
-        idx = torch.arange(p.r.count, device=p.device)[:, None] * p.dr + torch.arange(p.dr, device=p.device)
-        S[idx[:, :, None], idx[:, None, :]] = U
-        S += self.damping * torch.eye(n, dtype=torch.float64, device=p.device)
-        if E:
-            # W rows (retained columns) x eliminated columns, sparse COO -> dense chunks
-            lay = self.linear.layout
-            valid = (lay.dev["slab_r"] >= 0).nonzero().flatten()
-            slab = self.linear.w.view(lay.nslab // lay.cap, p.dr * p.de, lay.cap).permute(1, 0, 2).reshape(
-                p.dr, p.de, lay.nslab).to(torch.float64)
-            w = slab[:, :, valid]
-            er = lay.dev["slab_r"][valid].long()
-            ee = lay.dev["slab_e"][valid].long()
-            cols_all = ee[:, None] * p.de + torch.arange(p.de, device=p.device)[None, :]
-            rows_all = er[:, None] * p.dr + torch.arange(p.dr, device=p.device)[None, :]
-            step = max(1, (1 << 27) // max(n, 1))
-            ncols = p.e.count * p.de
-            for c0 in range(0, ncols, step):
-                c1 = min(ncols, c0 + step)
-                sel = ((cols_all[:, 0] >= c0) & (cols_all[:, 0] < c1)).nonzero().flatten()
-                if sel.numel() == 0:
-                    continue
-                Wd = torch.zeros((n, c1 - c0), dtype=torch.float64, device=p.device)
-                r_idx = rows_all[sel][:, :, None].expand(-1, p.dr, p.de)
-                c_idx = (cols_all[sel] - c0)[:, None, :].expand(-1, p.dr, p.de)
-                vals = w[:, :, sel].permute(2, 0, 1)
-                Wd[r_idx.reshape(-1), c_idx.reshape(-1)] = vals.reshape(-1)
-                S -= Wd @ Wd.T
-        return 0.5 * (S + S.T)
+        tr, tc, ptr, pa, pb = _dense_pairs(self.linear.layout)
+        S = torch.empty((p.dim, p.dim), dtype=torch.float64, device=p.device)
+        L.call("tls_schur_dense_matrix", C.byref(self.args), tr.numel(), tr.data_ptr(), tc.data_ptr(), ptr.data_ptr(),
+               pa.data_ptr(), pb.data_ptr(), S.data_ptr(), self.stream)
+        return S

@@ -25,6 +25,7 @@ import torch
 from torch import Tensor
 
 from . import _lib as L
+from . import dense
 from .bounds import BoundsPlan
 from .kernels import reduce
 from .schur import DampedSchurSystem, SchurLinearization, SchurPlan
@@ -716,10 +717,10 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
                         rhs = system.reduced_rhs(-linear_gradient)
                     with _region("linear_solve", profile):
                         if linear_solver == "schur_dense":
-                            fac, info = torch.linalg.cholesky_ex(system.dense_matrix())
+                            fac, info = dense.cholesky_ex(system.dense_matrix())
                             if int(info) > 0:
                                 raise torch.linalg.LinAlgError("dense Schur matrix is not positive definite")
-                            retained = torch.cholesky_solve(rhs.double()[:, None], fac).reshape(-1)
+                            retained = dense.cholesky_solve(rhs.double(), fac)
                             its, conv = 1, True
                             usable = _finite(retained)
                             summary.linear_relative_residual_history.append(None)
