@@ -497,6 +497,41 @@ TLS_API int tls_dense_cholesky(int64_t n, double* A, int64_t lda, int32_t* info,
 TLS_API int tls_dense_cholesky_solve(int64_t n, const double* L, int64_t lda, int64_t nrhs, double* B, int64_t ldb,
                                      tls_stream_t stream);
 
+/* ---------------------------------------------------------------- fixed linear systems
+ * Replaces: linear_system.py:15-141 (FixedLinearSystem, LinearFactor,
+ * least_absolute_deviations) for a sparse m x n matrix A (COO, coalesced):
+ * entries in row order with a column-ordered index, and the pairs of entries
+ * of each row that meet at normal-matrix element target = c1 * n + c2
+ * (sorted targets, pairs in row order). Vectors are float64, row-major
+ * [rows][k] for k right-hand sides. */
+typedef struct tls_fixed_system {
+  int64_t m, n, nnz, ntargets;
+  const int32_t* row_ptr;       /* [m + 1] entries of each row */
+  const int32_t* row;           /* [nnz] row of each entry */
+  const int32_t* col;           /* [nnz] column of each entry */
+  const double* val;            /* [nnz] */
+  const int32_t* col_ptr;       /* [n + 1] */
+  const int32_t* col_entry;     /* [nnz] entries of each column, ascending row */
+  const int64_t* target;        /* [ntargets] normal-matrix element c1 * n + c2 */
+  const int32_t* target_ptr;    /* [ntargets + 1] */
+  const int32_t* pair_left;     /* entry pairs (same row) of each target */
+  const int32_t* pair_right;
+} tls_fixed_system;
+
+/* y = A x (x [n][k], y [m][k]) (linear_system.py:42-46). */
+TLS_API int tls_fixed_matvec(const tls_fixed_system* s, const double* x, int64_t k, double* y, tls_stream_t stream);
+/* y = A^T x (x [m][k], y [n][k]) (linear_system.py:48-52). */
+TLS_API int tls_fixed_rmatvec(const tls_fixed_system* s, const double* x, int64_t k, double* y, tls_stream_t stream);
+/* N (n x n, dense) = A^T diag(w) A + ridge I; weights [m] or NULL (linear_system.py:54-73). */
+TLS_API int tls_fixed_normal(const tls_fixed_system* s, const double* weights, double ridge, double* N,
+                             tls_stream_t stream);
+/* One LAD ADMM update (linear_system.py:126-133) over `count` entries: z <- soft(ax - target + u, kappa),
+ * u += ax - z - target, zdiff = z_new - z_old, next = target + z - u (the next least-squares target);
+ * out[0..2] = |primal|^2, |ax|^2, |z|^2 (deterministic sums); partials holds >= 3 * 1024 doubles. */
+TLS_API int tls_admm_step(int64_t count, const double* ax, const double* target, double* z, double* u,
+                          double* zdiff, double* next, double kappa, double* partials, double* out,
+                          tls_stream_t stream);
+
 /* ---------------------------------------------------------------- retraction
  * Replaces: variables.py:153-160 / 242-249 with geometry.py:40-160 retractions.
  * out[i] = values[i] * Exp(delta[i]) (right update) for Lie groups,

@@ -89,6 +89,30 @@ def main(reference, only=None):
         np.savez_compressed(os.path.join(HERE, "typed_ba.npz"), **rec)
         print("typed_ba", summ.final_cost, summ.termination_reason, summ.iterations)
 
+    # ---------------------------------------------------------------- fixed linear system / LAD
+    if not only or "fixed_system" in only:
+        from torchls.linear_system import FixedLinearSystem, least_absolute_deviations
+
+        A, x, y, w, target = P.fixed_system_case()
+        fs = FixedLinearSystem(A.to_sparse())
+        rec = dict(A=arr(A), x=arr(x), y=arr(y), w=arr(w), target=arr(target))
+        rec["matvec"] = arr(fs.matvec(x))
+        rec["rmatvec"] = arr(fs.rmatvec(y))
+        rec["matvec1"] = arr(fs.matvec(x[:, 0]))
+        fac = fs.factor(w, ridge=0.1)
+        rec["weighted_ls"] = arr(fac.least_squares(target))
+        rec["cholesky"] = arr(fac.cholesky)
+        rec["solve"] = arr(fs.factor().solve(x))
+        lad = least_absolute_deviations(fs, target, rho=0.3, max_iterations=200)
+        rec["lad_solution"] = arr(lad.solution)
+        rec["lad_iterations"] = np.asarray(lad.iterations)
+        rec["lad_converged"] = np.asarray(lad.converged)
+        lad1 = least_absolute_deviations(fs, target[:, 0], rho=1.0, max_iterations=60)
+        rec["lad1_solution"] = arr(lad1.solution)
+        rec["lad1_iterations"] = np.asarray(lad1.iterations)
+        np.savez_compressed(os.path.join(HERE, "fixed_system.npz"), **rec)
+        print("fixed_system LAD", lad.iterations, lad.converged, lad1.iterations)
+
     # ---------------------------------------------------------------- general Schur system products
     if not only or "schur_general" in only:
         rec = {}

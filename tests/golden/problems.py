@@ -371,3 +371,22 @@ class OracleAPI:
 
 def oracle_problem(builder, **kw):
     return builder(OracleAPI, **kw).inner
+
+
+def fixed_system_case():
+    """A seeded sparse 240 x 30 matrix (about 4 entries per row), two
+    right-hand sides, row weights and an LAD target with 10 % gross outliers."""
+    g = torch.Generator().manual_seed(41)
+    m, n = 240, 30
+    A = torch.zeros(m, n, dtype=torch.float64)
+    for r in range(m):
+        cols = torch.randperm(n, generator=g)[:4]
+        A[r, cols] = torch.randn(4, generator=g, dtype=torch.float64)
+    x = torch.randn(n, 2, generator=g, dtype=torch.float64)
+    y = torch.randn(m, 2, generator=g, dtype=torch.float64)
+    w = torch.rand(m, generator=g, dtype=torch.float64) + 0.2
+    truth = torch.randn(n, 2, generator=g, dtype=torch.float64)
+    target = A @ truth + 0.01 * torch.randn(m, 2, generator=g, dtype=torch.float64)
+    bad = torch.randperm(m, generator=g)[: m // 10]
+    target[bad] += 5.0 * torch.randn(len(bad), 2, generator=g, dtype=torch.float64)
+    return A, x, y, w, target

@@ -27,6 +27,7 @@ STRUCTS = {
     "tls_schur_args": L.SchurArgs,
     "tls_pcg_args": L.PcgArgs,
     "tls_schur_general_args": L.SchurGeneralArgs,
+    "tls_fixed_system": L.FixedSystem,
 }
 
 

@@ -23,6 +23,7 @@ from .geometry import (
     so3_log,
     so3_retract_jvp,
 )
+from .linear_system import FixedLinearSystem, LADResult, LinearFactor, least_absolute_deviations
 from .losses import HuberLoss, Loss
 from .named import Problem
 from .problem import AnalyzedLeastSquaresProblem, LeastSquaresProblem, Linearization
@@ -48,6 +49,9 @@ __all__ = [
     "BlockJacobian",
     "ConjugateGradientConfig",
     "Cost",
+    "FixedLinearSystem",
+    "LADResult",
+    "LinearFactor",
     "CudaDiagonalPlan",
     "CudaNormalPlan",
     "HuberLoss",
@@ -67,6 +71,7 @@ __all__ = [
     "Var",
     "VarValues",
     "block_jacobi",
+    "least_absolute_deviations",
     "pcg",
     "reprojection",
     "se3_between",

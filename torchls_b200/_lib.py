@@ -115,6 +115,14 @@ class PcgArgs(C.Structure):
     ]
 
 
+class FixedSystem(C.Structure):
+    _fields_ = [
+        ("m", i64), ("n", i64), ("nnz", i64), ("ntargets", i64), ("row_ptr", vp), ("row", vp), ("col", vp),
+        ("val", vp), ("col_ptr", vp), ("col_entry", vp), ("target", vp), ("target_ptr", vp), ("pair_left", vp),
+        ("pair_right", vp),
+    ]
+
+
 class SchurGeneralArgs(C.Structure):
     _fields_ = [
         ("de", i32), ("nelim", i32), ("nretained", i32), ("wdtype", i32), ("nedges", i64), ("reduced_dim", i64),
@@ -153,6 +161,10 @@ _SIGNATURES = {
     "tls_schur_general_pair_blocks": [C.POINTER(SchurGeneralArgs), i32, vp, vp, vp, i32, i32, vp, vp],
     "tls_schur_dense_matrix": [C.POINTER(SchurArgs), i64, vp, vp, vp, vp, vp, vp, vp],
     "tls_dense_cholesky": [i64, vp, i64, vp, vp],
+    "tls_fixed_matvec": [C.POINTER(FixedSystem), vp, i64, vp, vp],
+    "tls_fixed_rmatvec": [C.POINTER(FixedSystem), vp, i64, vp, vp],
+    "tls_fixed_normal": [C.POINTER(FixedSystem), vp, f64, vp, vp],
+    "tls_admm_step": [i64, vp, vp, vp, vp, vp, vp, f64, vp, vp, vp],
     "tls_dense_cholesky_solve": [i64, vp, i64, i64, vp, i64, vp],
     "tls_retract": [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp],
     "tls_reduce": [vp, i32, i64, i32, vp, vp, vp],
