@@ -532,6 +532,101 @@ TLS_API int tls_admm_step(int64_t count, const double* ax, const double* target,
                           double* zdiff, double* next, double kappa, double* partials, double* out,
                           tls_stream_t stream);
 
+/* ---------------------------------------------------------------- batched independent problems
+ * Replaces, per problem, the reduced-system CG of solvers.py:167-256 (pcg)
+ * and the LM decisions of solvers.py:597-689 when thousands of independent
+ * problems are merged into one block-diagonal system (batched.py). Problem p
+ * owns the retained variables [ret_ptr[p], ret_ptr[p+1]) and one dense
+ * n_p x n_p reduced matrix (n_p = its variables x dr) at element s_off[p] of S,
+ * row-major in the storage type sdtype; diag keeps each variable's dr x dr
+ * diagonal block in float64 (the block-Jacobi preconditioner). */
+typedef struct tls_batched_systems {
+  int32_t nproblems, nretained;
+  int32_t dr, sdtype;             /* dr 3, 6 or 7; TLS_F32 / TLS_F64 */
+  const int32_t* ret_ptr;         /* [nproblems + 1] */
+  const int32_t* ret_problem;     /* [nretained] */
+  const int64_t* s_off;           /* [nproblems] */
+  void* S;
+  double* diag;                   /* [nretained][dr][dr] */
+} tls_batched_systems;
+
+/* S_p = s U s + lambda I - W W^T of every problem from the one-group Schur
+ * slabs (schur.py:380-397 per diagonal block of the merged system), the
+ * lower blocks (target_r, target_c) and their pairs as for
+ * tls_schur_dense_matrix; each entry is summed in float64 in list order and
+ * rounded once to sdtype, and S_p is exactly symmetric. */
+TLS_API int tls_batched_schur_dense(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntargets,
+                                    const int32_t* target_r, const int32_t* target_c, const int32_t* ptr,
+                                    const int32_t* pair_a, const int32_t* pair_b, tls_stream_t stream);
+
+/* Preconditioned CG of every problem in ONE persistent launch (torchls
+ * solvers.py:167-256 per problem: x0 = 0, threshold max(atol, rtol |b_p|),
+ * stop on the recurrence residual, on a curvature p.Ap that is not positive
+ * and finite, or after max_iterations). The CTAs pull tasks from a work
+ * queue (*queue, zeroed by this call): task t is task_size[t] <= task_groups[t]
+ * problems order[task_first[t] ...], task_groups[t] in {1, 2, 4, 8} problems
+ * sharing one 256-thread CTA (8 / task_groups[t] warps each) and smem_bytes /
+ * task_groups[t] bytes of its dynamic shared memory (tls_batched_share_bytes
+ * gives a problem's need; with the cache its matrix is read from shared
+ * memory). iterations[p] and status[p] (0; 1 when a diagonal block is not
+ * positive definite, x_p = 0; 2 when the share is too small, *err = 1) are
+ * written for every problem of the tasks. Results do not depend on the tiling. */
+typedef struct tls_batched_pcg_args {
+  const double* rhs;              /* [sum n_p] reduced right-hand sides */
+  double* x;                      /* [sum n_p] solutions */
+  int32_t* iterations;            /* [nproblems] */
+  int32_t* status;                /* [nproblems] */
+  const int32_t* order;
+  const int32_t* task_first;
+  const int32_t* task_size;
+  const int32_t* task_groups;
+  int32_t* queue;                 /* one device int32 */
+  int32_t* err;                   /* one device int32, set on failure */
+  double rtol, atol;
+  int32_t ntasks, max_iterations;
+  int32_t smem_bytes, pad_;       /* dynamic shared memory per CTA (<= 227 KB) */
+} tls_batched_pcg_args;
+
+TLS_API int tls_batched_pcg(const tls_batched_systems* sys, const tls_batched_pcg_args* a, tls_stream_t stream);
+
+/* Shared-memory bytes a problem of `blocks` variables needs in its group's
+ * share, without (with_cache = 0) or with its packed matrix. */
+TLS_API int64_t tls_batched_share_bytes(int32_t dr, int32_t blocks, int32_t sdtype, int32_t with_cache);
+
+/* Per factor of rows [nfactors][rdim]: obj = 1/2 w rho(|new|^2) and
+ * red = 1/2 w (rho(|old|^2) - rho(|new|^2)) with the exact forms of
+ * losses.py:92-107 (loss 0: rho(s) = s, difference (old-new).(old+new);
+ * loss 1: Huber delta, divided difference across the kink); weights may be NULL. */
+TLS_API int tls_factor_terms(int64_t nfactors, int32_t rdim, const double* old_raw, const double* new_raw,
+                             int32_t loss, double delta, const double* weights, double* obj, double* red,
+                             tls_stream_t stream);
+/* out[f] = |rows[f]|^2 for rows [nfactors][rdim]. */
+TLS_API int tls_factor_sqnorm(int64_t nfactors, int32_t rdim, const double* rows, double* out,
+                              tls_stream_t stream);
+
+enum { TLS_BATCH_MAX_ITERATIONS = 0, TLS_BATCH_GRADIENT_TOLERANCE = 1, TLS_BATCH_COST_TOLERANCE = 2,
+       TLS_BATCH_TRIALS_EXHAUSTED = 3 };
+
+/* Per-problem step decision (solvers.py:597-689): gain ratio actual /
+ * predicted (-inf when predicted <= 0), acceptance of tried problems (finite
+ * new cost, actual > 0, ratio >= step_quality_min), cost update, damping
+ * divided by lambda_factor when the ratio is above 0.75 and multiplied on
+ * rejection (clamped), step counters, and the cost-tolerance stop
+ * (|actual| <= cost_tolerance (cost + actual)), which clears active and sets
+ * reason; accepted problems leave pending. */
+typedef struct tls_batched_lm {
+  int32_t nproblems, pad_;
+  double lambda_factor, lambda_min, lambda_max, step_quality_min, cost_tolerance;
+  const double *actual, *predicted, *new_cost;
+  double *cost, *lam;
+  const uint8_t* tried;
+  uint8_t *ok, *active, *pending;
+  int64_t *accepted, *rejected;
+  int32_t* reason;
+} tls_batched_lm;
+
+TLS_API int tls_batched_lm_update(const tls_batched_lm* m, tls_stream_t stream);
+
 /* ---------------------------------------------------------------- retraction
  * Replaces: variables.py:153-160 / 242-249 with geometry.py:40-160 retractions.
  * out[i] = values[i] * Exp(delta[i]) (right update) for Lie groups,

@@ -134,6 +134,34 @@ class SchurGeneralArgs(C.Structure):
     ]
 
 
+# termination codes of tls_batched_lm_update's reason array
+BATCH_MAX_ITERATIONS, BATCH_GRADIENT_TOLERANCE, BATCH_COST_TOLERANCE, BATCH_TRIALS_EXHAUSTED = 0, 1, 2, 3
+
+
+class BatchedSystems(C.Structure):
+    _fields_ = [
+        ("nproblems", i32), ("nretained", i32), ("dr", i32), ("sdtype", i32), ("ret_ptr", vp), ("ret_problem", vp),
+        ("s_off", vp), ("S", vp), ("diag", vp),
+    ]
+
+
+class BatchedPcgArgs(C.Structure):
+    _fields_ = [
+        ("rhs", vp), ("x", vp), ("iterations", vp), ("status", vp), ("order", vp), ("task_first", vp),
+        ("task_size", vp), ("task_groups", vp), ("queue", vp), ("err", vp), ("rtol", f64), ("atol", f64),
+        ("ntasks", i32), ("max_iterations", i32), ("smem_bytes", i32), ("pad_", i32),
+    ]
+
+
+class BatchedLm(C.Structure):
+    _fields_ = [
+        ("nproblems", i32), ("pad_", i32), ("lambda_factor", f64), ("lambda_min", f64), ("lambda_max", f64),
+        ("step_quality_min", f64), ("cost_tolerance", f64), ("actual", vp), ("predicted", vp), ("new_cost", vp),
+        ("cost", vp), ("lam", vp), ("tried", vp), ("ok", vp), ("active", vp), ("pending", vp), ("accepted", vp),
+        ("rejected", vp), ("reason", vp),
+    ]
+
+
 _SIGNATURES = {
     "tls_linearize": [C.POINTER(LinearizeArgs), vp],
     "tls_segment_reduce": [C.POINTER(Segments), vp, i32, i32, i32, vp, i32, vp],
@@ -166,6 +194,12 @@ _SIGNATURES = {
     "tls_fixed_normal": [C.POINTER(FixedSystem), vp, f64, vp, vp],
     "tls_admm_step": [i64, vp, vp, vp, vp, vp, vp, f64, vp, vp, vp],
     "tls_dense_cholesky_solve": [i64, vp, i64, i64, vp, i64, vp],
+    "tls_batched_schur_dense": [C.POINTER(SchurArgs), C.POINTER(BatchedSystems), i64, vp, vp, vp, vp, vp, vp],
+    "tls_batched_pcg": [C.POINTER(BatchedSystems), C.POINTER(BatchedPcgArgs), vp],
+    "tls_batched_share_bytes": [i32, i32, i32, i32],
+    "tls_factor_terms": [i64, i32, vp, vp, i32, f64, vp, vp, vp, vp],
+    "tls_factor_sqnorm": [i64, i32, vp, vp, vp],
+    "tls_batched_lm_update": [C.POINTER(BatchedLm), vp],
     "tls_retract": [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp],
     "tls_reduce": [vp, i32, i64, i32, vp, vp, vp],
     "tls_trial_terms": [i64, i32, vp, vp, i32, f64, vp, vp, vp, i32, vp, vp, vp],
@@ -190,7 +224,8 @@ def lib():
         for name, argtypes in _SIGNATURES.items():
             fn = getattr(handle, name)
             fn.argtypes = argtypes
-            fn.restype = {"tls_last_error": C.c_char_p, "tls_launch_count": C.c_int64}.get(name, C.c_int)
+            fn.restype = {"tls_last_error": C.c_char_p, "tls_launch_count": C.c_int64,
+                          "tls_batched_share_bytes": C.c_int64}.get(name, C.c_int)
         _lib = handle
     return _lib
 

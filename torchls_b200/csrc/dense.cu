@@ -250,9 +250,11 @@ __global__ void schur_dense_base_kernel(tls_schur_args a, double* __restrict__ S
   double v = 0.0;
   if (i == j) {
     const int rr = (int)(r % a.dr), cc = (int)(c % a.dr);
-    const double sr = a.scale ? a.scale[a.retained_offset + r] : 1.0;
-    const double sc = a.scale ? a.scale[a.retained_offset + c] : 1.0;
-    v = sr * a.ret_diag[i * a.dr * a.dr + rr * a.dr + cc] * sc + (rr == cc ? a.damping : 0.0);
+    // scales in index order: entries (r, c) and (c, r) get the same bits
+    const int64_t lo = r < c ? r : c, hi = r < c ? c : r;
+    const double sl = a.scale ? a.scale[a.retained_offset + lo] : 1.0;
+    const double sh = a.scale ? a.scale[a.retained_offset + hi] : 1.0;
+    v = sl * a.ret_diag[i * a.dr * a.dr + rr * a.dr + cc] * sh + (rr == cc ? a.damping : 0.0);
   }
   S[e] = v;
 }
