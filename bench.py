@@ -12,7 +12,11 @@ the float64 reference cost within 1e-8 relative.
 Prints one JSON line (rank 0). ``value`` is seconds per solve in mixed
 precision (lower is better); ``fp64_s`` the same solve in float64. Several
 GPUs run independent replicas of the same solve ("replicas only": one coupled
-problem does not shard); timing is the max over ranks.
+problem does not shard); timing is the max over ranks. The line also carries
+``dense_cholesky`` (the reduced-camera matrix's assembly, factor and solve
+against cuSOLVER) and compact ``pose_graph`` and ``batched`` records (one
+timed solve each of the 100,000-pose graph and of the 4,096-problem batch;
+``--no-subrecords`` skips them, ``--workload`` runs either alone in full).
 """
 
 from __future__ import annotations
@@ -56,6 +60,8 @@ def parse():
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-subrecords", action="store_true",
+                    help="skip the compact pose-graph and batched records of the default line")
     ap.add_argument("--small", action="store_true", help="10-camera / 4,000-observation case (debug)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="only build the workload and time the matvec kernels (the ncu capture target)")
@@ -284,8 +290,42 @@ def kernel_roofline(problem, tls, device):
     torch.cuda.synchronize(device)
     pcg_s = s.elapsed_time(e) / 1e3
     applications = res.iterations + res.residual_checks
-    return dict(schur_s=schur_s, schur_bytes=schur_bytes, normal_s=normal_s, normal_bytes=normal_bytes,
-                normal_two_pass_s=two_pass_s, nedges=E, pcg_s=pcg_s, pcg_applications=applications)
+    out = dict(schur_s=schur_s, schur_bytes=schur_bytes, normal_s=normal_s, normal_bytes=normal_bytes,
+               normal_two_pass_s=two_pass_s, nedges=E, pcg_s=pcg_s, pcg_applications=applications)
+    out["dense"] = dense_cholesky_record(system, flush)
+    return out
+
+
+def dense_cholesky_record(system, flush):
+    """The schur_dense path's dense step on this system: assembly of the
+    reduced-camera matrix S from the slabs, its float64 Cholesky factor and one
+    solve, this package's kernels against torch.linalg.cholesky_ex /
+    torch.cholesky_solve (cuSOLVER) on the same matrix; mean device time of 20
+    calls each, L2 flushed before each."""
+    from torchls_b200 import dense
+
+    S = system.dense_matrix()
+    n = S.shape[0]
+    assemble_s = timed_reps(system.dense_matrix, 20, flush)
+    for _ in range(3):
+        dense.cholesky_ex(S)
+        torch.linalg.cholesky_ex(S)
+    ours_s = timed_reps(lambda: dense.cholesky_ex(S), 20, flush)
+    ref_s = timed_reps(lambda: torch.linalg.cholesky_ex(S), 20, flush)
+    fac, info = dense.cholesky_ex(S)
+    fac_ref = torch.linalg.cholesky(S)
+    rhs = torch.randn(n, dtype=torch.float64, device=S.device)
+    solve_s = timed_reps(lambda: dense.cholesky_solve(rhs, fac), 20, flush)
+    solve_ref_s = timed_reps(lambda: torch.cholesky_solve(rhs[:, None], fac_ref), 20, flush)
+    x = dense.cholesky_solve(rhs, fac)
+    flops = n ** 3 / 3.0
+    return {"n": n, "assembly_us": assemble_s * 1e6, "cholesky_us": ours_s * 1e6,
+            "cusolver_cholesky_us": ref_s * 1e6, "cholesky_speedup_vs_cusolver": ref_s / ours_s,
+            "cholesky_gflops": flops / ours_s / 1e9, "solve_us": solve_s * 1e6,
+            "cusolver_solve_us": solve_ref_s * 1e6, "info": int(info),
+            "max_factor_difference_rel": float((fac - fac_ref).abs().max() / fac_ref.abs().max()),
+            "solve_residual_rel": float((S @ x - rhs).norm() / rhs.norm()),
+            "matrix": "reduced-camera S of the 1M-observation BA (float32 W, lambda 1e-3)"}
 
 
 def e2e_steps(data, tls, device, steps, precision):
@@ -398,10 +438,11 @@ def pose_normal_matvec(problem, init, device, flush):
     return normal[True], normal[False], nnz * 4 + slots * 4 + 2 * J.shape[1] * 8
 
 
-def run_pose(args, world, rank, local):
+def pose_measure(args, world, rank, local, steps, warmup, normal=True):
     """SE(3) pose graph: 100,000 poses on a random walk, 99,999 odometry edges
     and 300,000 loop closures (drawn with replacement among pairs within 3 m),
-    pose 0 fixed; LM with full-system block-Jacobi PCG, 30 iterations."""
+    pose 0 fixed; LM with full-system block-Jacobi PCG, 30 iterations. Returns
+    the result line (every rank measures; rank 0 prints)."""
     import torchls_b200 as tls
     from torchls_b200 import synthetic
 
@@ -414,30 +455,31 @@ def run_pose(args, world, rank, local):
     target = json.load(open(POSE_TARGET_FILE))["final_cost"] if os.path.exists(POSE_TARGET_FILE) else None
     if args.roofline_only:
         normal_s, two_pass_s, normal_bytes = pose_normal_matvec(problem, init, device, flush)
-        if rank == 0:
-            print(json.dumps({"normal_s": normal_s, "normal_two_pass_s": two_pass_s, "normal_bytes": normal_bytes}),
-                  flush=True)
-        return
+        return {"normal_s": normal_s, "normal_two_pass_s": two_pass_s, "normal_bytes": normal_bytes}
     barrier(world)
     with ClockSampler(local) as clocks:
-        times, summ, launches = time_solves(problem, init, tls, "mixed", args.steps, args.warmup, device, flush,
+        times, summ, launches = time_solves(problem, init, tls, "mixed", steps, warmup, device, flush,
                                             opts=pose_opts(tls, "mixed"))
     mixed_s = dist_max(sum(times) / len(times), world, device)
-    t64, s64, _ = time_solves(problem, init, tls, "native", max(1, args.steps), 1, device, flush,
+    t64, s64, _ = time_solves(problem, init, tls, "native", max(1, steps), 1, device, flush,
                               opts=pose_opts(tls, "native"))
     fp64_s = dist_max(sum(t64) / len(t64), world, device)
-    normal_s, two_pass_s, normal_bytes = pose_normal_matvec(problem, init, device, flush)
+    roof = None
+    if normal:
+        normal_s, two_pass_s, normal_bytes = pose_normal_matvec(problem, init, device, flush)
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        gbs = normal_bytes / normal_s / 1e9
+        roof = {"kernel": "full normal matvec (normal_tile_kernel + tile_gather_kernel)", "bound": "hbm",
+                "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
+                "algorithmic_bytes": normal_bytes, "traffic": NCU_POSE_NORMAL_TRAFFIC_BYTES,
+                "two_pass_us": two_pass_s * 1e6, "l2": "flushed before each application (256 MB write, then read back)"}
     barrier(world)
-    if rank != 0:
-        return
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    gbs = normal_bytes / normal_s / 1e9
     rel = None if target is None else abs(summ.final_cost - target) / target
     line = {
-        "metric": POSE_METRIC, "value": mixed_s, "unit": "s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": mixed_s * 1e3, "higher_is_better": False, "scaling": "weak",
+        "metric": POSE_METRIC, "value": mixed_s, "unit": "s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": mixed_s * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
         "config": {"workload": "pose_graph_100k", "poses": 100_000, "edges": int(data.edge_i.numel()),
                    "solver": "conjugate_gradient", "max_lm_iterations": 30, "parallelism": f"replicas x{world}",
@@ -446,14 +488,17 @@ def run_pose(args, world, rank, local):
         "lm_iterations": summ.iterations, "cg_iterations": summ.linear_iterations_history,
         "lm_iterations_per_s": summ.iterations / mixed_s, "fp64_s": fp64_s, "fp64_final_cost": s64.final_cost,
         "fp64_cg_iterations": s64.linear_iterations_history, "mixed_speedup_vs_fp64": fp64_s / mixed_s,
-        "roofline": {"kernel": "full normal matvec (normal_tile_kernel + tile_gather_kernel)", "bound": "hbm",
-                     "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "us_per_launch": normal_s * 1e6,
-                     "algorithmic_bytes": normal_bytes, "traffic": NCU_POSE_NORMAL_TRAFFIC_BYTES,
-                     "two_pass_us": two_pass_s * 1e6,
-                     "l2": "flushed before each application (256 MB write, then read back)"},
         "gpu_launches": launches, "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    if roof is not None:
+        line["roofline"] = roof
+    return line
+
+
+def run_pose(args, world, rank, local):
+    line = pose_measure(args, world, rank, local, args.steps, args.warmup)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # ----------------------------------------------------------------------------- implicit adjoint workload
@@ -561,12 +606,12 @@ def run_adjoint(args, world, rank, local):
 BATCH_METRIC = "batched BA solve s (4,096 uneven problems, per-problem LM) vs one solve per problem"
 
 
-def run_batched(args, world, rank, local):
+def batched_measure(args, world, rank, local, steps, warmup, stride=64):
     """4,096 bundle adjustments (seeds 0..4095): cameras uniform in {2..32},
     points log-uniform in [20, 2000], min(6, cameras) views per point, Huber
     0.01, <= 20 LM iterations each; one batched solve against one solve per
-    problem through the same library (timed on a 64-problem sample,
-    extrapolated to 4,096)."""
+    problem through the same library (timed on every ``stride``-th problem,
+    extrapolated to 4,096). Returns the result line (rank 0's is printed)."""
     import torchls_b200 as tls
     from torchls_b200 import synthetic
     from torchls_b200.batched import BatchedProblem, partition_problems
@@ -598,18 +643,18 @@ def run_batched(args, world, rank, local):
         torch.cuda.synchronize(device)
         return e0.elapsed_time(e1) / 1e3, summ
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         batched_once("mixed")
     times, summ = [], None
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
+        for _ in range(steps):
             t, summ = batched_once("mixed")
             times.append(t)
     batched_s = dist_max(statistics.median(times), world, device)
     batched_once("native")  # untimed: the float64 tiling is tuned on the first native solve
     t64, summ64 = batched_once("native")
     t64 = dist_max(t64, world, device)
-    sample = list(range(0, 4096, 64)) if world == 1 else []
+    sample = list(range(0, 4096, stride)) if world == 1 else []
     single, diffs = [], []
     opts = dict(linear_solver="schur_cg", eliminate="points", return_summary=True,
                 conjugate_gradient=tls.ConjugateGradientConfig(precision="mixed"),
@@ -629,25 +674,31 @@ def run_batched(args, world, rank, local):
         diffs.append(abs(float(summ.final_cost[j]) - s.final_cost) / max(s.final_cost, 1e-300))
     per_problem_s = sum(single) / len(single) * 4096 if single else None
     barrier(world)
-    if rank != 0:
-        return
     reasons = {}
     for r in summ.termination:
         reasons[r] = reasons.get(r, 0) + 1
     line = {
-        "metric": BATCH_METRIC, "value": batched_s, "unit": "s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": batched_s * 1e3, "higher_is_better": False, "scaling": "weak",
+        "metric": BATCH_METRIC, "value": batched_s, "unit": "s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": batched_s * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
         "config": {"workload": "ba_batched_4096", "problems": 4096, "observations": obs,
                    "max_lm_iterations": 20, "parallelism": f"problems sharded x{world}"},
         "fp64_s": t64, "analysis_s": analysis_s, "one_solve_per_problem_s": per_problem_s,
-        "one_solve_per_problem_sample": f"{len(sample)} problems (every 64th seed), mean x 4096" if single else None,
+        "one_solve_per_problem_sample": (f"{len(sample)} problems (every {stride}th seed), mean x 4096"
+                                         if single else None),
         "speedup_vs_one_solve_per_problem": per_problem_s / batched_s if single else None,
         "max_rel_cost_difference_vs_individual_solves": max(diffs) if diffs else None,
         "batched_iterations": summ.iterations, "linear_solves": summ.linear_solves,
         "pcg_iterations": summ.linear_iterations, "termination": reasons, "clocks": clocks.summary(),
+        "tiling": bp.systems.tiling[torch.float32][1],
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_batched(args, world, rank, local):
+    line = batched_measure(args, world, rank, local, args.steps, args.warmup)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # ----------------------------------------------------------------------------- arms
@@ -688,6 +739,22 @@ def workload_config(args, world):
             "l2": "flushed between steps (256 MB write, then read back); working set also exceeds L2"}
 
 
+def subrecords_of(args, world, rank, local):
+    """Compact records of the pose-graph and batched workloads (one timed
+    solve each after one warm-up), so that the default line carries them."""
+    keep_pose = ("value", "unit", "final_cost", "target_cost", "rel_cost_error", "lm_iterations", "fp64_s",
+                 "fp64_final_cost", "mixed_speedup_vs_fp64", "gpu_launches", "clocks")
+    pose = pose_measure(args, world, rank, local, 1, 1, normal=False)
+    keep_batched = ("value", "unit", "fp64_s", "one_solve_per_problem_s", "one_solve_per_problem_sample",
+                    "speedup_vs_one_solve_per_problem", "max_rel_cost_difference_vs_individual_solves",
+                    "pcg_iterations", "termination", "tiling", "clocks")
+    batched = batched_measure(args, world, rank, local, 1, 1, stride=256)
+    return {"pose_graph": {"workload": "pose_graph_100k (SE(3), 100,000 poses, 399,999 edges)", "metric": POSE_METRIC,
+                           **{k: pose[k] for k in keep_pose}},
+            "batched": {"workload": "ba_batched_4096 (4,096 uneven bundle adjustments)", "metric": BATCH_METRIC,
+                        **{k: batched[k] for k in keep_batched}}}
+
+
 def run_cuda(args, world, rank, local):
     import torchls_b200 as tls
 
@@ -717,6 +784,9 @@ def run_cuda(args, world, rank, local):
     e2e_s, h2d, d2h = e2e_steps(data, tls, device, args.steps, "mixed")
     e2e_s = dist_max(e2e_s, world, device)
     barrier(world)
+    subrecords = None
+    if not (args.no_subrecords or args.small):
+        subrecords = subrecords_of(args, world, rank, local)
     if rank != 0:
         return
     peaks = {}
@@ -762,6 +832,9 @@ def run_cuda(args, world, rank, local):
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
     }
+    line["dense_cholesky"] = roof["dense"]
+    if subrecords is not None:
+        line.update(subrecords)
     if world == 1 and not args.no_cpu_baseline:
         torch.set_num_threads(os.cpu_count() or 1)
         v, cs = cpu_solve(args.small)

@@ -463,9 +463,10 @@ TLS_API int tls_schur_general_pair_blocks(const tls_schur_general_args* a, int32
                                           double* out, tls_stream_t stream);
 
 /* Dense reduced matrix S = s U s + lambda I - W W^T (n = nretained * dr, row-major,
- * symmetric) from the slabs (schur.py:380-397): per lower block (target_r[t],
- * target_c[t]) the pairs [ptr[t], ptr[t+1]) of slab entries (pair_a, pair_b) of a
- * shared eliminated variable, summed in list order. */
+ * exactly symmetric) from the slabs (schur.py:380-397): per lower block
+ * (target_r[t], target_c[t]) the pairs [ptr[t], ptr[t+1]) of slab entries
+ * (pair_a, pair_b) of a shared eliminated variable, summed in a fixed order
+ * (the assembly of tls_batched_schur_dense for one problem). */
 TLS_API int tls_schur_dense_matrix(const tls_schur_args* a, int64_t ntargets, const int32_t* target_r,
                                    const int32_t* target_c, const int32_t* ptr, const int32_t* pair_a,
                                    const int32_t* pair_b, double* S, tls_stream_t stream);
@@ -493,7 +494,7 @@ TLS_API int tls_schur_preconditioner_blocks(const tls_schur_args* a, double* out
  * *info (device) = 0, or the 1-based index of the first pivot that is not
  * positive (then L is not usable). */
 TLS_API int tls_dense_cholesky(int64_t n, double* A, int64_t lda, int32_t* info, tls_stream_t stream);
-/* In place: B (n x nrhs, leading dimension ldb) <- (L L^T)^-1 B; n <= 29,056. */
+/* In place: B (n x nrhs, leading dimension ldb) <- (L L^T)^-1 B; n <= 22,816. */
 TLS_API int tls_dense_cholesky_solve(int64_t n, const double* L, int64_t lda, int64_t nrhs, double* B, int64_t ldb,
                                      tls_stream_t stream);
 
@@ -544,17 +545,19 @@ typedef struct tls_batched_systems {
   int32_t nproblems, nretained;
   int32_t dr, sdtype;             /* dr 3, 6 or 7; TLS_F32 / TLS_F64 */
   const int32_t* ret_ptr;         /* [nproblems + 1] */
-  const int32_t* ret_problem;     /* [nretained] */
+  const int32_t* ret_problem;     /* [nretained]; NULL (with ret_ptr and s_off): one problem of every variable */
   const int64_t* s_off;           /* [nproblems] */
   void* S;
-  double* diag;                   /* [nretained][dr][dr] */
+  double* diag;                   /* [nretained][dr][dr]; may be NULL for the assembly alone */
 } tls_batched_systems;
 
 /* S_p = s U s + lambda I - W W^T of every problem from the one-group Schur
  * slabs (schur.py:380-397 per diagonal block of the merged system), the
  * lower blocks (target_r, target_c) and their pairs as for
- * tls_schur_dense_matrix; each entry is summed in float64 in list order and
- * rounded once to sdtype, and S_p is exactly symmetric. */
+ * tls_schur_dense_matrix; each entry is summed in float64 in a fixed order
+ * (for dr 3 or 6 and de 3: lane l of a block's warp takes pairs l, l + 32, ...
+ * and the 32 lane sums are added in lane order; else list order) and rounded
+ * once to sdtype, and S_p is exactly symmetric. */
 TLS_API int tls_batched_schur_dense(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntargets,
                                     const int32_t* target_r, const int32_t* target_c, const int32_t* ptr,
                                     const int32_t* pair_a, const int32_t* pair_b, tls_stream_t stream);

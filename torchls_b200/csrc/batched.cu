@@ -44,18 +44,29 @@ __device__ __forceinline__ int64_t slab_index(int64_t s, int k, int cap, int kw)
   return ((s / cap) * kw + k) * cap + (s % cap);
 }
 
+// The problem of retained variable i: its first variable, dimension and
+// matrix offset; without problem arrays, one problem of every variable.
+struct ProblemView {
+  int64_t first, n, off;
+};
+
+__device__ __forceinline__ ProblemView problem_of(const tls_batched_systems& b, int64_t i, int dr) {
+  if (!b.ret_problem) return {0, (int64_t)b.nretained * dr, 0};
+  const int p = b.ret_problem[i];
+  const int64_t first = b.ret_ptr[p];
+  return {first, (int64_t)(b.ret_ptr[p + 1] - first) * dr, b.s_off[p]};
+}
+
 // ---------------------------------------------------------------- assembly
 // One CTA per retained variable i: its dr rows of S_p (zeros outside the
 // diagonal block) and its float64 diagonal block.
 template <typename TS>
 __global__ void __launch_bounds__(128) batched_dense_base_kernel(tls_schur_args a, tls_batched_systems b) {
   const int64_t i = blockIdx.x;
-  const int p = b.ret_problem[i];
-  const int first = b.ret_ptr[p];
   const int dr = a.dr;
-  const int64_t n = (int64_t)(b.ret_ptr[p + 1] - first) * dr;
-  const int li = (int)(i - first);
-  TS* S = reinterpret_cast<TS*>(b.S) + b.s_off[p];
+  const ProblemView pv = problem_of(b, i, dr);
+  const int64_t n = pv.n, li = i - pv.first;
+  TS* S = reinterpret_cast<TS*>(b.S) + pv.off;
   for (int64_t e = threadIdx.x; e < dr * n; e += blockDim.x) {
     const int r = (int)(e / n);
     const int64_t c = e % n;
@@ -63,7 +74,7 @@ __global__ void __launch_bounds__(128) batched_dense_base_kernel(tls_schur_args 
     if (c / dr == li) {
       const int cc = (int)(c % dr);
       v = base_entry(a, i, r, cc);
-      b.diag[(i * dr + r) * dr + cc] = v;
+      if (b.diag) b.diag[(i * dr + r) * dr + cc] = v;
     }
     S[((int64_t)li * dr + r) * n + c] = static_cast<TS>(v);
   }
@@ -87,11 +98,9 @@ __global__ void __launch_bounds__(128) batched_dense_pairs_kernel(tls_schur_args
   const int dr = a.dr, de = a.de, kw = dr * de;
   const TW* w = reinterpret_cast<const TW*>(a.w);
   const int64_t i = target_r[t], j = target_c[t];
-  const int p = b.ret_problem[i];
-  const int first = b.ret_ptr[p];
-  const int64_t n = (int64_t)(b.ret_ptr[p + 1] - first) * dr;
-  const int64_t li = i - first, lj = j - first;
-  TS* S = reinterpret_cast<TS*>(b.S) + b.s_off[p];
+  const ProblemView pv = problem_of(b, i, dr);
+  const int64_t n = pv.n, li = i - pv.first, lj = j - pv.first;
+  TS* S = reinterpret_cast<TS*>(b.S) + pv.off;
   for (int ent = lane; ent < dr * dr; ent += 32) {
     const int r = ent / dr, c = ent % dr;
     double acc = 0.0;
@@ -106,7 +115,7 @@ __global__ void __launch_bounds__(128) batched_dense_pairs_kernel(tls_schur_args
     S[(li * dr + r) * n + lj * dr + c] = static_cast<TS>(v);
     if (i != j)
       S[(lj * dr + c) * n + li * dr + r] = static_cast<TS>(v);
-    else
+    else if (b.diag)
       b.diag[(i * dr + r) * dr + c] = v;
   }
 }
@@ -158,11 +167,9 @@ __global__ void __launch_bounds__(128) batched_dense_lanes_kernel(tls_schur_args
   for (int e = 0; e < NE; ++e) red[warp][lane][e] = acc[e];
   __syncwarp();
   const int64_t i = target_r[t], j = target_c[t];
-  const int p = b.ret_problem[i];
-  const int first = b.ret_ptr[p];
-  const int64_t n = (int64_t)(b.ret_ptr[p + 1] - first) * DR;
-  const int64_t li = i - first, lj = j - first;
-  TS* S = reinterpret_cast<TS*>(b.S) + b.s_off[p];
+  const ProblemView pv = problem_of(b, i, DR);
+  const int64_t n = pv.n, li = i - pv.first, lj = j - pv.first;
+  TS* S = reinterpret_cast<TS*>(b.S) + pv.off;
   for (int e = lane; e < NE; e += 32) {
     double sum = 0.0;
     for (int l = 0; l < 32; ++l) sum += red[warp][l][e];
@@ -171,7 +178,7 @@ __global__ void __launch_bounds__(128) batched_dense_lanes_kernel(tls_schur_args
     S[(li * DR + r) * n + lj * DR + c] = static_cast<TS>(v);
     if (i != j)
       S[(lj * DR + c) * n + li * DR + r] = static_cast<TS>(v);
-    else
+    else if (b.diag)
       b.diag[(i * DR + r) * DR + c] = v;
   }
 }
@@ -511,12 +518,11 @@ __global__ void batched_lm_update_kernel(tls_batched_lm m) {
 
 using namespace tls;
 
-extern "C" int tls_batched_schur_dense(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntargets,
-                                       const int32_t* target_r, const int32_t* target_c, const int32_t* ptr,
-                                       const int32_t* pair_a, const int32_t* pair_b, tls_stream_t stream) {
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (!a || !b || !b->S || !b->diag || b->nretained != a->nretained || b->dr != a->dr)
-    return tls_set_error(TLS_ERR_INVALID, "batched reduced matrices: bad arguments");
+namespace {
+
+int assemble(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntargets, const int32_t* target_r,
+             const int32_t* target_c, const int32_t* ptr, const int32_t* pair_a, const int32_t* pair_b,
+             cudaStream_t s) {
   if (b->nretained > 0) {
     if (b->sdtype == TLS_F64)
       batched_dense_base_kernel<double><<<b->nretained, 128, 0, s>>>(*a, *b);
@@ -548,6 +554,30 @@ extern "C" int tls_batched_schur_dense(const tls_schur_args* a, const tls_batche
   }
   TLS_CHECK_LAUNCH();
   return TLS_OK;
+}
+
+}  // namespace
+
+extern "C" int tls_batched_schur_dense(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntargets,
+                                       const int32_t* target_r, const int32_t* target_c, const int32_t* ptr,
+                                       const int32_t* pair_a, const int32_t* pair_b, tls_stream_t stream) {
+  if (!a || !b || !b->S || b->nretained != a->nretained || b->dr != a->dr ||
+      (b->ret_problem && (!b->ret_ptr || !b->s_off)))
+    return tls_set_error(TLS_ERR_INVALID, "batched reduced matrices: bad arguments");
+  return assemble(a, b, ntargets, target_r, target_c, ptr, pair_a, pair_b, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tls_schur_dense_matrix(const tls_schur_args* a, int64_t ntargets, const int32_t* target_r,
+                                      const int32_t* target_c, const int32_t* ptr, const int32_t* pair_a,
+                                      const int32_t* pair_b, double* S, tls_stream_t stream) {
+  if (!a || !S) return tls_set_error(TLS_ERR_INVALID, "dense Schur matrix: bad arguments");
+  tls_batched_systems b{};
+  b.nproblems = 1;
+  b.nretained = a->nretained;
+  b.dr = a->dr;
+  b.sdtype = TLS_F64;
+  b.S = S;
+  return assemble(a, &b, ntargets, target_r, target_c, ptr, pair_a, pair_b, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int64_t tls_batched_share_bytes(int32_t dr, int32_t blocks, int32_t sdtype, int32_t with_cache) {

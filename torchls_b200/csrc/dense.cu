@@ -4,9 +4,10 @@
 // call sites: the reduced-camera matrix of schur_dense (torchls
 // solvers.py:517-518, schur.py:380-397) and FixedLinearSystem's normal
 // matrix (linear_system.py:61-98). Blocked right-looking factorisation with
-// 64-column panels; per panel three launches:
-//   diag    the 64 x 64 diagonal block, unblocked, in shared memory
-//   panel   the rows below it times L_kk^-T (one thread per row)
+// 64-column panels; per panel two launches:
+//   panel   every CTA factors the 64 x 64 diagonal block in shared memory (one
+//           barrier per column; CTA 0 writes it back), then its 256 rows below
+//           it times L_kk^-T (one thread per row)
 //   update  the trailing lower triangle -= P P^T, one 64 x 64 tile per CTA on
 //           the FP64 tensor cores (mma.sync m8n8k4 .f64; 4 warps, each a
 //           32 x 32 quadrant of 16 accumulator tiles)
@@ -21,70 +22,115 @@ namespace tls {
 
 constexpr int kNB = 64;  // panel width
 
-// ---------------------------------------------------------------- diagonal block
-// Unblocked right-looking Cholesky of A[k:k+nb, k:k+nb] in shared memory.
-__global__ void __launch_bounds__(256) chol_diag_kernel(int64_t n, double* __restrict__ A, int64_t lda, int64_t k,
-                                                        int32_t* __restrict__ info) {
-  __shared__ double S[kNB][kNB + 1];
-  const int nb = (int)((n - k) < kNB ? (n - k) : kNB);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += 256) {
-    const int i = e / nb, j = e % nb;
-    S[i][j] = j <= i ? A[(k + i) * lda + k + j] : 0.0;
+// ---------------------------------------------------------------- diagonal block and panel
+// Cholesky of the nb x nb diagonal block A[k:k+nb, k:k+nb] in shared memory
+// (every CTA of the panel launch factors it; CTA 0 writes it back), then the
+// rows below it times L_kk^-T. The 64 x 64 block (a partial last block is
+// padded with the identity) is itself factored in four 16-column sub-panels:
+//   1. the 16 x 16 diagonal sub-block, column by column (thread (i, l) of a
+//      16 x 16 grid subtracts S[i][j] S[l][j] / S[j][j]; one barrier per
+//      column), then normalised: L[j][j] = sqrt(pivot), L[i][j] /= L[j][j];
+//   2. the rows below it inside the block times its L^-T (thread per row);
+//   3. the trailing part of the block minus that panel times its transpose.
+// The pivot tested is the Schur-complement diagonal (L[j][j]^2).
+__device__ __forceinline__ void factor_diag_block(int64_t n, const double* __restrict__ A, int64_t lda, int64_t k,
+                                                  int nb, double (*S)[kNB + 1], int32_t* info, bool report) {
+  constexpr int kSub = 16;
+  const int tid = threadIdx.x;  // blockDim.x == 256
+  __shared__ int first_bad;
+  for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+    const int i = e >> 6, j = e & (kNB - 1);
+    S[i][j] = (i < nb && j <= i) ? A[(k + i) * lda + k + j] : (i == j ? 1.0 : 0.0);
   }
+  if (tid == 0) first_bad = kNB;
   __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    if (tid == 0) {
+#pragma unroll
+  for (int sb = 0; sb < kNB; sb += kSub) {
+    const int ti = sb + (tid >> 4), tl = sb + (tid & (kSub - 1));
+    for (int j = sb; j < sb + kSub; ++j) {
+      double d = S[j][j];
+      if (!(d > 0.0) || !isfinite(d)) d = 1.0;  // keep going on a usable value; info reports it
+      if (tl > j && tl <= ti) S[ti][tl] -= S[ti][j] * S[tl][j] * (1.0 / d);
+      __syncthreads();
+    }
+    if (tid < kSub) {
+      const int j = sb + tid;
       double d = S[j][j];
       if (!(d > 0.0) || !isfinite(d)) {
-        atomicCAS(info, 0, (int32_t)(k + j + 1));
-        d = 1.0;  // keep going on a usable value; the caller reads info
+        atomicMin(&first_bad, j);
+        d = 1.0;
       }
-      S[j][j] = sqrt(d);
+      S[j][kNB] = sqrt(d);
     }
     __syncthreads();
-    const double inv = 1.0 / S[j][j];
-    for (int i = j + 1 + tid; i < nb; i += 256) S[i][j] *= inv;
+    if (tl < ti) S[ti][tl] /= S[tl][kNB];
     __syncthreads();
-    // trailing lower triangle of the block: S[i][l] -= S[i][j] S[l][j], j < l <= i
-    const int m = nb - j - 1;
-    for (int e = tid; e < m * m; e += 256) {
-      const int i = j + 1 + e / m, l = j + 1 + e % m;
-      if (l <= i) S[i][l] -= S[i][j] * S[l][j];
+    if (tid < kSub) S[sb + tid][sb + tid] = S[sb + tid][kNB];
+    __syncthreads();
+    const int m = kNB - sb - kSub;  // a constant in each unrolled copy
+    if (m > 0) {
+      if (tid < m) {  // row sb + 16 + tid of the block: x L_T^T = p
+        const int i = sb + kSub + tid;
+        double x[kSub];
+#pragma unroll
+        for (int j = 0; j < kSub; ++j) x[j] = S[i][sb + j];
+#pragma unroll
+        for (int j = 0; j < kSub; ++j) {
+          double t = x[j];
+#pragma unroll
+          for (int l = 0; l < j; ++l) t -= x[l] * S[sb + j][sb + l];
+          x[j] = t / S[sb + j][sb + j];
+        }
+#pragma unroll
+        for (int j = 0; j < kSub; ++j) S[i][sb + j] = x[j];
+      }
+      __syncthreads();
+      for (int e = tid; e < m * m; e += blockDim.x) {
+        const int i = sb + kSub + e / m, l = sb + kSub + e % m;
+        if (l <= i) {
+          double acc = 0.0;
+#pragma unroll
+          for (int q = 0; q < kSub; ++q) acc += S[i][sb + q] * S[l][sb + q];
+          S[i][l] -= acc;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += 256) {
-    const int i = e / nb, j = e % nb;
-    if (j <= i) A[(k + i) * lda + k + j] = S[i][j];
-  }
+  // the first failing pivot of the matrix: panels run in order, so an earlier
+  // panel's report is already in *info
+  if (report && tid == 0 && first_bad < nb) atomicCAS(info, 0, (int32_t)(k + first_bad + 1));
 }
 
-// ---------------------------------------------------------------- panel
-// A[r, k:k+nb] <- A[r, k:k+nb] L_kk^-T for r >= k + nb: forward substitution
-// x L_kk^T = a, one thread per row, L_kk in shared memory.
-__global__ void __launch_bounds__(128) chol_panel_kernel(int64_t n, double* __restrict__ A, int64_t lda, int64_t k) {
+constexpr int kPanelThreads = 256;
+
+__global__ void __launch_bounds__(kPanelThreads) chol_panel_kernel(int64_t n, double* __restrict__ A, int64_t lda,
+                                                                   int64_t k, int32_t* __restrict__ info) {
   __shared__ double L[kNB][kNB + 1];
   const int nb = (int)((n - k) < kNB ? (n - k) : kNB);
-  for (int e = threadIdx.x; e < nb * nb; e += 128) {
-    const int i = e / nb, j = e % nb;
-    L[i][j] = j <= i ? A[(k + i) * lda + k + j] : 0.0;
-  }
+  factor_diag_block(n, A, lda, k, nb, L, info, blockIdx.x == 0);
+  if (blockIdx.x == 0)
+    for (int e = threadIdx.x; e < nb * nb; e += kPanelThreads) {
+      const int i = e / nb, j = e % nb;
+      if (j <= i) A[(k + i) * lda + k + j] = L[i][j];
+    }
+  // rows below: x L_kk^T = a, forward substitution, one thread per row; the
+  // row is loaded whole first (64 independent loads in flight), and the
+  // diagonal is applied as its reciprocal (the padding column of L)
+  for (int j = threadIdx.x; j < kNB; j += kPanelThreads) L[j][kNB] = 1.0 / L[j][j];
   __syncthreads();
-  const int64_t r = k + nb + (int64_t)blockIdx.x * 128 + threadIdx.x;
+  const int64_t r = k + nb + (int64_t)blockIdx.x * kPanelThreads + threadIdx.x;
   if (r >= n) return;
   double* row = A + r * lda + k;
   double x[kNB];
 #pragma unroll
-  for (int j = 0; j < kNB; ++j) {
-    if (j < nb) {
-      double t = row[j];
+  for (int j = 0; j < kNB; ++j) x[j] = j < nb ? row[j] : 0.0;
 #pragma unroll
-      for (int l = 0; l < j; ++l) t -= x[l] * L[j][l];
-      x[j] = t / L[j][j];
-    } else {
-      x[j] = 0.0;
-    }
+  for (int j = 0; j < kNB; ++j) {
+    double t = x[j];
+#pragma unroll
+    for (int l = 0; l < j; ++l) t -= x[l] * L[j][l];
+    x[j] = t * L[j][kNB];
   }
 #pragma unroll
   for (int j = 0; j < kNB; ++j)
@@ -117,11 +163,32 @@ __global__ void __launch_bounds__(128) chol_update_kernel(int64_t n, double* __r
   const int64_t bj = t - bi * (bi + 1) / 2;
   const int64_t r0 = t0 + bi * kNB, c0 = t0 + bj * kNB;
   const int tid = threadIdx.x;
-  for (int e = tid; e < kNB * kNB; e += 128) {
-    const int i = e / kNB, j = e % kNB;
-    const int64_t ra = r0 + i, rb = c0 + i;
-    Pa[i][j] = (ra < n && j < nb) ? A[ra * lda + k + j] : 0.0;
-    Pb[i][j] = (rb < n && j < nb) ? A[rb * lda + k + j] : 0.0;
+  // 16-byte loads, all in flight before the stores (row starts are 16-byte
+  // aligned when lda and k are even; otherwise 8-byte loads)
+  if (((lda | k) & 1) == 0 && nb == kNB) {
+    double2 va[16], vb[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + q * 128, i = e >> 5, j2 = (e & 31) * 2;
+      const int64_t ra = r0 + i, rb = c0 + i;
+      va[q] = ra < n ? *reinterpret_cast<const double2*>(A + ra * lda + k + j2) : make_double2(0.0, 0.0);
+      vb[q] = rb < n ? *reinterpret_cast<const double2*>(A + rb * lda + k + j2) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int e = tid + q * 128, i = e >> 5, j2 = (e & 31) * 2;
+      Pa[i][j2] = va[q].x;
+      Pa[i][j2 + 1] = va[q].y;
+      Pb[i][j2] = vb[q].x;
+      Pb[i][j2 + 1] = vb[q].y;
+    }
+  } else {
+    for (int e = tid; e < kNB * kNB; e += 128) {
+      const int i = e >> 6, j = e & (kNB - 1);
+      const int64_t ra = r0 + i, rb = c0 + i;
+      Pa[i][j] = (ra < n && j < nb) ? A[ra * lda + k + j] : 0.0;
+      Pb[i][j] = (rb < n && j < nb) ? A[rb * lda + k + j] : 0.0;
+    }
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
@@ -164,154 +231,108 @@ __global__ void chol_zero_upper_kernel(int64_t n, double* __restrict__ A, int64_
 
 // ---------------------------------------------------------------- solves
 // L L^T x = b for one right-hand side column per CTA (b read from column c of
-// B, row stride ldb, solved in shared memory, written back). Forward:
-// per 64-row block, warp 0 solves the diagonal block (each step's x_j
-// broadcast by shuffle), then every thread updates one later row with the
-// block's columns in order. Backward: the same with L^T, block by block from
-// the end; the update of an earlier row r sums column r of the block's rows.
-__global__ void __launch_bounds__(256) chol_solve_kernel(int64_t n, const double* __restrict__ L, int64_t lda,
-                                                         double* __restrict__ B, int64_t ldb) {
-  extern __shared__ double y[];
+// B, row stride ldb, solved in shared memory, written back), left-looking by
+// 64-row blocks. Forward, block kb: the 32 warps subtract L[kb:kb+64, :kb] y
+// (a warp per row, lanes over the columns, butterfly sums), then warp 0 solves
+// the diagonal block (each step's x_j broadcast by shuffle; the block and its
+// reciprocal diagonal staged in shared memory). Backward, block kb from the
+// end: each warp sums its rows r >= kb + 64 of L[r, kb:kb+64] y_r per column
+// (lanes over the columns), the 32 warp partials are added in warp order, and
+// warp 0 solves with the block's transpose.
+constexpr int kSolveThreads = 1024;
+constexpr int kSolveWarps = kSolveThreads / 32;
+
+__global__ void __launch_bounds__(kSolveThreads) chol_solve_kernel(int64_t n, const double* __restrict__ L,
+                                                                   int64_t lda, double* __restrict__ B, int64_t ldb) {
+  // dynamic shared memory: the current diagonal block (column kNB: 1 / D[j][j]),
+  // the warp partials, then y
+  extern __shared__ double solve_smem[];
+  double (*D)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(solve_smem);
+  double (*part)[kNB + 1] = D + kNB;
+  double* y = solve_smem + (kNB + kSolveWarps) * (kNB + 1);
   const int64_t col = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int64_t i = tid; i < n; i += 256) y[i] = B[i * ldb + col];
+  for (int64_t i = tid; i < n; i += kSolveThreads) y[i] = B[i * ldb + col];
+  auto stage = [&](int64_t kb, int nb) {
+    for (int e = tid; e < nb * kNB; e += kSolveThreads) {
+      const int i = e >> 6, j = e & (kNB - 1);
+      if (j < nb) D[i][j] = L[(kb + i) * lda + kb + j];
+    }
+    __syncthreads();
+    if (tid < nb) D[tid][kNB] = 1.0 / D[tid][tid];
+  };
   __syncthreads();
   for (int64_t kb = 0; kb < n; kb += kNB) {
     const int nb = (int)((n - kb) < kNB ? (n - kb) : kNB);
+    stage(kb, nb);
+    for (int i = warp; i < nb; i += kSolveWarps) {
+      const double* lr = L + (kb + i) * lda;
+      double t = 0.0;
+#pragma unroll 8
+      for (int64_t c = lane; c < kb; c += 32) t += lr[c] * y[c];
+      t = warp_sum(t);
+      if (lane == 0) y[kb + i] -= t;
+    }
+    __syncthreads();
     if (warp == 0) {
       double v0 = lane < nb ? y[kb + lane] : 0.0, v1 = lane + 32 < nb ? y[kb + lane + 32] : 0.0;
       for (int j = 0; j < nb; ++j) {
-        const double bj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        const double xj = bj / L[(kb + j) * lda + kb + j];
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31) * D[j][kNB];
         if (lane == (j & 31)) {
           if (j < 32) v0 = xj;
           else v1 = xj;
         }
-        if (lane > j && lane < nb) v0 -= L[(kb + lane) * lda + kb + j] * xj;
-        if (lane + 32 > j && lane + 32 < nb) v1 -= L[(kb + lane + 32) * lda + kb + j] * xj;
+        if (lane > j && lane < nb) v0 -= D[lane][j] * xj;
+        if (lane + 32 > j && lane + 32 < nb) v1 -= D[lane + 32][j] * xj;
       }
       if (lane < nb) y[kb + lane] = v0;
       if (lane + 32 < nb) y[kb + lane + 32] = v1;
-    }
-    __syncthreads();
-    for (int64_t r = kb + nb + tid; r < n; r += 256) {
-      double t = y[r];
-      const double* lr = L + r * lda + kb;
-      for (int j = 0; j < nb; ++j) t -= lr[j] * y[kb + j];
-      y[r] = t;
     }
     __syncthreads();
   }
   const int64_t last = ((n - 1) / kNB) * kNB;
   for (int64_t kb = last; kb >= 0; kb -= kNB) {
     const int nb = (int)((n - kb) < kNB ? (n - kb) : kNB);
+    stage(kb, nb);
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll 4
+    for (int64_t r = kb + nb + warp; r < n; r += kSolveWarps) {
+      const double* lr = L + r * lda + kb;
+      const double yr = y[r];
+      if (lane < nb) a0 += lr[lane] * yr;
+      if (lane + 32 < nb) a1 += lr[lane + 32] * yr;
+    }
+    part[warp][lane] = a0;
+    part[warp][lane + 32] = a1;
+    __syncthreads();
+    if (tid < nb) {
+      double t = 0.0;
+      for (int w = 0; w < kSolveWarps; ++w) t += part[w][tid];
+      y[kb + tid] -= t;
+    }
+    __syncthreads();
     if (warp == 0) {
       double v0 = lane < nb ? y[kb + lane] : 0.0, v1 = lane + 32 < nb ? y[kb + lane + 32] : 0.0;
       for (int j = nb - 1; j >= 0; --j) {
-        const double bj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-        const double xj = bj / L[(kb + j) * lda + kb + j];
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31) * D[j][kNB];
         if (lane == (j & 31)) {
           if (j < 32) v0 = xj;
           else v1 = xj;
         }
-        if (lane < j) v0 -= L[(kb + j) * lda + kb + lane] * xj;
-        if (lane + 32 < j) v1 -= L[(kb + j) * lda + kb + lane + 32] * xj;
+        if (lane < j) v0 -= D[j][lane] * xj;
+        if (lane + 32 < j) v1 -= D[j][lane + 32] * xj;
       }
       if (lane < nb) y[kb + lane] = v0;
       if (lane + 32 < nb) y[kb + lane + 32] = v1;
     }
     __syncthreads();
-    for (int64_t r = tid; r < kb; r += 256) {
-      double t = y[r];
-      for (int j = 0; j < nb; ++j) t -= L[(kb + j) * lda + r] * y[kb + j];
-      y[r] = t;
-    }
-    __syncthreads();
   }
-  for (int64_t i = tid; i < n; i += 256) B[i * ldb + col] = y[i];
-}
-
-// ---------------------------------------------------------------- reduced-camera matrix
-// S = s U s + lambda I - W W^T from the one-group Schur system's slabs
-// (schur.py:380-397). Pass 1 writes the block diagonal base (zeros
-// elsewhere); pass 2 has one warp per lower block (i, j) sum W_a W_b^T over
-// the pairs (a, b) of edges of a shared eliminated variable, in list order,
-// and subtract it from block (i, j) and its mirror. W is read as stored.
-__device__ __forceinline__ int64_t slab_w(int64_t s, int k, int cap, int kw) {
-  return ((s / cap) * kw + k) * cap + (s % cap);
-}
-
-__global__ void schur_dense_base_kernel(tls_schur_args a, double* __restrict__ S) {
-  const int64_t n = (int64_t)a.nretained * a.dr;
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * n) return;
-  const int64_t r = e / n, c = e % n;
-  const int64_t i = r / a.dr, j = c / a.dr;
-  double v = 0.0;
-  if (i == j) {
-    const int rr = (int)(r % a.dr), cc = (int)(c % a.dr);
-    // scales in index order: entries (r, c) and (c, r) get the same bits
-    const int64_t lo = r < c ? r : c, hi = r < c ? c : r;
-    const double sl = a.scale ? a.scale[a.retained_offset + lo] : 1.0;
-    const double sh = a.scale ? a.scale[a.retained_offset + hi] : 1.0;
-    v = sl * a.ret_diag[i * a.dr * a.dr + rr * a.dr + cc] * sh + (rr == cc ? a.damping : 0.0);
-  }
-  S[e] = v;
-}
-
-template <typename TW>
-__global__ void __launch_bounds__(128) schur_dense_pairs_kernel(tls_schur_args a, int64_t ntargets,
-                                                                const int32_t* __restrict__ target_r,
-                                                                const int32_t* __restrict__ target_c,
-                                                                const int32_t* __restrict__ ptr,
-                                                                const int32_t* __restrict__ pa,
-                                                                const int32_t* __restrict__ pb,
-                                                                double* __restrict__ S) {
-  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (t >= ntargets) return;
-  const int dr = a.dr, de = a.de, kw = dr * de;
-  const TW* w = reinterpret_cast<const TW*>(a.w);
-  const int64_t n = (int64_t)a.nretained * dr;
-  const int64_t i = target_r[t], j = target_c[t];
-  for (int ent = lane; ent < dr * dr; ent += 32) {
-    const int r = ent / dr, c = ent % dr;
-    double acc = 0.0;
-    for (int k = ptr[t]; k < ptr[t + 1]; ++k) {
-      const int64_t sa = pa[k], sb = pb[k];
-      double v = 0.0;
-      for (int b = 0; b < de; ++b)
-        v += to_d(w[slab_w(sa, r * de + b, a.cap, kw)]) * to_d(w[slab_w(sb, c * de + b, a.cap, kw)]);
-      acc += v;
-    }
-    const int64_t row = i * dr + r, col = j * dr + c;
-    S[row * n + col] -= acc;
-    if (i != j) S[col * n + row] -= acc;
-  }
+  for (int64_t i = tid; i < n; i += kSolveThreads) B[i * ldb + col] = y[i];
 }
 
 }  // namespace tls
 
 using namespace tls;
-
-extern "C" int tls_schur_dense_matrix(const tls_schur_args* a, int64_t ntargets, const int32_t* target_r,
-                                      const int32_t* target_c, const int32_t* ptr, const int32_t* pair_a,
-                                      const int32_t* pair_b, double* S, tls_stream_t stream) {
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (!a || !S) return tls_set_error(TLS_ERR_INVALID, "dense Schur matrix: bad arguments");
-  const int64_t n = (int64_t)a->nretained * a->dr;
-  if (n > 0) schur_dense_base_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(*a, S);
-  TLS_CHECK_LAUNCH();
-  if (ntargets > 0) {
-    const unsigned grid = (unsigned)((ntargets * 32 + 127) / 128);
-    if (a->wdtype == TLS_F64)
-      schur_dense_pairs_kernel<double><<<grid, 128, 0, s>>>(*a, ntargets, target_r, target_c, ptr, pair_a, pair_b, S);
-    else
-      schur_dense_pairs_kernel<float><<<grid, 128, 0, s>>>(*a, ntargets, target_r, target_c, ptr, pair_a, pair_b, S);
-  }
-  TLS_CHECK_LAUNCH();
-  return TLS_OK;
-}
 
 extern "C" int tls_dense_cholesky(int64_t n, double* A, int64_t lda, int32_t* info, tls_stream_t stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -328,12 +349,11 @@ extern "C" int tls_dense_cholesky(int64_t n, double* A, int64_t lda, int32_t* in
       }))
     return rc;
   for (int64_t k = 0; k < n; k += kNB) {
-    chol_diag_kernel<<<1, 256, 0, s>>>(n, A, lda, k, info);
-    TLS_CHECK_LAUNCH();
     const int64_t below = n - k - kNB;
-    if (below <= 0) break;
-    chol_panel_kernel<<<(unsigned)((below + 127) / 128), 128, 0, s>>>(n, A, lda, k);
+    const int64_t panel_ctas = below > 0 ? (below + kPanelThreads - 1) / kPanelThreads : 1;
+    chol_panel_kernel<<<(unsigned)panel_ctas, kPanelThreads, 0, s>>>(n, A, lda, k, info);
     TLS_CHECK_LAUNCH();
+    if (below <= 0) break;
     const int64_t T = (below + kNB - 1) / kNB;
     chol_update_kernel<<<(unsigned)(T * (T + 1) / 2), 128, kUpdateSmem, s>>>(n, A, lda, k);
     TLS_CHECK_LAUNCH();
@@ -349,13 +369,13 @@ extern "C" int tls_dense_cholesky_solve(int64_t n, const double* L, int64_t lda,
   if (n < 0 || nrhs < 0 || lda < n || ldb < nrhs || (n > 0 && (!L || !B)))
     return tls_set_error(TLS_ERR_INVALID, "dense Cholesky solve: bad arguments");
   if (n == 0 || nrhs == 0) return TLS_OK;
-  const size_t smem = (size_t)n * sizeof(double);
-  if (smem > 227 * 1024) return tls_set_error(TLS_ERR_UNSUPPORTED, "dense Cholesky solve: n above 29,056");
+  const size_t smem = ((size_t)n + (kNB + kSolveWarps) * (kNB + 1)) * sizeof(double);
+  if (smem > 227 * 1024) return tls_set_error(TLS_ERR_UNSUPPORTED, "dense Cholesky solve: n above 22,816");
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(chol_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return tls_set_cuda_error(e);
   }
-  chol_solve_kernel<<<(unsigned)nrhs, 256, smem, s>>>(n, L, lda, B, ldb);
+  chol_solve_kernel<<<(unsigned)nrhs, kSolveThreads, smem, s>>>(n, L, lda, B, ldb);
   TLS_CHECK_LAUNCH();
   return TLS_OK;
 }
