@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--problems", type=int, default=4096,
+                    help="batched workload: solve the first N of the 4,096 problems (profiling captures)")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed solves with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-subrecords", action="store_true",
                     help="skip the compact pose-graph and batched records of the default line")
     ap.add_argument("--small", action="store_true", help="10-camera / 4,000-observation case (debug)")
@@ -191,6 +195,9 @@ def flush_l2(buf):
     buf.sum()
 
 
+PROFILE_RANGE = False  # set from --profile-range
+
+
 def time_solves(problem, init, tls, precision, steps, warmup, device, flush, opts=None):
     """Warm up, then time `steps` solves individually with CUDA events."""
     from torchls_b200 import _lib
@@ -208,10 +215,14 @@ def time_solves(problem, init, tls, precision, steps, warmup, device, flush, opt
         torch.cuda.synchronize(device)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push("timed_solve")
+        if PROFILE_RANGE:
+            torch.cuda.profiler.start()
         start.record()
         _, summ = problem.solve(**opts)
         end.record()
         torch.cuda.synchronize(device)
+        if PROFILE_RANGE:
+            torch.cuda.profiler.stop()
         torch.cuda.nvtx.range_pop()
         times.append(start.elapsed_time(end) / 1e3)
     launches = (_lib.launch_count() - launches0) // steps
@@ -619,7 +630,7 @@ def batched_measure(args, world, rank, local, steps, warmup, stride=64):
 
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    all_datas = synthetic.batched_bundle_adjustment(4096, first_seed=0)
+    all_datas = synthetic.batched_bundle_adjustment(args.problems, first_seed=0)
     obs = sum(d.num_observations for d in all_datas)
     # several GPUs: each rank solves its share of the problems (by observation
     # count); no data-path exchange, timing is the max over ranks
@@ -634,14 +645,18 @@ def batched_measure(args, world, rank, local, steps, warmup, stride=64):
     torch.cuda.synchronize(device)
     analysis_s = time.perf_counter() - t0
 
-    def batched_once(precision):
+    def batched_once(precision, profile=False):
         bp.reset()
         torch.cuda.synchronize(device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if profile:
+            torch.cuda.profiler.start()
         e0.record()
         sols, summ = bp.solve(max_iterations=20, precision=precision)
         e1.record()
         torch.cuda.synchronize(device)
+        if profile:
+            torch.cuda.profiler.stop()
         return e0.elapsed_time(e1) / 1e3, summ
 
     for _ in range(max(1, warmup)):
@@ -649,13 +664,13 @@ def batched_measure(args, world, rank, local, steps, warmup, stride=64):
     times, summ = [], None
     with ClockSampler(local) as clocks:
         for _ in range(steps):
-            t, summ = batched_once("mixed")
+            t, summ = batched_once("mixed", profile=PROFILE_RANGE)
             times.append(t)
     batched_s = dist_max(statistics.median(times), world, device)
     batched_once("native")  # untimed: the float64 tiling is tuned on the first native solve
     t64, summ64 = batched_once("native")
     t64 = dist_max(t64, world, device)
-    sample = list(range(0, 4096, stride)) if world == 1 else []
+    sample = list(range(0, len(datas), stride)) if world == 1 else []
     single, diffs = [], []
     opts = dict(linear_solver="schur_cg", eliminate="points", return_summary=True,
                 conjugate_gradient=tls.ConjugateGradientConfig(precision="mixed"),
@@ -673,7 +688,7 @@ def batched_measure(args, world, rank, local, steps, warmup, stride=64):
         torch.cuda.synchronize(device)
         single.append(e0.elapsed_time(e1) / 1e3)
         diffs.append(abs(float(summ.final_cost[j]) - s.final_cost) / max(s.final_cost, 1e-300))
-    per_problem_s = sum(single) / len(single) * 4096 if single else None
+    per_problem_s = sum(single) / len(single) * len(datas) if single else None
     barrier(world)
     reasons = {}
     for r in summ.termination:
@@ -682,10 +697,10 @@ def batched_measure(args, world, rank, local, steps, warmup, stride=64):
         "metric": BATCH_METRIC, "value": batched_s, "unit": "s", "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": batched_s * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 storage / f64 reductions", "data": "synthetic (seeded generator)",
-        "config": {"workload": "ba_batched_4096", "problems": 4096, "observations": obs,
+        "config": {"workload": f"ba_batched_{args.problems}", "problems": args.problems, "observations": obs,
                    "max_lm_iterations": 20, "parallelism": f"problems sharded x{world}"},
         "fp64_s": t64, "analysis_s": analysis_s, "one_solve_per_problem_s": per_problem_s,
-        "one_solve_per_problem_sample": (f"{len(sample)} problems (every {stride}th seed), mean x 4096"
+        "one_solve_per_problem_sample": (f"{len(sample)} problems (every {stride}th seed), mean x {len(datas)}"
                                          if single else None),
         "speedup_vs_one_solve_per_problem": per_problem_s / batched_s if single else None,
         "max_rel_cost_difference_vs_individual_solves": max(diffs) if diffs else None,
@@ -847,7 +862,9 @@ def run_cuda(args, world, rank, local):
 
 
 def main():
+    global PROFILE_RANGE
     args = parse()
+    PROFILE_RANGE = args.profile_range
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
