@@ -44,7 +44,7 @@ __device__ __forceinline__ void factor_diag_block(int64_t n, const double* __res
   }
   if (tid == 0) first_bad = kNB;
   __syncthreads();
-#pragma unroll
+#pragma unroll 1
   for (int sb = 0; sb < kNB; sb += kSub) {
     const int ti = sb + (tid >> 4), tl = sb + (tid & (kSub - 1));
     for (int j = sb; j < sb + kSub; ++j) {
@@ -67,7 +67,7 @@ __device__ __forceinline__ void factor_diag_block(int64_t n, const double* __res
     __syncthreads();
     if (tid < kSub) S[sb + tid][sb + tid] = S[sb + tid][kNB];
     __syncthreads();
-    const int m = kNB - sb - kSub;  // a constant in each unrolled copy
+    const int m = kNB - sb - kSub;
     if (m > 0) {
       if (tid < m) {  // row sb + 16 + tid of the block: x L_T^T = p
         const int i = sb + kSub + tid;
@@ -85,9 +85,9 @@ __device__ __forceinline__ void factor_diag_block(int64_t n, const double* __res
         for (int j = 0; j < kSub; ++j) S[i][sb + j] = x[j];
       }
       __syncthreads();
-      for (int e = tid; e < m * m; e += blockDim.x) {
-        const int i = sb + kSub + e / m, l = sb + kSub + e % m;
-        if (l <= i) {
+      for (int e = tid; e < kNB * kNB; e += blockDim.x) {
+        const int i = e >> 6, l = e & (kNB - 1);
+        if (l >= sb + kSub && l <= i) {
           double acc = 0.0;
 #pragma unroll
           for (int q = 0; q < kSub; ++q) acc += S[i][sb + q] * S[l][sb + q];
@@ -114,27 +114,46 @@ __global__ void __launch_bounds__(kPanelThreads) chol_panel_kernel(int64_t n, do
       const int i = e / nb, j = e % nb;
       if (j <= i) A[(k + i) * lda + k + j] = L[i][j];
     }
-  // rows below: x L_kk^T = a, forward substitution, one thread per row; the
-  // row is loaded whole first (64 independent loads in flight), and the
-  // diagonal is applied as its reciprocal (the padding column of L)
+  // rows below: x L_kk^T = a, one thread per row, in 16-column blocks (the
+  // block loops are not unrolled, so the code stays small): a block of x is
+  // the row's block minus the solved blocks times L's block, then a 16-step
+  // forward substitution with the reciprocal diagonal (the padding column of
+  // L); solved blocks go back to the row and are re-read from L1.
   for (int j = threadIdx.x; j < kNB; j += kPanelThreads) L[j][kNB] = 1.0 / L[j][j];
   __syncthreads();
   const int64_t r = k + nb + (int64_t)blockIdx.x * kPanelThreads + threadIdx.x;
   if (r >= n) return;
   double* row = A + r * lda + k;
-  double x[kNB];
+  constexpr int kB = 16;
+#pragma unroll 1
+  for (int sb = 0; sb < nb; sb += kB) {
+    double x[kB];
 #pragma unroll
-  for (int j = 0; j < kNB; ++j) x[j] = j < nb ? row[j] : 0.0;
+    for (int j = 0; j < kB; ++j) x[j] = sb + j < nb ? row[sb + j] : 0.0;
+#pragma unroll 1
+    for (int cb = 0; cb < sb; cb += kB) {
+      double y[kB];
 #pragma unroll
-  for (int j = 0; j < kNB; ++j) {
-    double t = x[j];
+      for (int l = 0; l < kB; ++l) y[l] = row[cb + l];
 #pragma unroll
-    for (int l = 0; l < j; ++l) t -= x[l] * L[j][l];
-    x[j] = t * L[j][kNB];
+      for (int j = 0; j < kB; ++j) {
+        double t = x[j];
+#pragma unroll
+        for (int l = 0; l < kB; ++l) t -= y[l] * L[(sb + j) & (kNB - 1)][cb + l];
+        x[j] = t;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kB; ++j) {
+      double t = x[j];
+#pragma unroll
+      for (int l = 0; l < j; ++l) t -= x[l] * L[(sb + j) & (kNB - 1)][sb + l];
+      x[j] = t * L[(sb + j) & (kNB - 1)][kNB];
+    }
+#pragma unroll
+    for (int j = 0; j < kB; ++j)
+      if (sb + j < nb) row[sb + j] = x[j];
   }
-#pragma unroll
-  for (int j = 0; j < kNB; ++j)
-    if (j < nb) row[j] = x[j];
 }
 
 // ---------------------------------------------------------------- trailing update
