@@ -539,22 +539,14 @@ __global__ void __launch_bounds__(256) schur_precond_warp_kernel(tls_schur_args 
     const int64_t s0 = a.crun_start[j];
     const int len = a.crun_len[j];
     for (int64_t s = s0 + lane; s < s0 + len; s += 32) {
-      const int64_t p = a.slab_e[s];
-      double se[DE];
-#pragma unroll
-      for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
-      const double* Li = a.inv_l + p * DE * DE;
-      const double* E = a.cross + s * DR * DE;
+      // the whitened block as the operator stores it (lanes read consecutive
+      // slab entries: coalesced)
+      const TW* ws = reinterpret_cast<const TW*>(a.w) + ((s / a.cap) * (DR * DE)) * a.cap + (s % a.cap);
       double wv[DR][DE];
 #pragma unroll
       for (int r = 0; r < DR; ++r)
 #pragma unroll
-        for (int c = 0; c < DE; ++c) {
-          double v = 0.0;
-#pragma unroll
-          for (int k = 0; k < DE; ++k) v += sr[r] * E[r * DE + k] * se[k] * Li[c * DE + k];
-          wv[r][c] = to_d(static_cast<TW>(v));  // the operator's (stored) precision
-        }
+        for (int c = 0; c < DE; ++c) wv[r][c] = to_d(ws[(int64_t)(r * DE + c) * a.cap]);
       int idx = 0;
 #pragma unroll
       for (int r = 0; r < DR; ++r)
@@ -1033,23 +1025,35 @@ __global__ void __launch_bounds__(128) schur_whiten_kernel(tls_schur_args a) {
   const int64_t s = s0 + threadIdx.x;
   const int64_t nslab = (int64_t)a.nchunks * a.cap;
   const int nvalid = (int)((nslab - s0) < 128 ? (nslab - s0) : 128);
-  for (int k = threadIdx.x; k < nvalid * kW; k += 128) e_s[k] = a.cross[s0 * kW + k];
+  // this thread's edge, its scales and its point's factor: loaded before the
+  // staging barrier so that every load of the block is in flight together
+  const bool live = s < nslab;
+  const int64_t i = live ? a.slab_r[s] : -1;
+  const int64_t p = i >= 0 ? a.slab_e[s] : 0;
+  double sr[DR], se[DE], Li[DE * DE];
+#pragma unroll
+  for (int k = 0; k < DR; ++k) sr[k] = (a.scale && i >= 0) ? a.scale[a.retained_offset + i * DR + k] : 1.0;
+#pragma unroll
+  for (int k = 0; k < DE; ++k) se[k] = (a.scale && i >= 0) ? a.scale[a.elim_offset + p * DE + k] : 1.0;
+#pragma unroll
+  for (int k = 0; k < DE * DE; ++k) Li[k] = i >= 0 ? a.inv_l[p * DE * DE + k] : 0.0;
+  if (nvalid == 128) {  // a full block: kW coalesced loads per thread, all in flight
+    double v[kW];
+#pragma unroll
+    for (int q = 0; q < kW; ++q) v[q] = a.cross[s0 * kW + threadIdx.x + q * 128];
+#pragma unroll
+    for (int q = 0; q < kW; ++q) e_s[threadIdx.x + q * 128] = v[q];
+  } else {
+    for (int k = threadIdx.x; k < nvalid * kW; k += 128) e_s[k] = a.cross[s0 * kW + k];
+  }
   __syncthreads();
-  if (s >= nslab) return;
+  if (!live) return;
   TW* w = reinterpret_cast<TW*>(a.w);
-  const int64_t i = a.slab_r[s];
   if (i < 0) {
 #pragma unroll
     for (int k = 0; k < kW; ++k) w[w_index<DR, DE>(s, k, a.cap)] = TW(0);
     return;
   }
-  const int64_t p = a.slab_e[s];
-  double sr[DR], se[DE];
-#pragma unroll
-  for (int k = 0; k < DR; ++k) sr[k] = a.scale ? a.scale[a.retained_offset + i * DR + k] : 1.0;
-#pragma unroll
-  for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
-  const double* Li = a.inv_l + p * DE * DE;
   const double* E = e_s + threadIdx.x * kW;
 #pragma unroll
   for (int r = 0; r < DR; ++r) {
@@ -1134,22 +1138,14 @@ __global__ void __launch_bounds__(256) schur_precond_kernel(tls_schur_args a, do
     const int64_t s0 = a.crun_start[j];
     const int len = a.crun_len[j];
     for (int64_t s = s0; s < s0 + len; ++s) {
-      const int64_t p = a.slab_e[s];
-      double se[DE];
-#pragma unroll
-      for (int k = 0; k < DE; ++k) se[k] = a.scale ? a.scale[a.elim_offset + p * DE + k] : 1.0;
-      const double* Li = a.inv_l + p * DE * DE;
-      const double* E = a.cross + s * DR * DE;
+      // the whitened block as the operator stores it (schur_whiten_kernel
+      // rounds exactly this product to TW)
+      const TW* ws = reinterpret_cast<const TW*>(a.w) + w_index<DR, DE>(s, 0, a.cap);
       double wv[DR][DE];
 #pragma unroll
       for (int r = 0; r < DR; ++r)
 #pragma unroll
-        for (int c = 0; c < DE; ++c) {
-          double v = 0.0;
-#pragma unroll
-          for (int k = 0; k < DE; ++k) v += sr[r] * E[r * DE + k] * se[k] * Li[c * DE + k];
-          wv[r][c] = to_d(static_cast<TW>(v));  // the operator's (stored) precision
-        }
+        for (int c = 0; c < DE; ++c) wv[r][c] = to_d(ws[(int64_t)(r * DE + c) * a.cap]);
       int idx = 0;
 #pragma unroll
       for (int r = 0; r < DR; ++r)
