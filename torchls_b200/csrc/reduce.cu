@@ -82,6 +82,24 @@ __global__ void __launch_bounds__(256) segment_reduce_kernel(tls_segments seg, c
   }
 }
 
+// Vector targets summed by one lane: one thread per (target, component), so
+// consecutive threads read and write consecutive addresses when consecutive
+// targets' contributions are contiguous (the Schur cross blocks: one
+// contribution per edge). Each element sums its contributions in list order,
+// exactly as the one-lane path of segment_reduce_kernel does.
+template <typename TC, typename TO>
+__global__ void __launch_bounds__(256) segment_reduce_elem_kernel(tls_segments seg, const TC* __restrict__ contrib,
+                                                                  TO* __restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int W = seg.width;
+  if (e >= (int64_t)seg.count * W) return;
+  const int64_t t = e / W;
+  const int k = (int)(e - t * W);
+  double acc = 0.0;
+  for (int j = seg.ptr[t]; j < seg.ptr[t + 1]; ++j) acc += to_d(contrib[seg.src[j] + k]);
+  out[e] = static_cast<TO>(acc);
+}
+
 template <typename TC, typename TO>
 static int launch_segments(const tls_segments* seg, const TC* c, int mode, int dim, TO* out, cudaStream_t st) {
   if (seg->count == 0) return TLS_OK;
@@ -91,6 +109,12 @@ static int launch_segments(const tls_segments* seg, const TC* c, int mode, int d
   const int block = 256;
   const int64_t grid = L > 32 ? seg->count : ((int64_t)seg->count * L + block - 1) / block;
   const int W = seg->width;
+  if (mode == 0 && L == 1 && W >= 4) {
+    const int64_t elems = (int64_t)seg->count * W;
+    segment_reduce_elem_kernel<TC, TO><<<(unsigned)((elems + block - 1) / block), block, 0, st>>>(*seg, c, out);
+    TLS_CHECK_LAUNCH();
+    return TLS_OK;
+  }
   if (W <= 4)
     segment_reduce_kernel<4, TC, TO><<<grid, block, 0, st>>>(*seg, c, mode, dim, out);
   else if (W <= 8)

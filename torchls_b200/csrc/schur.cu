@@ -1095,6 +1095,9 @@ __global__ void schur_backsub_kernel(tls_schur_args a, const TV* __restrict__ xc
 #pragma unroll
   for (int b = 0; b < DE; ++b) t[b] = a.ybuf[p * DE + b];
   const int pb = a.elim_ptr[p], pe = a.elim_ptr[p + 1];
+  // unrolled so that several edges' loads are in flight (the subtractions
+  // keep their order)
+#pragma unroll 4
   for (int j = pb; j < pe; ++j) {
     const int64_t s = a.elim_slab[j];
     const int64_t i = a.slab_r[s];
