@@ -17,6 +17,8 @@
 // reads p); the saved direction is restored if the iteration continues.
 #include <type_traits>
 
+#include <map>
+
 #include "blocks.cuh"
 #include "common.cuh"
 #include "pcg_device.cuh"
@@ -325,6 +327,74 @@ static int operator_blocks(const tls_pcg_args* a) {
   return a->schur->nretained;  // one gather block per retained variable
 }
 
+// CUDA-graph replay of the queued PCG steps: the steps are recorded on a
+// private capture stream of this thread and device, the recording updates the
+// thread's executable graph (instantiated again only when the topology
+// changes) and the graph is launched on the caller's stream. The kernels and
+// their order are exactly those of direct launches. When the caller's stream
+// is itself being captured, or recording fails (an API call that cannot be
+// captured, such as a first-use attribute setting), the steps are launched
+// directly; after repeated failures the thread stops trying. The executable
+// graphs live until the process exits.
+struct GraphSlot {
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int failures = 0;
+};
+
+template <typename F>
+static int replay_steps(F&& enqueue, cudaStream_t s) {
+  thread_local std::map<int, GraphSlot> slots;
+  int dev = 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaStreamIsCapturing(s, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return enqueue(s);
+  }
+  GraphSlot& g = slots[dev];
+  if (g.failures >= 3) return enqueue(s);
+  if (!g.cap && cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    g.cap = nullptr;
+    g.failures = 3;
+    return enqueue(s);
+  }
+  cudaGraph_t graph = nullptr;
+  int rc = TLS_OK;
+  cudaError_t e = cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = enqueue(g.cap);
+    e = cudaStreamEndCapture(g.cap, &graph);
+  }
+  if (rc != TLS_OK || e != cudaSuccess || graph == nullptr) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    ++g.failures;
+    return enqueue(s);  // the same steps, launched directly
+  }
+  if (g.exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(g.exec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+  }
+  if (!g.exec && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+    cudaGetLastError();
+    g.exec = nullptr;
+    cudaGraphDestroy(graph);
+    ++g.failures;
+    return enqueue(s);
+  }
+  cudaGraphDestroy(graph);
+  e = cudaGraphLaunch(g.exec, s);
+  if (e != cudaSuccess) return tls_set_cuda_error(e);
+  g.failures = 0;
+  return TLS_OK;
+}
+
 template <typename TV>
 static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
   PcgState* st = reinterpret_cast<PcgState*>(a->control);
@@ -361,6 +431,7 @@ static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
   }
   // multi-kernel path: at most 16 queued steps per call (the host polls between calls)
   if (steps > 16) steps = 16;
+  auto enqueue = [&](cudaStream_t s) -> int {
   return with_dim(maxdim, [&](auto dim) -> int {
     constexpr int D = decltype(dim)::value;
     for (int k = 0; k < steps; ++k) {
@@ -394,6 +465,8 @@ static int pcg_run_t(const tls_pcg_args* a, int steps, cudaStream_t s) {
     }
     return TLS_OK;
   });
+  };
+  return replay_steps(enqueue, s);
 }
 
 // ---------------------------------------------------------------- block Jacobi
