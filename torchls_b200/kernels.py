@@ -59,3 +59,25 @@ def segment_reduce(seg: L.Segments, contrib: torch.Tensor, out: torch.Tensor, mo
     L.call("tls_segment_reduce", C.byref(seg), L.ptr(contrib), L.dtype_code(contrib.dtype), mode, dim, L.ptr(out),
            L.dtype_code(out.dtype), L.stream_handle(contrib.device))
     return out
+
+
+def ordered_index_add_(out: torch.Tensor, index: torch.Tensor, source: torch.Tensor) -> torch.Tensor:
+    """``out[index[k]] += source[k]`` with each target's contributions summed
+    in ascending k by ``tls_segment_reduce`` and then added once: a fixed
+    order, so the result is the same on every run (``index_add_`` on CUDA
+    adds with atomics in arrival order). ``out`` may be a strided view."""
+    if index.numel() == 0:
+        return out
+    idx = index.to(device=out.device, dtype=torch.int64).reshape(-1)
+    width = int(source[0].numel())
+    sidx, order = torch.sort(idx, stable=True)
+    uniq, counts = torch.unique_consecutive(sidx, return_counts=True)
+    ptr = torch.zeros(uniq.numel() + 1, dtype=torch.int32, device=out.device)
+    ptr[1:] = torch.cumsum(counts, 0).to(torch.int32)
+    src = (order * width).to(torch.int32)
+    seg = L.Segments(uniq.numel(), width, 1, 0, ptr.data_ptr(), src.data_ptr())
+    values = source.reshape(-1, width).to(device=out.device, dtype=torch.float64).contiguous()
+    sums = torch.empty((uniq.numel(), width), dtype=torch.float64, device=out.device)
+    segment_reduce(seg, values, sums)
+    out[uniq] = out[uniq] + sums.view(-1, *out.shape[1:]).to(out.dtype)
+    return out

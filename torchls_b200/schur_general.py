@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .kernels import segment_reduce
+from .kernels import ordered_index_add_, segment_reduce
 from .variables import VariableLayout
 
 
@@ -311,7 +311,7 @@ class GeneralSchurLinearization:
                     if key not in out:
                         out[key] = torch.zeros((plan.layout[a].count, *cross.shape[1:]), dtype=torch.float64,
                                                device=plan.device)
-                    out[key].index_add_(0, g.variable_indices[p], cross)
+                    ordered_index_add_(out[key], g.variable_indices[p], cross)
         return out
 
     def damped(self, damping, check: bool = True):
@@ -454,8 +454,11 @@ class GeneralDampedSchurSystem:
                         cross = (g.blocks[a_].double().transpose(-1, -2) @ g.blocks[b_].double()) * mask[:, None, None]
                         ra = ea.offset + g.variable_indices[a_][:, None] * ea.dim + ar(ea.dim)
                         rb = eb.offset + g.variable_indices[b_][:, None] * eb.dim + ar(eb.dim)
-                        S.index_put_((ra[:, :, None], rb[:, None, :]), cross, accumulate=True)
-                        S.index_put_((rb[:, :, None], ra[:, None, :]), cross.transpose(-1, -2), accumulate=True)
+                        flat = S.view(-1)
+                        ordered_index_add_(flat, (ra[:, :, None] * n + rb[:, None, :]).reshape(-1),
+                                           cross.reshape(-1, 1))
+                        ordered_index_add_(flat, (rb[:, :, None] * n + ra[:, None, :]).reshape(-1),
+                                           cross.transpose(-1, -2).reshape(-1, 1))
         S += self.damping * torch.eye(n, dtype=torch.float64, device=p.device)
         # W W^T by column chunks of a dense W (rows: reduced indices, columns: eliminated tangent)
         de, ncols = p.de, p.e.count * p.de

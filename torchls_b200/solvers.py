@@ -27,7 +27,7 @@ from torch import Tensor
 from . import _lib as L
 from . import dense
 from .bounds import BoundsPlan
-from .kernels import reduce
+from .kernels import ordered_index_add_, reduce
 from .schur import DampedSchurSystem, SchurLinearization, SchurPlan
 from .sparse import BlockJacobian
 
@@ -294,8 +294,8 @@ def _joint_specs(layout, groups, jacobian: BlockJacobian, diagonal):
                     cross = (g.blocks[p].double().transpose(-1, -2) @ g.blocks[q].double()) * mask[:, None, None]
                     da, db = cross.shape[-2:]
                     rows = g.variable_indices[p]
-                    specs[bi][0][:, a : a + da, c : c + db].index_add_(0, rows, cross)
-                    specs[bi][0][:, c : c + db, a : a + da].index_add_(0, rows, cross.transpose(-1, -2))
+                    ordered_index_add_(specs[bi][0][:, a : a + da, c : c + db], rows, cross)
+                    ordered_index_add_(specs[bi][0][:, c : c + db, a : a + da], rows, cross.transpose(-1, -2))
     return [tuple(s) for s in specs]
 
 
