@@ -440,7 +440,25 @@ struct tls_schur_general_args {
   double damping;
   int32_t* bad;                 /* device: number of non-PD eliminated blocks */
   int32_t max_dim;              /* largest retained dim (<= 16) */
+  int32_t pad2_;
+  /* retained couplings with the cached retained normal matrix
+   * (cache_retained_matrix, schur.py:225-241, 303-306): base = B x + lambda x
+   * from this block-sparse B = (s J_r)^T (s J_r) (yfull is then the base
+   * workspace and `normal` may be NULL); like `normal`, a host pointer to a
+   * struct of device pointers; NULL: as above */
+  const struct tls_retained_matrix* retained;
 };
+
+/* The retained normal matrix B = (s J_r)^T (s J_r) of a general Schur system,
+ * block-sparse by retained variable: row v's blocks [row_ptr[v], row_ptr[v+1])
+ * name their column variable (ascending) and the element offset of a
+ * var_dim[v] x var_dim[col] row-major block in `values`. */
+typedef struct tls_retained_matrix {
+  const int32_t* row_ptr;       /* [nretained + 1] */
+  const int32_t* block_col;     /* [nblocks] */
+  const int64_t* block_off;     /* [nblocks] */
+  const double* values;
+} tls_retained_matrix;
 
 /* Factor eliminated blocks and whiten every edge (schur.py:263-283). */
 TLS_API int tls_schur_general_damp(const tls_schur_general_args* a, tls_stream_t stream);

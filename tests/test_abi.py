@@ -28,6 +28,7 @@ STRUCTS = {
     "tls_pcg_args": L.PcgArgs,
     "tls_schur_general_args": L.SchurGeneralArgs,
     "tls_fixed_system": L.FixedSystem,
+    "tls_retained_matrix": L.RetainedMatrix,
 }
 
 

@@ -233,3 +233,39 @@ def test_general_schur_system(tls, tag, precision):
     close(system.preconditioner()(vc), fx[f"{tag}_preconditioner"], max(tol, 1e-10), what="preconditioner")
     close(system.backsubstitute(vc), fx[f"{tag}_backsubstitute"], tol, what="backsubstitute")
     close(system.dense_matrix(), fx[f"{tag}_dense"], tol, what="dense")
+
+
+@pytest.mark.parametrize("tag", ["priors", "intr", "two"])
+def test_cached_retained_matrix(tls, tag):
+    """cache_retained_matrix (schur.py:225-241): with retained couplings the
+    base term comes from the cached block-sparse (s J_r)^T (s J_r) instead of
+    the normal operator; torchls's product to 1e-11, the matrix-free operator
+    to 1e-12 with a column scale, and the same solve as without the cache."""
+    from torchls_b200.schur import SchurLinearization, SchurPlan
+
+    f64 = torch.float64
+    builder, _ = GENERAL_SCHUR[tag]
+    fx = load("schur_general")
+    prob = builder(tls, device=DEV)
+    an = prob._ensure_analyzed()
+    plan = SchurPlan(an, "points", torch.device(DEV))
+    lin = prob.linearize(jacobian_dtype=f64, schur=plan)
+    diag = lin.jacobian.diagonal_blocks()
+    vc = torch.from_numpy(fx[f"{tag}_vc"]).to(DEV)
+
+    def system(scale, cache, damping):
+        return SchurLinearization(plan, lin, diag, scale, wdtype=f64, vec_dtype=f64,
+                                  cache_retained=cache).damped(damping)
+
+    cached = system(None, True, 1e-3)
+    assert (cached.linear.retained is not None) == bool(plan.couplings)
+    close(cached.matvec(vc), fx[f"{tag}_matvec"], 1e-11, what="matvec")
+    g = torch.Generator().manual_seed(3)
+    s = (torch.rand(an.tangent_dim, generator=g, dtype=f64) + 0.5).to(DEV)
+    close(system(s, True, 0.1).matvec(vc), system(s, False, 0.1).matvec(vc), 1e-12, what="scaled matvec")
+    opts = dict(linear_solver="schur_cg", eliminate="points", return_summary=True)
+    _, s0 = builder(tls, device=DEV).solve(**opts)
+    _, s1 = builder(tls, device=DEV).solve(conjugate_gradient=tls.ConjugateGradientConfig(cache_retained_matrix=True),
+                                           **opts)
+    assert s1.linear_iterations_history == s0.linear_iterations_history
+    close(s1.final_cost, s0.final_cost, 1e-10, what="final cost")

@@ -130,8 +130,12 @@ class SchurGeneralArgs(C.Structure):
         ("var_diag", vp), ("var_ptr", vp), ("edge_var", vp), ("edge_elim", vp), ("edge_w", vp), ("elim_ptr", vp),
         ("elim_edge", vp), ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp),
         ("w", vp), ("tbuf", vp), ("ybuf", vp), ("normal", C.POINTER(NormalArgs)), ("xfull", vp), ("yfull", vp),
-        ("damping", f64), ("bad", vp), ("max_dim", i32),
+        ("damping", f64), ("bad", vp), ("max_dim", i32), ("pad2_", i32), ("retained", vp),
     ]
+
+
+class RetainedMatrix(C.Structure):
+    _fields_ = [("row_ptr", vp), ("block_col", vp), ("block_off", vp), ("values", vp)]
 
 
 # termination codes of tls_batched_lm_update's reason array

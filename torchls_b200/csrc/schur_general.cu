@@ -151,6 +151,28 @@ __global__ void sg_elim_rhs_kernel(tls_schur_general_args a, const double* __res
 }
 
 // dst (full tangent layout) at var_full <- x (reduced layout) at var_row.
+// base = B x + lambda x from the cached retained normal matrix, written to the
+// full-vector workspace at the variable's full offset (where the normal-operator
+// path leaves its base too): one thread per (variable, component); blocks in
+// row order, columns in order.
+__global__ void sg_retained_kernel(tls_schur_general_args a, tls_retained_matrix m, const double* __restrict__ x) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t v = t / kSgMaxDim;
+  const int r = (int)(t % kSgMaxDim);
+  if (v >= a.nretained) return;
+  const int dim = a.var_dim[v];
+  if (r >= dim) return;
+  double acc = 0.0;
+  for (int k = m.row_ptr[v]; k < m.row_ptr[v + 1]; ++k) {
+    const int j = m.block_col[k];
+    const int dj = a.var_dim[j];
+    const double* B = m.values + m.block_off[k] + (int64_t)r * dj;
+    const double* xj = x + a.var_row[j];
+    for (int c = 0; c < dj; ++c) acc += B[c] * xj[c];
+  }
+  a.yfull[a.var_full[v] + r] = acc + a.damping * x[a.var_row[v] + r];
+}
+
 __global__ void sg_scatter_kernel(tls_schur_general_args a, const double* __restrict__ x, double* __restrict__ dst) {
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= a.nretained) return;
@@ -205,7 +227,7 @@ __global__ void __launch_bounds__(kSgThreads) sg_ret_kernel(tls_schur_general_ar
       if constexpr (MODE == 0) {
         const double xr = x[row];
         double base;
-        if (a.normal) {
+        if (a.normal || a.retained) {
           base = a.yfull[full];
         } else {
           const double* U = a.ret_diag + a.var_diag[v] + (int64_t)lane * dim;
@@ -361,7 +383,12 @@ int tls_schur_general_apply(const tls_schur_general_args* a, const double* x, do
   return sg_dispatch(a, maxdim, [&](auto de, auto dm, auto tw) -> int {
     constexpr int DE = decltype(de)::value, DM = decltype(dm)::value;
     using TW = decltype(tw);
-    if (a->normal) {  // retained couplings: base = the normal operator on x padded with zeros
+    if (a->retained) {  // retained couplings, cached matrix: base = B x + lambda x
+      if (!a->yfull) return tls_set_error(TLS_ERR_INVALID, "general Schur: the retained matrix needs yfull");
+      // the struct lives in host memory (like `normal`): its device pointers go by value
+      sg_retained_kernel<<<grid_of_n((int64_t)a->nretained * kSgMaxDim, 128), 128, 0, s>>>(*a, *a->retained, x);
+      TLS_CHECK_LAUNCH();
+    } else if (a->normal) {  // retained couplings: base = the normal operator on x padded with zeros
       cudaError_t e = cudaMemsetAsync(a->xfull, 0, a->full_dim * sizeof(double), s);
       if (e != cudaSuccess) return tls_set_cuda_error(e);
       if (a->nretained > 0) sg_scatter_kernel<<<grid_of_n(a->nretained, 128), 128, 0, s>>>(*a, x, a->xfull);

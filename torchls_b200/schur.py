@@ -330,7 +330,10 @@ class SchurLinearization:
             return GeneralSchurLinearization(plan, *args, **kwargs)
         return super().__new__(cls)
 
-    def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
+    def __init__(self, plan: SchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False,
+                 cache_retained=False):
+        """``cache_retained`` (cache_retained_matrix) matters only with retained
+        couplings, which one retained group without them never has."""
         self.plan = plan
         dev = plan.device
         self.layout = plan.chunks_for(wdtype)

@@ -171,6 +171,10 @@ class GeneralSchurPlan:
             edge_w=_t(cat(edge_w, np.int64), dev, torch.int64), elim_ptr=_t(elim_ptr, dev), elim_edge=_t(order, dev),
         )
         self._edge_var_np, self._edge_elim_np = edge_var_np, edge_elim_np
+        self._var_dim_np = cat(var_dim, np.int32)
+        self._plans_host = [(tuple(pl.type_indices), [i.numpy() for i in pl.indices], pl.count)
+                            for pl in problem.plans]
+        self._retained_pattern = None
         # ---- cross-block segments per retained group (fixed order: record, factor)
         self.cross_segs, self._keep = [], []
         for gi, (e0, ne, w0, d) in enumerate(self.group_edges):
@@ -189,6 +193,12 @@ class GeneralSchurPlan:
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)  # no bounded waits here: stays 0
         self.wait_cycles = 0
 
+    def retained_pattern(self) -> _RetainedPattern:
+        """The block pattern of the retained normal matrix (built on first use)."""
+        if self._retained_pattern is None:
+            self._retained_pattern = _RetainedPattern(self)
+        return self._retained_pattern
+
     # ---------------------------------------------------------------- linearization hooks
     def cross_buffer(self, device):
         return torch.empty(self.cross_size, dtype=torch.float64, device=device)
@@ -204,6 +214,104 @@ class GeneralSchurPlan:
             la.slot_cross[s] = info["slot_cross"][s] if info["width"] else -1
         la.cross_width = info["width"]
         return info["base"]
+
+
+class _RetainedPattern:
+    """Block pattern of B = (s J_r)^T (s J_r) for ``cache_retained_matrix``
+    (schur.py:171-189, 225-241): every retained variable's diagonal block and a
+    block per coupled pair (a residual with two retained slots naming
+    different variables), both orientations; blocks sorted by (row, column),
+    values row-major back to back. Per coupling record (residual batch k,
+    slots a > b) the selected factors and the value positions of their
+    contributions, factor-major as the contributions are computed."""
+
+    def __init__(self, plan: GeneralSchurPlan):
+        dims = plan._var_dim_np.astype(np.int64)
+        nret = plan.nretained
+        base, acc = {}, 0
+        for orig in plan.retained:
+            base[orig] = acc
+            acc += plan.original_layout[orig].count
+        recs = []
+        rows = [np.arange(nret, dtype=np.int64)]
+        cols = [np.arange(nret, dtype=np.int64)]
+        for k, (tis, idxs, count) in enumerate(plan._plans_host):
+            for a in range(len(tis)):
+                for b in range(a):
+                    ta, tb = tis[a], tis[b]
+                    if ta not in base or tb not in base:
+                        continue
+                    ia, ib = idxs[a].astype(np.int64), idxs[b].astype(np.int64)
+                    sel = np.flatnonzero(ia != ib) if ta == tb else np.arange(count, dtype=np.int64)
+                    if not len(sel):
+                        continue
+                    va, vb = base[ta] + ia[sel], base[tb] + ib[sel]
+                    recs.append((k, a, b, sel, va, vb))
+                    rows += [va, vb]
+                    cols += [vb, va]
+        keys = np.unique(np.concatenate(rows) * nret + np.concatenate(cols))
+        brow, bcol = keys // nret, keys % nret
+        size = dims[brow] * dims[bcol]
+        off = np.concatenate(([0], np.cumsum(size)))
+        self.nvalues = int(off[-1])
+        row_ptr = np.concatenate(([0], np.cumsum(np.bincount(brow, minlength=nret))))
+        dev = plan.device
+        self.row_ptr, self.block_col = _t(row_ptr, dev), _t(bcol, dev)
+        self.block_off = _t(off[:-1], dev, torch.int64)
+        where = lambda r, c: off[np.searchsorted(keys, r * nret + c)]  # noqa: E731
+        self.diag_off = where(np.arange(nret), np.arange(nret))
+        self.records = []
+        for k, a, b, sel, va, vb in recs:
+            tis = plan._plans_host[k][0]
+            da, db = plan.original_layout[tis[a]].dim, plan.original_layout[tis[b]].dim
+            r_, c_ = np.arange(da), np.arange(db)
+            ab = where(va, vb)[:, None, None] + r_[None, :, None] * db + c_[None, None, :]
+            ba = where(vb, va)[:, None, None] + c_[None, None, :] * da + r_[None, :, None]
+            self.records.append((k, a, b, _t(sel, dev, torch.int64), _t(ab.reshape(-1), dev, torch.int64),
+                                 _t(ba.reshape(-1), dev, torch.int64)))
+        # per retained group: its entry in the full layout, the offset of its
+        # diagonal blocks in the retained diagonal buffer, their value positions
+        self.groups, dbase = [], 0
+        for orig in plan.retained:
+            e = plan.original_layout[orig]
+            v0 = base[orig]
+            pos = self.diag_off[v0 : v0 + e.count][:, None] + np.arange(e.dim * e.dim)[None, :]
+            self.groups.append((e, dbase, _t(pos.reshape(-1), dev, torch.int64)))
+            dbase += e.count * e.dim * e.dim
+
+    def values(self, lin, ret_diag, scale):
+        """B's values for one linearization: s U s on the diagonal blocks and
+        the coupled pairs' (s J_a)^T (s J_b), each block's contributions summed
+        in a fixed order (``ordered_index_add_``)."""
+        dev = ret_diag.device
+        vals = torch.zeros(max(self.nvalues, 1), dtype=torch.float64, device=dev)
+        for e, dbase, pos in self.groups:
+            U = ret_diag[dbase : dbase + e.count * e.dim * e.dim].view(e.count, e.dim, e.dim)
+            if scale is not None:
+                sv = scale[e.offset : e.offset + e.size].view(e.count, e.dim)
+                U = U * sv[:, :, None] * sv[:, None, :]
+            vals[pos] = U.reshape(-1)
+        jac = lin.jacobian
+        st = jac.structure
+        for k, a, b, sel, ab, ba in self.records:
+            cross = _slot_block(jac, st, k, a, sel, scale).transpose(-1, -2) @ _slot_block(jac, st, k, b, sel, scale)
+            ordered_index_add_(vals, ab, cross.reshape(-1, 1))
+            ordered_index_add_(vals, ba, cross.reshape(-1, 1))
+        return vals
+
+
+def _slot_block(jac, st, k, s, sel, scale):
+    """Slot s's Jacobian blocks [n, r, d] (float64, column-scaled) of the
+    selected factors of residual batch k."""
+    R, D, N = st.rdims[k], st.D[k], st.plans[k].count
+    e = jac.layout[st.plans[k].type_indices[s]]
+    c0 = st.slot_col[k][s]
+    blk = jac.jacs[k].view(R, D, N)[:, c0 : c0 + e.dim, :][:, :, sel].permute(2, 0, 1).to(torch.float64)
+    if scale is not None:
+        col = (st.index[k][s].long()[sel][:, None] * e.dim + e.offset
+               + torch.arange(e.dim, device=blk.device)[None, :])
+        blk = blk * scale[col][:, None, :]
+    return blk
 
 
 class _JointPlan:
@@ -267,7 +375,8 @@ class GeneralSchurLinearization:
     joint preconditioner groups, the member-pair couplings of the retained
     Jacobian (schur.py:192-257), for one linearization."""
 
-    def __init__(self, plan: GeneralSchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False):
+    def __init__(self, plan: GeneralSchurPlan, lin, diagonal_raw, scale, *, wdtype, vec_dtype, dense=False,
+                 cache_retained=False):
         self.plan = plan
         dev = plan.device
         self.cross = torch.zeros(max(plan.w_size, 1), dtype=torch.float64, device=dev)
@@ -283,9 +392,15 @@ class GeneralSchurLinearization:
         self.tbuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
         self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
         self.jacobian = lin.jacobian if self.scale is None else lin.jacobian.scale_columns(self.scale)
+        self.retained = None
         if plan.couplings:
             self.xfull = torch.empty(plan.full_dim, dtype=torch.float64, device=dev)
             self.yfull = torch.empty(plan.full_dim, dtype=torch.float64, device=dev)
+            if cache_retained:  # cache_retained_matrix (schur.py:225-241): B once per linearization
+                pat = plan.retained_pattern()
+                self.retained_values = pat.values(lin, self.ret_diag, self.scale)
+                self.retained = L.RetainedMatrix(pat.row_ptr.data_ptr(), pat.block_col.data_ptr(),
+                                                 pat.block_off.data_ptr(), self.retained_values.data_ptr())
         self.joint_couplings = self._joint_couplings() if plan.joint is not None else {}
 
     def _joint_couplings(self):
@@ -325,7 +440,8 @@ class GeneralDampedSchurSystem:
 
     def __init__(self, lin: GeneralSchurLinearization, damping: float, check: bool = True):
         self.linear, self.plan, self.damping = lin, lin.plan, float(damping)
-        self._normal = lin.jacobian.normal_args(torch.float64, self.damping) if self.plan.couplings else None
+        self._normal = (lin.jacobian.normal_args(torch.float64, self.damping)
+                        if self.plan.couplings and lin.retained is None else None)
         self.args = self._args()
         L.call("tls_schur_general_damp", C.byref(self.args), self.stream)
         if check and int(self.plan.bad.item()) > 0:
@@ -347,6 +463,9 @@ class GeneralDampedSchurSystem:
         if self._normal is not None:
             a.normal = C.pointer(self._normal)
             a.xfull, a.yfull = lin.xfull.data_ptr(), lin.yfull.data_ptr()
+        if lin.retained is not None:
+            a.retained = C.addressof(lin.retained)
+            a.yfull = lin.yfull.data_ptr()
         a.damping = self.damping
         a.bad = p.bad.data_ptr()
         a.max_dim = p.max_dim

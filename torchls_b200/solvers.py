@@ -677,7 +677,8 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             linear_gradient = gradient if solve_scale is None else gradient * solve_scale
             scaled = lin.jacobian if combined is None else lin.jacobian.scale_columns(combined)
             schur_lin = SchurLinearization(schur_plan, lin, raw_diag, combined, wdtype=jdt, vec_dtype=vdt,
-                                           dense=linear_solver == "schur_dense") if is_schur else None
+                                           dense=linear_solver == "schur_dense",
+                                           cache_retained=cg.cache_retained_matrix) if is_schur else None
             joint_specs = None
             if not is_schur and cg.preconditioner is not None:
                 if cg.preconditioner_groups:
