@@ -162,6 +162,11 @@ def main(reference, only=None):
         "curve_bounds": (P.curve_bounds, dict(bounds=P.CURVE_BOUNDS)),
         "rotations_small": (P.rotations_small, dict(jacobi_scaling=True, trust_region=tls.TrustRegionConfig(
             lambda_initial=1e-3, strategy="adaptive", damping_mode="diagonal"))),
+        "rotations_small_qr": (P.rotations_small, dict(linear_solver="dense_qr", jacobi_scaling=True,
+                                                       trust_region=tls.TrustRegionConfig(
+                                                           lambda_initial=1e-3, strategy="adaptive",
+                                                           damping_mode="diagonal"))),
+        "ba_tiny_qr": (P.ba_tiny, dict(linear_solver="dense_qr")),
         "alias_weights": (P.alias_weights, dict()),
         "alias_cauchy": (lambda api, **k: P.alias_weights(api, loss=P.cauchy_loss(api)), dict()),
         "alias_softsq": (lambda api, **k: P.alias_weights(api, loss=P.soft_square_loss(api)), dict()),

@@ -569,9 +569,7 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
           jacobi_scaling: bool = False, eliminate=None, profile: bool = False, record_trials: bool = False,
           bounds=None, normal_blocks_backend: str = "auto"):
     """Optimize with LM (or GN when trust_region=None) on the GPU (solvers.py:288-696)."""
-    if linear_solver == "dense_qr":
-        raise ValueError("dense_qr is not a block-sparse inner loop; use conjugate_gradient, schur_cg or schur_dense")
-    if linear_solver not in ("conjugate_gradient", "schur_dense", "schur_cg"):
+    if linear_solver not in ("conjugate_gradient", "dense_qr", "schur_dense", "schur_cg"):
         raise ValueError("Unknown linear solver")
     if normal_blocks_backend not in ("auto", *_BACKENDS):
         raise ValueError("normal_blocks_backend must be auto, cuda, torch or warp")
@@ -678,9 +676,10 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             scaled = lin.jacobian if combined is None else lin.jacobian.scale_columns(combined)
             schur_lin = SchurLinearization(schur_plan, lin, raw_diag, combined, wdtype=jdt, vec_dtype=vdt,
                                            dense=linear_solver == "schur_dense",
-                                           cache_retained=cg.cache_retained_matrix) if is_schur else None
+                                           cache_retained=cg.cache_retained_matrix and linear_solver == "schur_cg"
+                                           ) if is_schur else None
             joint_specs = None
-            if not is_schur and cg.preconditioner is not None:
+            if linear_solver == "conjugate_gradient" and cg.preconditioner is not None:
                 if cg.preconditioner_groups:
                     sdiag = scaled.diagonal_blocks()
                     joint_specs = _joint_specs(layout, cg.preconditioner_groups, scaled, sdiag)
@@ -711,7 +710,24 @@ def solve(problem, initial_vals, *, linear_solver: str = "conjugate_gradient",
             summary.lambda_history.append(damping)
             trial = None
             try:
-                if is_schur:
+                if linear_solver == "dense_qr":
+                    # the damped least-squares step [J; sqrt(lambda) I] delta = [-r; 0]
+                    # (solvers.py:504-510, a QR there): the normal equations factored by the
+                    # tensor-core Cholesky, then one correction whose residual goes through J
+                    # itself (Bjorck's corrected semi-normal equations)
+                    with _region("linear_solve", profile):
+                        jd = scaled.to_dense().to(torch.float64)
+                        r0 = lin.residual.to(torch.float64)
+                        nrm = jd.T @ jd
+                        nrm.diagonal().add_(damping)
+                        fac, info = dense.cholesky_ex(nrm)
+                        if int(info) > 0:
+                            raise torch.linalg.LinAlgError("damped normal matrix is not positive definite")
+                        delta = dense.cholesky_solve(-(jd.T @ r0), fac)
+                        corr = jd.T @ (-r0 - jd @ delta) - damping * delta
+                        delta = delta + dense.cholesky_solve(corr, fac)
+                        usable = _finite(delta)
+                elif is_schur:
                     with _region("prepare_schur", profile):
                         # schur_cg reads the non-positive-definite counts with the PCG control block
                         system = schur_lin.damped(damping, check=linear_solver == "schur_dense")

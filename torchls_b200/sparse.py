@@ -201,17 +201,25 @@ class BlockJacobian:
         return self._groups
 
     def to_dense(self) -> Tensor:
-        """Dense copy for diagnostics (sparse.py:123-143); the solver never calls it."""
-        dense = torch.zeros(self.shape, dtype=self.dtype, device=self.device)
+        """Dense copy (sparse.py:123-143; the dense_qr solver's matrix). Slots
+        of one factor that name the same variable add their blocks, in slot
+        order per element (``ordered_index_add_``: the same sums every run)."""
+        from .kernels import ordered_index_add_
+
+        dense = torch.zeros(self.shape, dtype=torch.float64, device=self.device)
+        flat = dense.view(-1)
+        ncols = self.shape[1]
         offset = 0
         for g in self.groups:
             n, r, _ = g.blocks[0].shape
             rows = torch.arange(n * r, device=self.device).reshape(n, r, 1) + offset
+            idx, val = [], []
             for b, col in zip(g.blocks, g.columns):
-                dense.index_put_((rows.expand_as(b).reshape(-1), col[:, None, :].expand_as(b).reshape(-1)),
-                                 b.reshape(-1), accumulate=True)
+                idx.append((rows * ncols + col[:, None, :]).reshape(-1))
+                val.append(b.reshape(-1).to(torch.float64))
+            ordered_index_add_(flat, torch.cat(idx), torch.cat(val).reshape(-1, 1))
             offset += n * r
-        return dense
+        return dense.to(self.dtype)
 
 
 class _ForeignPlan(NamedTuple):
