@@ -125,77 +125,89 @@ __global__ void __launch_bounds__(128) batched_dense_pairs_kernel(tls_schur_args
 // keeps all DR x DR partial sums in registers; the 32 lane partials of every
 // entry are then added in lane order through shared memory. Fixed order:
 // deterministic (the order differs from the list order of the generic kernel).
-template <int DR, int DE, typename TW, typename TS>
-__global__ void __launch_bounds__(128) batched_dense_lanes_kernel(tls_schur_args a, tls_batched_systems b,
+template <int DR, int DE, typename TW, typename TS, int H>
+__global__ void __launch_bounds__(128, H == 2 ? 6 : 1) batched_dense_lanes_kernel(tls_schur_args a,
+                                                                                  tls_batched_systems b,
                                                                   int64_t ntargets,
                                                                   const int32_t* __restrict__ target_r,
                                                                   const int32_t* __restrict__ target_c,
                                                                   const int32_t* __restrict__ ptr,
                                                                   const int32_t* __restrict__ pa,
                                                                   const int32_t* __restrict__ pb) {
-  constexpr int NE = DR * DR, KW = DR * DE;
-  __shared__ double red[4][32][NE + 1];
+  // rows in H parts (one pass over the pairs each, W re-read from L2): with
+  // H = 2 half the sums live in registers at a time, so more warps fit an SM
+  // (many blocks of few pairs: the batched problems); H = 1 reads W once
+  // (few blocks of many pairs: one problem). Every entry's products and sums
+  // run in the same order either way.
+  static_assert(DR % H == 0, "rows split evenly");
+  constexpr int RH = DR / H, NEH = RH * DR;
+  __shared__ double red[4][32][NEH + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t t = (int64_t)blockIdx.x * 4 + warp;
   if (t >= ntargets) return;
   const TW* w = reinterpret_cast<const TW*>(a.w);
-  double acc[NE];
-#pragma unroll
-  for (int e = 0; e < NE; ++e) acc[e] = 0.0;
   const int k0 = ptr[t], k1 = ptr[t + 1];
-  for (int k = k0 + lane; k < k1; k += 32) {
-    const int64_t sa = pa[k], sb = pb[k];
-    const int64_t ba = (sa / a.cap) * KW * a.cap + (sa % a.cap), bb = (sb / a.cap) * KW * a.cap + (sb % a.cap);
-    double wa[KW];
-#pragma unroll
-    for (int m = 0; m < KW; ++m) wa[m] = to_d(w[ba + (int64_t)m * a.cap]);
-#pragma unroll
-    for (int c = 0; c < DR; ++c) {
-      double wc[DE];
-#pragma unroll
-      for (int q = 0; q < DE; ++q) wc[q] = to_d(w[bb + (int64_t)(c * DE + q) * a.cap]);
-#pragma unroll
-      for (int r = 0; r < DR; ++r) {
-        double v = 0.0;
-#pragma unroll
-        for (int q = 0; q < DE; ++q) v += wa[r * DE + q] * wc[q];
-        acc[r * DR + c] += v;
-      }
-    }
-  }
-#pragma unroll
-  for (int e = 0; e < NE; ++e) red[warp][lane][e] = acc[e];
-  __syncwarp();
   const int64_t i = target_r[t], j = target_c[t];
   const ProblemView pv = problem_of(b, i, DR);
   const int64_t n = pv.n, li = i - pv.first, lj = j - pv.first;
   TS* S = reinterpret_cast<TS*>(b.S) + pv.off;
-  for (int e = lane; e < NE; e += 32) {
-    double sum = 0.0;
-    for (int l = 0; l < 32; ++l) sum += red[warp][l][e];
-    const int r = e / DR, c = e % DR;
-    const double v = (i == j ? base_entry(a, i, r, c) : 0.0) - sum;
-    S[(li * DR + r) * n + lj * DR + c] = static_cast<TS>(v);
-    if (i != j)
-      S[(lj * DR + c) * n + li * DR + r] = static_cast<TS>(v);
-    else if (b.diag)
-      b.diag[(i * DR + r) * DR + c] = v;
+#pragma unroll 1
+  for (int h = 0; h < H; ++h) {
+    double acc[NEH];
+#pragma unroll
+    for (int e = 0; e < NEH; ++e) acc[e] = 0.0;
+    for (int k = k0 + lane; k < k1; k += 32) {
+      const int64_t sa = pa[k], sb = pb[k];
+      const int64_t ba = (sa / a.cap) * DR * DE * a.cap + (sa % a.cap),
+                    bb = (sb / a.cap) * DR * DE * a.cap + (sb % a.cap);
+      double wa[RH * DE];
+#pragma unroll
+      for (int m = 0; m < RH * DE; ++m) wa[m] = to_d(w[ba + (int64_t)(h * RH * DE + m) * a.cap]);
+#pragma unroll
+      for (int c = 0; c < DR; ++c) {
+        double wc[DE];
+#pragma unroll
+        for (int q = 0; q < DE; ++q) wc[q] = to_d(w[bb + (int64_t)(c * DE + q) * a.cap]);
+#pragma unroll
+        for (int r = 0; r < RH; ++r) {
+          double v = 0.0;
+#pragma unroll
+          for (int q = 0; q < DE; ++q) v += wa[r * DE + q] * wc[q];
+          acc[r * DR + c] += v;
+        }
+      }
+    }
+    __syncwarp();  // the previous half's sums have been read
+#pragma unroll
+    for (int e = 0; e < NEH; ++e) red[warp][lane][e] = acc[e];
+    __syncwarp();
+    for (int e = lane; e < NEH; e += 32) {
+      double sum = 0.0;
+      for (int l = 0; l < 32; ++l) sum += red[warp][l][e];
+      const int r = h * RH + e / DR, c = e % DR;
+      const double v = (i == j ? base_entry(a, i, r, c) : 0.0) - sum;
+      S[(li * DR + r) * n + lj * DR + c] = static_cast<TS>(v);
+      if (i != j)
+        S[(lj * DR + c) * n + li * DR + r] = static_cast<TS>(v);
+      else if (b.diag)
+        b.diag[(i * DR + r) * DR + c] = v;
+    }
   }
 }
 
-template <int DR, int DE>
+template <int DR, int DE, int H>
 void launch_lanes(const tls_schur_args& a, const tls_batched_systems& b, int64_t ntargets, const int32_t* tr,
                   const int32_t* tc, const int32_t* ptr, const int32_t* pa, const int32_t* pb, cudaStream_t s) {
   const unsigned grid = (unsigned)((ntargets + 3) / 4);
   const bool w64 = a.wdtype == TLS_F64, s64 = b.sdtype == TLS_F64;
   if (w64 && s64)
-    batched_dense_lanes_kernel<DR, DE, double, double><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
+    batched_dense_lanes_kernel<DR, DE, double, double, H><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
   else if (w64)
-    batched_dense_lanes_kernel<DR, DE, double, float><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
+    batched_dense_lanes_kernel<DR, DE, double, float, H><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
   else if (s64)
-    batched_dense_lanes_kernel<DR, DE, float, double><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
+    batched_dense_lanes_kernel<DR, DE, float, double, H><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
   else
-    batched_dense_lanes_kernel<DR, DE, float, float><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
+    batched_dense_lanes_kernel<DR, DE, float, float, H><<<grid, 128, 0, s>>>(a, b, ntargets, tr, tc, ptr, pa, pb);
 }
 
 // ---------------------------------------------------------------- PCG
@@ -532,10 +544,14 @@ int assemble(const tls_schur_args* a, const tls_batched_systems* b, int64_t ntar
   TLS_CHECK_LAUNCH();
   const bool lanes = (a->dr == 6 || a->dr == 3) && a->de == 3;
   if (ntargets > 0 && lanes) {
-    if (a->dr == 6)
-      launch_lanes<6, 3>(*a, *b, ntargets, target_r, target_c, ptr, pair_a, pair_b, s);
+    // batched problems (many blocks of few shared points): rows in two halves
+    const bool halves = b->ret_problem != nullptr;
+    if (a->dr == 6 && halves)
+      launch_lanes<6, 3, 2>(*a, *b, ntargets, target_r, target_c, ptr, pair_a, pair_b, s);
+    else if (a->dr == 6)
+      launch_lanes<6, 3, 1>(*a, *b, ntargets, target_r, target_c, ptr, pair_a, pair_b, s);
     else
-      launch_lanes<3, 3>(*a, *b, ntargets, target_r, target_c, ptr, pair_a, pair_b, s);
+      launch_lanes<3, 3, 1>(*a, *b, ntargets, target_r, target_c, ptr, pair_a, pair_b, s);
   } else if (ntargets > 0) {
     const unsigned grid = (unsigned)((ntargets * 32 + 127) / 128);
     const bool w64 = a->wdtype == TLS_F64, s64 = b->sdtype == TLS_F64;
