@@ -34,6 +34,9 @@
 namespace tls {
 
 constexpr int kChunkThreads = 256;
+// Largest dynamic shared memory of the vector-CTA kernel: two CTAs (with
+// their static shared memory and the per-CTA reservation) still fit an SM.
+constexpr int64_t kVectorSmemMax = 110 * 1024;
 constexpr int kMetaHead = 4;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -375,29 +378,57 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
 // the writers release them through a GPU-scope fence and an atomic before the
 // grid barrier, and this CTA acquires them (a fence after the barrier wait,
 // then a block barrier) before it reads.
-template <int DR, int MODE, typename TV, typename TP, bool COH>
-__device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* __restrict__ x,
-                                             const double* __restrict__ b, TV* __restrict__ out, int64_t i,
-                                             double (*sm)[DR], double* ux) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const TP* part = reinterpret_cast<const TP*>(a.run_partial);
+// What gather_one needs before the run partials: retained variable i's run
+// range and (MODE 0, threads < DR*DR) its term of s U s x. None of it depends
+// on this step's partials, so a persistent kernel loads it ahead of the
+// barrier that precedes the gather.
+struct GatherPrep {
+  int rb, re;
+  double ux;
+};
+
+template <int DR, int MODE, typename TV>
+__device__ __forceinline__ GatherPrep gather_prep(const tls_schur_args& a, const TV* __restrict__ x, int64_t i) {
+  const int tid = threadIdx.x;
+  GatherPrep g;
+  g.rb = __ldg(a.rrun_ptr + i);
+  g.re = __ldg(a.rrun_ptr + i + 1);
+  g.ux = 0.0;
   if constexpr (MODE == 0) {
     if (tid < DR * DR) {
       const int l = tid % DR;
       const double sl = a.scale ? a.scale[a.retained_offset + i * DR + l] : 1.0;
       const double xl = to_d(x[i * DR + l]);
-      ux[tid] = a.ret_diag[i * DR * DR + tid] * (sl * xl);
+      g.ux = a.ret_diag[i * DR * DR + tid] * (sl * xl);
     }
+  }
+  return g;
+}
+
+// Run partials each thread keeps in flight per round of gather_one (256
+// threads: 1,280 runs per round).
+constexpr int kGatherInFlight = 5;
+
+template <int DR, int MODE, typename TV, typename TP, bool COH>
+__device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* __restrict__ x,
+                                             const double* __restrict__ b, TV* __restrict__ out, int64_t i,
+                                             double (*sm)[DR], double* ux, const GatherPrep& g) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const TP* part = reinterpret_cast<const TP*>(a.run_partial);
+  if constexpr (MODE == 0) {
+    if (tid < DR * DR) ux[tid] = g.ux;
   }
   double acc[DR];
 #pragma unroll
   for (int k = 0; k < DR; ++k) acc[k] = 0.0;
-  const int rb = __ldg(a.rrun_ptr + i), re = __ldg(a.rrun_ptr + i + 1);
-  // four runs per thread in flight per round; fixed order j, j+256, j+512, j+768
-  for (int j0 = rb + tid; j0 < re; j0 += 1024) {
-    TP v[4][DR];
+  const int rb = g.rb, re = g.re;
+  // kGatherInFlight runs per thread in flight per round; thread t sums runs
+  // t, t + 256, t + 512, ... in that order whatever the round size
+  constexpr int F = kGatherInFlight;
+  for (int j0 = rb + tid; j0 < re; j0 += F * 256) {
+    TP v[F][DR];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < F; ++q) {
       const int j = j0 + q * 256;
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
@@ -406,7 +437,7 @@ __device__ __forceinline__ double gather_one(const tls_schur_args& a, const TV* 
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < F; ++q)
 #pragma unroll
       for (int k = 0; k < DR; ++k) acc[k] += static_cast<double>(v[q][k]);
   }
@@ -452,7 +483,8 @@ __global__ void __launch_bounds__(256) schur_gather_kernel(tls_schur_args a, con
   __shared__ double sm[8][DR];
   __shared__ double ux[DR * DR];
   __shared__ double smd[8];
-  const double dot = gather_one<DR, MODE, TV, TP, false>(a, x, b, out, blockIdx.x, sm, ux);
+  const GatherPrep g = gather_prep<DR, MODE, TV>(a, x, blockIdx.x);
+  const double dot = gather_one<DR, MODE, TV, TP, false>(a, x, b, out, blockIdx.x, sm, ux, g);
   if constexpr (MODE == 0) {
     if (threadIdx.x == 0 && dot_partials) dot_partials[blockIdx.x] = dot;
     if (pst) pcg_operator_epilogue<256>(pst, dot_partials, gridDim.x, smd);
@@ -691,7 +723,8 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
     if (!grid_barrier(st, a.err, lim, [] {})) break;
     // ---- B: gather per retained variable
     for (int64_t i = blockIdx.x; i < a.nretained; i += gridDim.x) {
-      const double dot = gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
+      const double dot =
+          gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux, gather_prep<DR, 0>(a, q.p, i));
       if (tid == 0) q.dots[i] = dot;
     }
     // ---- C (the last CTA through the barrier): curvature and alpha, update,
@@ -742,9 +775,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
 }
 
 // Variant for small reduced systems: the LAST CTA is a "vector CTA" that
-// keeps x, r, z, p, psave and Ap of the PCG in its shared memory (where the
-// other CTAs keep chunk slabs) and runs the whole vector phase; the other
-// CTAs stream the chunks and gather. Per step:
+// keeps x, r, z, p and Ap of the PCG in its shared memory (where the other
+// CTAs keep chunk slabs), with the preconditioner factors and block columns
+// when one thread per block suffices, and runs the whole vector phase; the
+// other CTAs stream the chunks and gather. Per step:
 //   A  chunk CTAs: chunk partials of A p            -- barrier over chunk CTAs --
 //   B  chunk CTAs: gather Ap and x.Ap partials, then arrive at the vector CTA
 //   C  vector CTA (after every arrival): curvature and alpha, update,
@@ -752,6 +786,132 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
 //      the control block, then releases the chunk CTAs.
 // The arithmetic (and its order) is that of schur_pcg_kernel. Every wait is
 // bounded; on timeout the kernel flags a.err and every CTA leaves.
+// The vector CTA's per-block work: thread b owns preconditioner block b. Its
+// columns (bcol[k * kChunkThreads + b], -1 past the block's size) and its
+// packed factor (fac[k * kChunkThreads + b], the diagonal entries replaced by
+// their reciprocals) sit in shared memory from the start of the solve, so a
+// step reads no kernel parameters, divides nothing and keeps few values live.
+// The vector CTA runs this code once per step after a long wait during which
+// its SM runs the chunk code, so its instructions are fetched cold: it is kept
+// short. The arithmetic and its order are pcg_update_block's.
+template <int D>
+__device__ __forceinline__ void vc_update_block(int b, int mode, double alpha, const double* __restrict__ rhs,
+                                                double* x, double* r, double* z, const double* p, double* ap,
+                                                double* ztrue, const double* fac, const int* bcol, bool solve,
+                                                double& a0, double& a1, double& a2) {
+  int cols[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) cols[k] = bcol[k * kChunkThreads + b];
+  double rb[D];
+  if (mode == M_ITER) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      rb[k] = 0.0;
+      if (cols[k] >= 0) {
+        const int c = cols[k];
+        x[c] = x[c] + alpha * p[c];
+        const double rn = r[c] - alpha * ap[c];
+        r[c] = rn;
+        rb[k] = rn;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      rb[k] = 0.0;
+      if (cols[k] >= 0) {
+        const int c = cols[k];
+        const double t = rhs[c] - ap[c];
+        const double rv = r[c];
+        ap[c] = t;
+        rb[k] = t;
+        a0 += t * t;
+        const double dr = t - rv;
+        a1 += dr * dr;
+      }
+    }
+  }
+  if (mode == M_FINAL) return;
+  double zb[D];
+  if (!solve) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) zb[k] = rb[k];
+  } else {
+    auto L = [&](int row, int col) -> double { return fac[(row * (row + 1) / 2 + col) * kChunkThreads + b]; };
+    double inv[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) inv[k] = (cols[k] >= 0) ? L(k, k) : 0.0;
+    double y[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      double t = rb[k];
+#pragma unroll
+      for (int m = 0; m < k; ++m) t -= (cols[k] >= 0) ? L(k, m) * y[m] : 0.0;
+      y[k] = (cols[k] >= 0) ? t * inv[k] : 0.0;
+    }
+#pragma unroll
+    for (int k = D - 1; k >= 0; --k) {
+      double t = y[k];
+#pragma unroll
+      for (int m = k + 1; m < D; ++m) t -= (cols[m] >= 0) ? L(m, k) * zb[m] : 0.0;
+      zb[k] = (cols[k] >= 0) ? t * inv[k] : 0.0;
+    }
+  }
+  double* zdst = (mode == M_ITER) ? z : ztrue;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    if (cols[k] >= 0) {
+      zdst[cols[k]] = zb[k];
+      if (mode == M_ITER) {
+        a0 += rb[k] * rb[k];
+        a1 += rb[k] * zb[k];
+      } else {
+        a2 += rb[k] * zb[k];
+      }
+    }
+  }
+}
+
+// pcg_direction_elems over block b's columns, each new p also stored to
+// global memory (`pg`, which the chunk CTAs read); one loop per action.
+template <int D>
+__device__ __forceinline__ void vc_direction_block(int b, int action, double beta, bool to_final, const double* x,
+                                                   double* r, const double* z, double* p, double* psave,
+                                                   const double* ap, const double* ztrue, const int* bcol,
+                                                   double* pg) {
+  int cols[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) cols[k] = bcol[k * kChunkThreads + b];
+  auto put = [&](int i, double pn) {
+    if (to_final) pn = x[i];
+    p[i] = pn;
+    pg[i] = pn;
+  };
+  if (action == A_DIR) {
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (cols[k] >= 0) put(cols[k], z[cols[k]] + beta * p[cols[k]]);
+  } else if (action == A_RESTORE_DIR) {
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (cols[k] >= 0) put(cols[k], z[cols[k]] + beta * psave[cols[k]]);
+  } else if (action == A_RESTART) {
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (cols[k] >= 0) {
+        r[cols[k]] = ap[cols[k]];
+        put(cols[k], ztrue[cols[k]]);
+      }
+  } else if (action == A_SWAP_TO_X) {
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (cols[k] >= 0) {
+        psave[cols[k]] = p[cols[k]];
+        put(cols[k], x[cols[k]]);
+      }
+  }
+}
+
 template <int DR, int DE, int CAP, typename TW, int D>
 __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schur_args a, PcgLoop q) {
   using TA = double;
@@ -774,8 +934,49 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     double* r = x + n;
     double* z = r + n;
     double* p = z + n;
-    double* psave = p + n;
-    double* ap = psave + n;
+    double* ap = p + n;
+    double* psave = q.psave;  // read at residual checks only: global memory
+    // one preconditioner block per thread when they fit: its factor (fixed
+    // during the solve) is held in shared memory, column-major over threads
+    constexpr int LD = D * (D + 1) / 2;
+    uint32_t dyn = 0;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    const bool one_block =
+        q.nb <= kChunkThreads && n * 5 * 8 + kChunkThreads * (LD * 8 + D * 4) <= (int64_t)dyn;
+    double* fac = ap + n;                                       // [LD][kChunkThreads] when one_block
+    int* bcol = reinterpret_cast<int*>(fac + LD * kChunkThreads);  // [D][kChunkThreads] when one_block
+    bool have_f = false;
+    int bdim = 0;
+    if (one_block) {
+      if (tid < q.nb) {
+        double l[LD];
+        have_f = pcg_prefetch_factor<D>(q.bs, tid, M_ITER, l);
+        if (have_f) {
+#pragma unroll
+          for (int k = 0; k < LD; ++k) fac[k * kChunkThreads + tid] = l[k];
+#pragma unroll
+          for (int k = 0; k < D; ++k) fac[(k * (k + 3) / 2) * kChunkThreads + tid] = 1.0 / l[k * (k + 3) / 2];
+        }
+        const int gi = find_group(q.bs, tid);
+        const tls_block_group& g = q.bs.g[gi];
+        int64_t cols[D];
+        block_cols<D>(g, tid - q.bs.block_begin[gi], cols);
+        bdim = g.dim;
+#pragma unroll
+        for (int k = 0; k < D; ++k) bcol[k * kChunkThreads + tid] = k < bdim ? (int)cols[k] : -1;
+      } else {
+#pragma unroll
+        for (int k = 0; k < D; ++k) bcol[k * kChunkThreads + tid] = -1;
+      }
+    }
+    // the direction runs per block when the (disjoint) blocks cover every column
+    __shared__ int s_block_dir;
+    {
+      const double cover = block_sum<kChunkThreads>((double)bdim, smd);
+      if (tid == 0) s_block_dir = one_block && cover == (double)n;
+      __syncthreads();
+    }
+    const bool block_dir = s_block_dir != 0;
     // The control block lives in this CTA's shared memory during the solve;
     // status and mode are published to global memory every step (the chunk
     // CTAs read them), the rest when the loop ends.
@@ -786,22 +987,15 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       r[i] = q.r[i];
       z[i] = q.z[i];
       p[i] = q.p[i];
-      psave[i] = q.psave[i];
     }
     __syncthreads();
-    // one preconditioner block per thread when they fit: its factor is loaded
-    // while the chunk CTAs still stream, ahead of the update
-    const bool one_block = q.nb <= kChunkThreads;
-    constexpr int LD = D * (D + 1) / 2;
     for (int step = 0; step < q.steps; ++step) {
       if (tid == 0) s_go = sst.pub.status == TLS_PCG_ACTIVE && sst.pub.mode != M_DONE;
       __syncthreads();
       if (!s_go) break;
       const int mode = sst.pub.mode;
-      double lpre[LD];
-      bool have = false;
-      if (one_block && tid < q.nb) have = pcg_prefetch_factor<D>(q.bs, tid, mode, lpre);
       // wait until every chunk CTA has gathered its variables
+      uint32_t gen_now = 0;  // thread 0: the barrier generation this step releases
       if (tid == 0) {
         s_ok = 1;
         volatile uint32_t* cnt = &st->bar_count2;
@@ -815,15 +1009,30 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
           }
         }
         __threadfence();
+        // stable until this CTA's release (every chunk CTA has passed this
+        // step's chunk barrier); read now, used at the release
+        gen_now = *reinterpret_cast<volatile uint32_t*>(&st->bar_gen);
       }
       __syncthreads();
       if (!s_ok) break;
       // Ap into shared memory, and the curvature p.Ap in the same pass
+      // (eight loads per thread in flight; the sum runs in element order)
       double part = 0.0;
-      for (int64_t i = tid; i < n; i += kChunkThreads) {
-        const double v = __ldcg(q.ap + i);
-        ap[i] = v;
-        part += p[i] * v;
+      for (int64_t i0 = tid; i0 < n; i0 += 8 * kChunkThreads) {
+        double v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const int64_t i = i0 + m * kChunkThreads;
+          v[m] = i < n ? __ldcg(q.ap + i) : 0.0;
+        }
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const int64_t i = i0 + m * kChunkThreads;
+          if (i < n) {
+            ap[i] = v[m];
+            part += p[i] * v[m];
+          }
+        }
       }
       const double curv = block_sum<kChunkThreads>(part, smd);
       tls_pcg_control& c = sst.pub;
@@ -845,8 +1054,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       if (work) {
         if (one_block) {
           if (tid < q.nb)
-            pcg_update_block<D, double, false>(q.bs, tid, mode, alpha, q.rhs, x, r, z, p, ap, q.ztrue, lpre, have,
-                                               a0, a1, a2);
+            vc_update_block<D>(tid, mode, alpha, q.rhs, x, r, z, p, ap, q.ztrue, fac, bcol, have_f, a0, a1, a2);
         } else {
           pcg_update_blocks<D, double, false>(q.bs, q.nb, tid, kChunkThreads, mode, alpha, q.rhs, x, r, z, p, ap,
                                               q.ztrue, a0, a1, a2);
@@ -866,16 +1074,22 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
         st->pub.mode = sst.pub.mode;
       }
       __syncthreads();
-      if (s_action != A_NONE)
-        pcg_direction_elems<double, false>(n, tid, kChunkThreads, s_action, s_beta, s_tofinal != 0, x, r, z, p,
-                                           psave, ap, q.ztrue);
-      __syncthreads();
-      for (int64_t i = tid; i < n; i += kChunkThreads) q.p[i] = p[i];  // the operator reads p
-      __syncthreads();
+      if (block_dir) {
+        if (s_action != A_NONE)
+          vc_direction_block<D>(tid, s_action, s_beta, s_tofinal != 0, x, r, z, p, psave, ap, q.ztrue, bcol, q.p);
+        __syncthreads();
+      } else {
+        if (s_action != A_NONE)
+          pcg_direction_elems<double, false>(n, tid, kChunkThreads, s_action, s_beta, s_tofinal != 0, x, r, z, p,
+                                             psave, ap, q.ztrue);
+        __syncthreads();
+        for (int64_t i = tid; i < n; i += kChunkThreads) q.p[i] = p[i];  // the operator reads p
+        __syncthreads();
+      }
       if (tid == 0) {
         st->bar_count2 = 0;
         __threadfence();
-        atomicExch(&st->bar_gen, st->bar_gen + 1u);
+        atomicExch(&st->bar_gen, gen_now + 1u);
       }
     }
     __syncthreads();
@@ -893,7 +1107,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       q.r[i] = r[i];
       q.z[i] = z[i];
       q.p[i] = p[i];
-      q.psave[i] = psave[i];
     }
     return;
   }
@@ -943,6 +1156,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
       chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
     }
     if (failed) break;
+    // this CTA's first retained variable: its run range and diagonal term load
+    // while the barrier waits
+    GatherPrep g0{0, 0, 0.0};
+    if ((int64_t)blockIdx.x < a.nretained) g0 = gather_prep<DR, 0>(a, q.p, blockIdx.x);
     // ---- barrier over the chunk CTAs
     __syncthreads();
     if (tid == 0) {
@@ -971,7 +1188,9 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_ok) break;
     // ---- B (the vector CTA forms p.Ap itself)
-    for (int64_t i = blockIdx.x; i < a.nretained; i += G) gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux);
+    for (int64_t i = blockIdx.x; i < a.nretained; i += G)
+      gather_one<DR, 0, double, double, true>(a, q.p, nullptr, q.ap, i, sm, ux,
+                                              i == blockIdx.x ? g0 : gather_prep<DR, 0>(a, q.p, i));
     // ---- arrive at the vector CTA, wait for its release
     __syncthreads();
     if (tid == 0) {
@@ -1278,21 +1497,35 @@ struct SchurOps {
     if (a.meta_ints != S::kMetaInts) return tls_set_error(TLS_ERR_INVALID, "metadata slab size mismatch");
     if ((reinterpret_cast<uintptr_t>(a.w) & 15) || (reinterpret_cast<uintptr_t>(a.meta) & 15))
       return tls_set_error(TLS_ERR_INVALID, "W and metadata slabs must be 16-byte aligned");
-    // six float64 vectors of the reduced system in one CTA's shared memory?
-    if (q.n * 6 * (int64_t)sizeof(double) <= S::kBaseSmem) return pcg_launch<TW, CAP, D, true>(a, q, s);
-    return pcg_launch<TW, CAP, D, false>(a, q, s);
+    // Five float64 vectors of the reduced system in one CTA's shared memory,
+    // and with them (one block per thread) the preconditioner factors and
+    // block columns when they fit too; the kernel reads which from its
+    // dynamic shared-memory size.
+    constexpr int LD = D * (D + 1) / 2;
+    const int64_t vec = q.n * 5 * (int64_t)sizeof(double);
+    const int64_t blocks = (int64_t)kChunkThreads * (LD * (int64_t)sizeof(double) + D * (int64_t)sizeof(int));
+    int64_t need = -1;
+    if (q.nb <= kChunkThreads && vec + blocks <= kVectorSmemMax) need = vec + blocks;
+    else if (vec <= kVectorSmemMax) need = vec;
+    if (need >= 0) return pcg_launch<TW, CAP, D, true>(a, q, need > S::kBaseSmem ? (int)need : S::kBaseSmem, s);
+    return pcg_launch<TW, CAP, D, false>(a, q, S::kBaseSmem, s);
   }
   template <typename TW, int CAP, int D, bool VC>
-  static int pcg_launch(const tls_schur_args& a, const PcgLoop& q, cudaStream_t s) {
-    using S = SlabShape<DR, DE, CAP, TW, double>;
+  static int pcg_launch(const tls_schur_args& a, const PcgLoop& q, int smem, cudaStream_t s) {
     auto k = VC ? schur_pcg_vc_kernel<DR, DE, CAP, TW, D> : schur_pcg_kernel<DR, DE, CAP, TW, D>;
-    const int smem = S::kBaseSmem;
     // co-resident CTAs (per-SM occupancy x SMs), per device and instantiation;
     // 0 when the device cannot launch cooperatively
     static DeviceGridCache cache;
     int grid = 0;
     const int rc = cache.get(smem, &grid, [&](int dev) -> int {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      // the largest dynamic size this kernel can take, so that the smem of any
+      // later call (cached under its own key) stays within the attribute
+      cudaFuncAttributes fa{};
+      int optin = 0;
+      cudaError_t e = cudaFuncGetAttributes(&fa, k);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
       int per_sm = 0, sms = 0, coop = 0;
       if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
