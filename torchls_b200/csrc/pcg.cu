@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, in
                                                                  const TV* __restrict__ rhs, TV* x, TV* r, TV* z,
                                                                  const TV* p, TV* ap, TV* ztrue,
                                                                  double* partials) {
-  __shared__ double sm[kUpdThreads / 32];
+  __shared__ double sm3[3][kUpdThreads / 32];
   __shared__ int last;
   const tls_pcg_control& c = st->pub;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
@@ -165,13 +165,11 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, in
     pcg_update_blocks<D, TV>(bs, nblocks, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
                              (int64_t)gridDim.x * blockDim.x, mode, alpha, rhs, x, r, z, p, ap, ztrue, a0, a1, a2);
   double* up = partials + kOpPartials;
-  const double s0 = block_sum<kUpdThreads>(a0, sm);
-  const double s1 = block_sum<kUpdThreads>(a1, sm);
-  const double s2 = block_sum<kUpdThreads>(a2, sm);
+  block_sum3<kUpdThreads>(a0, a1, a2, sm3);
   if (threadIdx.x == 0) {
-    up[blockIdx.x] = s0;
-    up[kMaxUpdBlocks + blockIdx.x] = s1;
-    up[2 * kMaxUpdBlocks + blockIdx.x] = s2;
+    up[blockIdx.x] = a0;
+    up[kMaxUpdBlocks + blockIdx.x] = a1;
+    up[2 * kMaxUpdBlocks + blockIdx.x] = a2;
   }
   // last block to finish takes the step's decision
   __threadfence();
@@ -180,10 +178,8 @@ __global__ void __launch_bounds__(kUpdThreads) pcg_update_kernel(BlockSet bs, in
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const int nb = gridDim.x;
-  const double t0 = block_sum_cg<kUpdThreads>(up, nb, sm);
-  const double t1 = block_sum_cg<kUpdThreads>(up + kMaxUpdBlocks, nb, sm);
-  const double t2 = block_sum_cg<kUpdThreads>(up + 2 * kMaxUpdBlocks, nb, sm);
+  double t0, t1, t2;
+  block_sum3_cg<kUpdThreads>(up, up + kMaxUpdBlocks, up + 2 * kMaxUpdBlocks, gridDim.x, t0, t1, t2, sm3);
   if (threadIdx.x == 0) {
     st->ticket_upd = 0;
     pcg_decide(st, t0, t1, t2);
@@ -214,7 +210,6 @@ __global__ void __launch_bounds__(kSmallThreads) pcg_step_small_kernel(BlockSet 
                                                                        PcgState* st, const TV* __restrict__ rhs,
                                                                        TV* x, TV* r, TV* z, TV* p, TV* psave, TV* ap,
                                                                        TV* ztrue) {
-  __shared__ double sm[kSmallThreads / 32];
   __shared__ int s_action, s_tofinal;
   __shared__ double s_beta;
   const tls_pcg_control& c = st->pub;

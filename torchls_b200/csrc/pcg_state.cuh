@@ -29,11 +29,51 @@ struct PcgState {
 
 // Deterministic sum of p[0..n) by one block (fixed strided order, fixed tree).
 // Loads bypass L1: the values were written by other blocks of this kernel.
+// Four strides per round are loaded together; the sum runs in stride order.
 template <int BLOCK>
 __device__ __forceinline__ double block_sum_cg(const double* p, int n, double* sm) {
   double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += BLOCK) acc += __ldcg(p + i);
+  for (int i = threadIdx.x; i < n; i += 4 * BLOCK) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = i + u * BLOCK < n ? __ldcg(p + i + u * BLOCK) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i + u * BLOCK < n) acc += v[u];
+  }
   return block_sum<BLOCK>(acc, sm);
+}
+
+// block_sum_cg of three arrays of n values in one pass: bitwise the three
+// calls' results (same strided order per thread, same tree), with four
+// strides of all three arrays in flight per round and two barriers instead of
+// six. Valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ void block_sum3_cg(const double* p0, const double* p1, const double* p2, int n,
+                                              double& s0, double& s1, double& s2, double (*sm)[BLOCK / 32]) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int i = threadIdx.x; i < n; i += 4 * BLOCK) {
+    double v0[4], v1[4], v2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int j = i + u * BLOCK;
+      v0[u] = j < n ? __ldcg(p0 + j) : 0.0;
+      v1[u] = j < n ? __ldcg(p1 + j) : 0.0;
+      v2[u] = j < n ? __ldcg(p2 + j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (i + u * BLOCK < n) {
+        a0 += v0[u];
+        a1 += v1[u];
+        a2 += v2[u];
+      }
+    }
+  }
+  block_sum3<BLOCK>(a0, a1, a2, sm);
+  s0 = a0;
+  s1 = a1;
+  s2 = a2;
 }
 
 // Called by every block of an operator's final kernel after thread 0 stored
