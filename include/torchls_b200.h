@@ -325,6 +325,13 @@ typedef struct tls_pcg_args {
   double* partials;              /* >= 65536 + 3 * 1024 doubles */
   tls_pcg_control* control;      /* device buffer of tls_pcg_state_bytes() bytes */
   const tls_schur_general_args* schur_general; /* op_kind 2 */
+  /* Nonzero: tls_pcg_run calls with this key and the same step count on the
+   * same device and host thread launch again the CUDA graph recorded by the
+   * first of them instead of recording the steps again. The caller keeps
+   * *args and everything it points to unchanged between those calls (a PCG
+   * solve's repeated calls; a new solve takes a new key). 0: record every
+   * call. */
+  uint64_t graph_key;
 } tls_pcg_args;
 
 /* Initialise: x = 0, r = rhs, norms, threshold = max(atol, rtol |rhs|),

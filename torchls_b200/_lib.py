@@ -111,7 +111,7 @@ class PcgArgs(C.Structure):
         ("n", i64), ("vec_dtype", i32), ("op_kind", i32), ("normal", C.POINTER(NormalArgs)),
         ("schur", C.POINTER(SchurArgs)), ("pre", C.POINTER(BlockGroup)), ("npre", i32), ("pad_", i32),
         ("rhs", vp), ("x", vp), ("r", vp), ("z", vp), ("p", vp), ("ap", vp), ("ztrue", vp), ("psave", vp),
-        ("partials", vp), ("control", vp), ("schur_general", vp),
+        ("partials", vp), ("control", vp), ("schur_general", vp), ("graph_key", C.c_uint64),
     ]
 
 

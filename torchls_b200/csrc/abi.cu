@@ -8,8 +8,19 @@
 
 static thread_local char g_last_error[512] = "";
 static std::atomic<long long> g_launches{0};
+static thread_local long long t_launches = 0;  // this host thread's share
 
-void tls_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void tls_count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+
+void tls_count_launches(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+
+long long tls_launches_now() { return t_launches; }
 
 extern "C" int64_t tls_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 

@@ -20,6 +20,10 @@
 int tls_set_cuda_error(cudaError_t e);
 int tls_set_error(int code, const char* msg);
 void tls_count_launch();
+// Adds n launches at once (a recorded graph of n of this library's kernels).
+void tls_count_launches(long long n);
+// This thread's launches counted so far (for the size of a recorded graph).
+long long tls_launches_now();
 
 namespace tls {
 

@@ -14,6 +14,7 @@ LM iterations refine the float32-operator inner solves.
 from __future__ import annotations
 
 import ctypes as C
+import itertools
 import math
 import time
 from collections.abc import Callable
@@ -38,6 +39,10 @@ from .sparse import BlockJacobian
 # backends compute (same algorithm, same stopping rules, results within the
 # tolerances the parity tests state).
 _BACKENDS = ("cuda", "torch", "warp")
+
+# Keys that let one PCG solve's repeated tls_pcg_run calls launch the CUDA
+# graph recorded by its first call (a new key per solve).
+_GRAPH_KEYS = itertools.count(1)
 
 
 def normalize_groups(groups):
@@ -372,6 +377,7 @@ class DevicePCG:
             setattr(a, name, getattr(self, name).data_ptr())
         a.partials = self.partials.data_ptr()
         a.control = self.control.data_ptr()
+        a.graph_key = next(_GRAPH_KEYS)
         stream = L.stream_handle(self.device)
         L.call("tls_pcg_start", C.byref(a), float(config.rtol), float(config.atol), int(config.max_iterations),
                int(config.residual_check_interval), int(config.restart_strategy == "periodic"),
