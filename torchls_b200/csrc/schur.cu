@@ -213,15 +213,19 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
     }
     __syncthreads();
   }
-  // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges), then overwrite t_s
+  // ---- phase 1.5: y_p per eliminated variable (float64 sum over its edges),
+  // written over t of the variable's first edge: only this thread reads the
+  // t entries of its variable's edges, so no barrier separates the sum from
+  // the store (the metadata word of every edge points phase 2 at that entry)
   constexpr int PPT = CAP / kChunkThreads;
-  double yreg[PPT][DE];
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
     const int pl = tid + q * kChunkThreads;
+    double yreg[DE];
 #pragma unroll
-    for (int b = 0; b < DE; ++b) yreg[q][b] = 0.0;
+    for (int b = 0; b < DE; ++b) yreg[b] = 0.0;
     if (pl < np) {
+      const int slot = pe[pp[pl]];
       if constexpr (MODE == 0) {
         // four edges per round: independent shared-memory loads, fixed-order sums
         const int jb = pp[pl], je = pp[pl + 1];
@@ -236,24 +240,17 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
           for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int b = 0; b < DE; ++b)
-              if (j + u < je) yreg[q][b] += static_cast<double>(t[u][b]);
+              if (j + u < je) yreg[b] += static_cast<double>(t[u][b]);
         }
       } else {
-        const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + pe[pp[pl]]);
+        const int64_t p = __ldg(a.slab_e + (int64_t)c * CAP + slot);
 #pragma unroll
-        for (int b = 0; b < DE; ++b) yreg[q][b] = a.ybuf[p * DE + b];
+        for (int b = 0; b < DE; ++b) yreg[b] = a.ybuf[p * DE + b];
       }
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < PPT; ++q) {
-    const int pl = tid + q * kChunkThreads;
-    if (pl < np) {
       TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
 #pragma unroll
-      for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[q][b]);
-      sts4(t_s + pl * 4, y);
+      for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[b]);
+      sts4(t_s + slot * 4, y);
     }
   }
   __syncthreads();
@@ -277,7 +274,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       head[j] = valid ? (int)((m >> 16) & 63u) : pos;
       tail[j] = valid && ((m >> 22) & 1u);
       TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
-      if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);
+      if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);  // y_p at its variable's first edge
       const bool cont = j > 0 && head[j] < pos;  // same run as edge j-1
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
@@ -318,7 +315,8 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       }
     }
   }
-  __syncthreads();
+  // No barrier here: a caller passes a block barrier before the next chunk's
+  // phase 1 rewrites t_s and before its thread 0 refills this stage.
 }
 
 // MODE 0: S x partials; MODE 1: reduced rhs. Persistent over chunks: thread 0
@@ -357,12 +355,13 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_chunk_kernel(tls_schur
   for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x, ++it) {
     const int stg = it & 1;
     const bool next = c + (int)gridDim.x < a.nchunks;
-    if (tid == 0 && next) issue(c + gridDim.x, stg ^ 1);
     const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+    // the block barrier also ends the previous chunk's reads of the other stage and of t_s
     if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
-      if (tid == 0) mbar_drain(bar, it, it + (next ? 2 : 1), a.err);
+      if (tid == 0) mbar_drain(bar, it, it + 1, a.err);
       return;
     }
+    if (tid == 0 && next) issue(c + gridDim.x, stg ^ 1);
     const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
     const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
     chunk_compute<DR, DE, CAP, MODE, TW, TA, XS, false>(a, x, x_s, t_s, Ws, Ms, c);
@@ -695,7 +694,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
   auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * (int)gridDim.x; };
   const long long lim = wait_limit(a);
   int it = 0;  // chunk consumptions so far; the copy for `it` is always in flight
-  int inflight = 1;  // copies in flight from `it` on when the loop ends
   if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
   for (int step = 0; step < q.steps; ++step) {
     if (tid == 0) {
@@ -708,13 +706,13 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
     bool failed = false;
     for (int j = 0; j < kct; ++j, ++it) {
       const int stg = it & 1;
-      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
       const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+      // the block barrier also ends the previous chunk's reads of the other stage and of t_s
       if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
         failed = true;
-        inflight = 2;
         break;
       }
+      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
       const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
       const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
       chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
@@ -770,7 +768,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_kernel(tls_schur_a
     if (!grid_barrier(st, a.err, lim, phase_c)) break;
   }
   // drain this CTA's copies in flight before leaving (bounded)
-  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + inflight, a.err);
+  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + 1, a.err);  // the copy for `it` is in flight
   __syncthreads();
 }
 
@@ -1131,7 +1129,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
   auto chunk_of = [&](int j) { return (int)blockIdx.x + (j % kct) * G; };
   const long long lim = wait_limit(a);
   int it = 0;
-  int inflight = 1;  // copies in flight from `it` on when the loop ends
   if (tid == 0 && kct > 0) issue(chunk_of(0), 0);
   for (int step = 0; step < q.steps; ++step) {
     if (tid == 0) {
@@ -1144,13 +1141,13 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     bool failed = false;
     for (int j = 0; j < kct; ++j, ++it) {
       const int stg = it & 1;
-      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
       const bool ok = mbar_wait_bounded(&bar[stg], (it >> 1) & 1, a.err, lim);
+      // the block barrier also ends the previous chunk's reads of the other stage and of t_s
       if (__syncthreads_or(!ok)) {  // this stage may be incomplete: leave without reading it
         failed = true;
-        inflight = 2;
         break;
       }
+      if (tid == 0) issue(chunk_of(it + 1), stg ^ 1);
       const TW* Ws = reinterpret_cast<const TW*>(smem + stg * S::kStageBytes);
       const int32_t* Ms = reinterpret_cast<const int32_t*>(smem + stg * S::kStageBytes + S::kWBytes);
       chunk_compute<DR, DE, CAP, 0, TW, TA, false, true>(a, q.p, nullptr, t_s, Ws, Ms, chunk_of(it));
@@ -1212,7 +1209,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) schur_pcg_vc_kernel(tls_schu
     __syncthreads();
     if (!s_ok) break;
   }
-  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + inflight, a.err);
+  if (kct > 0 && tid == 0) mbar_drain(bar, it, it + 1, a.err);  // the copy for `it` is in flight
   __syncthreads();
 }
 

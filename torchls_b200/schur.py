@@ -235,8 +235,16 @@ class ChunkLayout:
         cpt_ptr = np.searchsorted(cpt_chunk, np.arange(nchunks + 1))
         npts = np.diff(cpt_ptr)
         pl = cp_inv - cpt_ptr[cid] if E else np.zeros(0, np.int64)
-        # meta word: local variable (16 bits) | run start inside the window (6 bits) | run tail flag
-        meta = pl | (head << 16) | (tail.astype(np.int64) << 22)
+        # point-local CSR: edges of each chunk point in ascending local position
+        po = np.lexsort((local, pl, cid))
+        pcount = np.bincount(cp_inv, minlength=len(uniq_cp))
+        pstart = np.cumsum(pcount) - pcount  # global start per (chunk, point)
+        # a point's sum y_p is written over t of its first edge (only the
+        # thread summing that point reads that entry), so the kernel reads
+        # y_p at the local position of the point's first edge
+        yslot = local[po[pstart]][cp_inv] if E else np.zeros(0, np.int64)
+        # meta word: y_p's entry (16 bits) | run start inside the window (6 bits) | run tail flag
+        meta = yslot | (head << 16) | (tail.astype(np.int64) << 22)
         # ---- metadata slab
         self.meta_ints = 5 * cap + 8
         M = np.zeros((max(nchunks, 1), self.meta_ints), np.int64)
@@ -247,10 +255,6 @@ class ChunkLayout:
             M[cid, off_r + local] = c_r
             M[cid, off_m + local] = meta
             M[cid, off_t + local] = tailpos
-            # point-local CSR: edges of each chunk point in ascending local position
-            po = np.lexsort((local, pl, cid))
-            pcount = np.bincount(cp_inv, minlength=len(uniq_cp))
-            pstart = np.cumsum(pcount) - pcount  # global start per (chunk, point)
             local_start = pstart - pstart[cpt_ptr[cpt_chunk]]
             M[cpt_chunk, off_pp + (np.arange(len(uniq_cp)) - cpt_ptr[cpt_chunk])] = local_start
             M[np.arange(nchunks), off_pp + npts] = ne
