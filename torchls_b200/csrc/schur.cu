@@ -184,12 +184,17 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
   const int32_t* pp = Ms + kMetaHead + 3 * CAP;
   const int32_t* pe = Ms + 2 * kMetaHead + 4 * CAP;
   const int le0 = tid * EPT;  // this thread's first edge
+  // This thread's W entries: read from the stage once and kept in registers
+  // for phases 1 and 2 (MODE 1 reads them in phase 2). Entries past ne are
+  // the slab's padding and are never used.
+  TW w[DR * DE][EPT];
+  if constexpr (MODE == 0) {
+#pragma unroll
+    for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
+  }
   // ---- phase 1: t_e = W_e^T x_i
   if constexpr (MODE == 0) {
     if (le0 < ne) {
-      TW w[DR * DE][EPT];
-#pragma unroll
-      for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
 #pragma unroll
       for (int j = 0; j < EPT; ++j) {
         if (le0 + j < ne) {
@@ -262,9 +267,10 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
     TA v[EPT][DR];
     int head[EPT];
     bool tail[EPT];
-    TW wv[DR * DE][EPT];
+    if constexpr (MODE == 1) {
 #pragma unroll
-    for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, wv[kb]);
+      for (int kb = 0; kb < DR * DE; ++kb) lds_vec<EPT>(Ws + kb * CAP + le0, w[kb]);
+    }
 #pragma unroll
     for (int j = 0; j < EPT; ++j) {
       const int le = le0 + j;
@@ -280,7 +286,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       for (int k = 0; k < DR; ++k) {
         TA u = TA(0);
 #pragma unroll
-        for (int b = 0; b < DE; ++b) u = fma(static_cast<TA>(wv[k * DE + b][j]), y[b], u);
+        for (int b = 0; b < DE; ++b) u = fma(static_cast<TA>(w[k * DE + b][j]), y[b], u);
         v[j][k] = cont ? v[j > 0 ? j - 1 : 0][k] + u : u;
       }
     }
@@ -310,8 +316,22 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
         // only the thread's first run can have begun in an earlier lane
         const bool join = from_left && head[j] == head[0];
         TA* dst = reinterpret_cast<TA*>(a.run_partial) + (int64_t)tpos[le0 + j] * DR;
+        bool paired = false;
+        if constexpr (sizeof(TA) == 8 && DR % 2 == 0) {
+          // float64 partials of even width start on 16-byte boundaries when
+          // the buffer does: pairs per store
+          paired = (reinterpret_cast<uintptr_t>(a.run_partial) & 15) == 0;
+          if (paired) {
 #pragma unroll
-        for (int k = 0; k < DR; ++k) dst[k] = join ? v[j][k] + prev[k] : v[j][k];
+            for (int k = 0; k < DR; k += 2)
+              reinterpret_cast<double2*>(dst)[k / 2] = join ? make_double2(v[j][k] + prev[k], v[j][k + 1] + prev[k + 1])
+                                                            : make_double2(v[j][k], v[j][k + 1]);
+          }
+        }
+        if (!paired) {
+#pragma unroll
+          for (int k = 0; k < DR; ++k) dst[k] = join ? v[j][k] + prev[k] : v[j][k];
+        }
       }
     }
   }
