@@ -164,6 +164,41 @@ __device__ __forceinline__ void sts4(TA* p, const TA (&v)[4]) {
   }
 }
 
+// The first N (the eliminated block width) of four values held at p; the
+// rest of v is zero. float64 rows of four start on 32-byte boundaries.
+template <int N, typename TA>
+__device__ __forceinline__ void ldsn(const TA* p, TA (&v)[4]) {
+  if constexpr (sizeof(TA) == 8 && N >= 2) {
+    const double2 q0 = reinterpret_cast<const double2*>(p)[0];
+    v[0] = q0.x, v[1] = q0.y;
+    if constexpr (N == 4) {
+      const double2 q1 = reinterpret_cast<const double2*>(p)[1];
+      v[2] = q1.x, v[3] = q1.y;
+    } else if constexpr (N == 3) {
+      v[2] = p[2], v[3] = TA(0);
+    } else {
+      v[2] = v[3] = TA(0);
+    }
+  } else if constexpr (N == 1) {
+    v[0] = p[0], v[1] = v[2] = v[3] = TA(0);
+  } else {
+    lds4(p, v);
+  }
+}
+
+template <int N, typename TA>
+__device__ __forceinline__ void stsn(TA* p, const TA (&v)[4]) {
+  if constexpr (sizeof(TA) == 8 && N >= 2) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    if constexpr (N == 4) reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+    else if constexpr (N == 3) p[2] = v[2];
+  } else if constexpr (N == 1) {
+    p[0] = v[0];
+  } else {
+    sts4(p, v);
+  }
+}
+
 // Compute one chunk held in shared memory (W slab `Ws`, metadata `Ms`):
 // MODE 0: S x partials (phase 1 from x); MODE 1: reduced rhs (y_p = a.ybuf[p]).
 // TA: arithmetic type of the per-edge products and of the run sums (float64:
@@ -200,11 +235,23 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
         if (le0 + j < ne) {
           const int i = er[le0 + j];
           TA xr[DR];
+          if (!XS && DR % 2 == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+            // x rows of even width start on 16-byte boundaries when x does:
+            // pairs per load (COH: plain loads, x is rewritten by this kernel;
+            // see gather_one)
+            const double2* xp = reinterpret_cast<const double2*>(x + (int64_t)i * DR);
 #pragma unroll
-          for (int k = 0; k < DR; ++k) {
-            if constexpr (XS) xr[k] = x_s[i * DR + k];
-            else if constexpr (COH) xr[k] = static_cast<TA>(x[(int64_t)i * DR + k]);  // see gather_one: COH  // rewritten by this kernel: L2
-            else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
+            for (int k = 0; k < DR; k += 2) {
+              const double2 v2 = COH ? xp[k / 2] : __ldg(xp + k / 2);
+              xr[k] = static_cast<TA>(v2.x), xr[k + 1] = static_cast<TA>(v2.y);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < DR; ++k) {
+              if constexpr (XS) xr[k] = x_s[i * DR + k];
+              else if constexpr (COH) xr[k] = static_cast<TA>(x[(int64_t)i * DR + k]);
+              else xr[k] = static_cast<TA>(__ldg(x + (int64_t)i * DR + k));
+            }
           }
           TA t[4] = {TA(0), TA(0), TA(0), TA(0)};
 #pragma unroll
@@ -212,7 +259,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
 #pragma unroll
             for (int k = 0; k < DR; ++k) t[b] = fma(static_cast<TA>(w[k * DE + b][j]), xr[k], t[b]);
           }
-          sts4(t_s + (le0 + j) * 4, t);
+          stsn<DE>(t_s + (le0 + j) * 4, t);
         }
       }
     }
@@ -238,7 +285,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
           TA t[4][4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            if (j + u < je) lds4(t_s + pe[j + u] * 4, t[u]);
+            if (j + u < je) ldsn<DE>(t_s + pe[j + u] * 4, t[u]);
             else t[u][0] = t[u][1] = t[u][2] = t[u][3] = TA(0);
           }
 #pragma unroll
@@ -255,7 +302,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
 #pragma unroll
       for (int b = 0; b < DE; ++b) y[b] = static_cast<TA>(yreg[b]);
-      sts4(t_s + slot * 4, y);
+      stsn<DE>(t_s + slot * 4, y);
     }
   }
   __syncthreads();
@@ -280,7 +327,7 @@ __device__ __forceinline__ void chunk_compute(const tls_schur_args& a, const dou
       head[j] = valid ? (int)((m >> 16) & 63u) : pos;
       tail[j] = valid && ((m >> 22) & 1u);
       TA y[4] = {TA(0), TA(0), TA(0), TA(0)};
-      if (valid) lds4(t_s + (int)(m & 0xFFFFu) * 4, y);  // y_p at its variable's first edge
+      if (valid) ldsn<DE>(t_s + (int)(m & 0xFFFFu) * 4, y);  // y_p at its variable's first edge
       const bool cont = j > 0 && head[j] < pos;  // same run as edge j-1
 #pragma unroll
       for (int k = 0; k < DR; ++k) {
