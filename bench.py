@@ -40,9 +40,9 @@ METRIC = "BA solve s to rel-cost 1e-8 (mixed vs FP64 CUDA); normal-matvec HBM GB
 TARGET_FILE = os.path.join(ROOT, "tests", "golden", "ba_mid_target.json")
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the persistent
 # Schur-PCG kernel (vector-CTA variant) in the roofline measurement (100 iterations
-# + 3 residual checks on the 1M-observation reduced system): 5.990 GB + 0.327 GB
+# + 3 residual checks on the 1M-observation reduced system): 5.767 GB + 0.328 GB
 # (profiles/schur_pcg_kernel_ba_mid_1M.md).
-NCU_TRAFFIC_BYTES = 6_317_141_248
+NCU_TRAFFIC_BYTES = 6_095_001_856
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one full normal matvec
 # through the tile plan (normal_tile_pair_kernel + tile_gather_kernel): the
 # 1M-observation BA (90.04 + 3.78 + 4.83 MB, profiles/normal_tile_ba_mid_1M.md)
