@@ -399,6 +399,14 @@ struct tls_schur_args {
                                    up (never expected); cleared (in stream order) by tls_schur_damp, so
                                    it covers one damped system: its rhs, PCG and back-substitution */
   int64_t wait_cycles;          /* limit of every bounded wait in SM cycles; <= 0: 2^31 (about a second) */
+  /* Optional: when cross_contrib is set, `cross` is not read; tls_schur_damp's
+   * whitening forms each slab entry's cross block itself from the
+   * linearization's per-factor contributions (float64 sums in list order, the
+   * sums tls_segment_reduce forms): entry s sums the dr*de values at
+   * cross_contrib + cross_src[j] for j in [cross_ptr[s], cross_ptr[s+1]). */
+  const double* cross_contrib;
+  const int32_t* cross_ptr;     /* [nchunks*cap + 1] */
+  const int32_t* cross_src;     /* [contributions] offsets into cross_contrib */
 };
 
 /* ---------------------------------------------------------------- general Schur complement

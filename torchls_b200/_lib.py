@@ -103,6 +103,7 @@ class SchurArgs(C.Structure):
         ("elim_ptr", vp), ("elim_slab", vp), ("rrun_ptr", vp), ("crun_start", vp), ("crun_len", vp),
         ("cross", vp), ("elim_diag", vp), ("ret_diag", vp), ("scale", vp), ("inv_l", vp), ("w", vp),
         ("run_partial", vp), ("ybuf", vp), ("damping", f64), ("bad", vp), ("err", vp), ("wait_cycles", i64),
+        ("cross_contrib", vp), ("cross_ptr", vp), ("cross_src", vp),
     ]
 
 

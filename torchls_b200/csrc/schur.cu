@@ -1320,7 +1320,36 @@ __global__ void __launch_bounds__(128) schur_whiten_kernel(tls_schur_args a) {
   for (int k = 0; k < DE; ++k) se[k] = (a.scale && i >= 0) ? a.scale[a.elim_offset + p * DE + k] : 1.0;
 #pragma unroll
   for (int k = 0; k < DE * DE; ++k) Li[k] = i >= 0 ? a.inv_l[p * DE * DE + k] : 0.0;
-  if (nvalid == 128) {  // a full block: kW coalesced loads per thread, all in flight
+  if (a.cross_contrib) {
+    // each element is the float64 sum of its entry's contributions in list
+    // order (tls_segment_reduce's sums): usually one, so the first one of
+    // every element is loaded with all of them in flight, then any further
+    // ones in order
+    const int ne = nvalid * kW;
+    int jb[kW], je[kW], o[kW];
+#pragma unroll
+    for (int q = 0; q < kW; ++q) {
+      const int e = threadIdx.x + q * 128;
+      const int64_t t = s0 + e / kW;
+      jb[q] = e < ne ? a.cross_ptr[t] : 0;
+      je[q] = e < ne ? a.cross_ptr[t + 1] : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < kW; ++q) o[q] = jb[q] < je[q] ? a.cross_src[jb[q]] : -1;
+    double v[kW];
+#pragma unroll
+    for (int q = 0; q < kW; ++q) {
+      const int k = (threadIdx.x + q * 128) % kW;
+      v[q] = 0.0;
+      if (o[q] >= 0) v[q] += a.cross_contrib[(int64_t)o[q] + k];
+    }
+#pragma unroll
+    for (int q = 0; q < kW; ++q) {
+      const int k = (threadIdx.x + q * 128) % kW;
+      for (int j = jb[q] + 1; j < je[q]; ++j) v[q] += a.cross_contrib[(int64_t)a.cross_src[j] + k];
+      if (threadIdx.x + q * 128 < ne) e_s[threadIdx.x + q * 128] = v[q];
+    }
+  } else if (nvalid == 128) {  // a full block: kW coalesced loads per thread, all in flight
     double v[kW];
 #pragma unroll
     for (int q = 0; q < kW; ++q) v[q] = a.cross[s0 * kW + threadIdx.x + q * 128];

@@ -342,9 +342,10 @@ class SchurLinearization:
         dev = plan.device
         self.layout = plan.chunks_for(wdtype)
         lay = self.layout
-        self.cross = torch.empty((lay.nslab, plan.dr, plan.de), dtype=torch.float64, device=dev)
-        if plan.nedges:
-            segment_reduce(lay.cross_seg, lin.cross_contrib, self.cross)
+        # the whitening kernel sums each slab entry's cross contributions
+        # itself; the summed blocks are formed only on request (``cross``)
+        self.cross_contrib = lin.cross_contrib
+        self._cross = None
         self.ret_diag = diagonal_raw[plan.retained[0]].contiguous()
         self.elim_diag = diagonal_raw[plan.eliminated].contiguous()
         self.scale = None if scale is None else scale.to(torch.float64).contiguous()
@@ -354,6 +355,17 @@ class SchurLinearization:
         self.inv_l = torch.empty((plan.e.count, plan.de, plan.de), dtype=torch.float64, device=dev)
         self.run_partial = torch.empty((max(lay.nruns, 1), plan.dr), dtype=torch.float64, device=dev)
         self.ybuf = torch.empty((plan.e.count, plan.de), dtype=torch.float64, device=dev)
+
+    @property
+    def cross(self) -> torch.Tensor:
+        """Per slab entry the unscaled cross block J_r^T J_e ([nslab, dr, de]
+        float64, zero for padding): the sums the whitening kernel forms."""
+        if self._cross is None:
+            plan, lay = self.plan, self.layout
+            self._cross = torch.zeros((lay.nslab, plan.dr, plan.de), dtype=torch.float64, device=plan.device)
+            if plan.nedges:
+                segment_reduce(lay.cross_seg, self.cross_contrib, self._cross)
+        return self._cross
 
     def damped(self, damping, check: bool = True):
         return DampedSchurSystem(self, damping, check)
@@ -384,7 +396,8 @@ class DampedSchurSystem:
         d = lay.dev
         for name in ("meta", "slab_r", "slab_e", "elim_ptr", "elim_slab", "rrun_ptr", "crun_start", "crun_len"):
             setattr(a, name, d[name].data_ptr())
-        a.cross = lin.cross.data_ptr()
+        a.cross_contrib = lin.cross_contrib.data_ptr()
+        a.cross_ptr, a.cross_src = d["cross_ptr"].data_ptr(), d["cross_src"].data_ptr()
         a.elim_diag = lin.elim_diag.data_ptr()
         a.ret_diag = lin.ret_diag.data_ptr()
         a.scale = None if lin.scale is None else lin.scale.data_ptr()
