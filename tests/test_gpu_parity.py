@@ -98,6 +98,33 @@ def test_ba_schur_system(tls, ba):
     close(sys_.matvec(vc), fx["schur_matvec"], 1e-11, what="schur matvec")
     close(sys_.preconditioner()(vc), fx["schur_preconditioner"], 1e-10, what="schur preconditioner")
     close(sys_.backsubstitute(vc), fx["schur_backsubstitute"], 1e-11, what="backsubstitute")
+
+
+@pytest.mark.parametrize("wdtype", [torch.float32, torch.float64])
+def test_whitening_from_contributions_matches_summed_cross(tls, ba, wdtype):
+    """tls_schur_damp whitens from the linearization's cross contributions
+    (cross_contrib) by default; given the summed cross blocks (cross, with
+    cross_contrib NULL) it must write bitwise the same W slabs."""
+    import ctypes
+
+    from torchls_b200 import _lib as L
+    from torchls_b200.schur import SchurLinearization, SchurPlan
+
+    fx, prob = ba
+    an = prob._ensure_analyzed()
+    plan = SchurPlan(an, "points", torch.device(DEV))
+    lin = prob.linearize(schur=plan)
+    raw = lin.jacobian.diagonal_blocks()
+    slin = SchurLinearization(plan, lin, raw, None, wdtype=wdtype, vec_dtype=torch.float64)
+    sys_ = slin.damped(1e-3)
+    w_fused = slin.w.clone()
+    a = sys_._args()
+    a.cross = slin.cross.data_ptr()
+    a.cross_contrib = None
+    slin.w.zero_()
+    L.call("tls_schur_damp", ctypes.byref(a), L.stream_handle(plan.device))
+    torch.cuda.synchronize()
+    assert torch.equal(slin.w, w_fused)
     close(sys_.dense_matrix(), fx["schur_dense"], 1e-11, what="dense")
 
 
