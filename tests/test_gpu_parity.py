@@ -98,6 +98,7 @@ def test_ba_schur_system(tls, ba):
     close(sys_.matvec(vc), fx["schur_matvec"], 1e-11, what="schur matvec")
     close(sys_.preconditioner()(vc), fx["schur_preconditioner"], 1e-10, what="schur preconditioner")
     close(sys_.backsubstitute(vc), fx["schur_backsubstitute"], 1e-11, what="backsubstitute")
+    close(sys_.dense_matrix(), fx["schur_dense"], 1e-11, what="dense")
 
 
 @pytest.mark.parametrize("wdtype", [torch.float32, torch.float64])
@@ -125,7 +126,6 @@ def test_whitening_from_contributions_matches_summed_cross(tls, ba, wdtype):
     L.call("tls_schur_damp", ctypes.byref(a), L.stream_handle(plan.device))
     torch.cuda.synchronize()
     assert torch.equal(slin.w, w_fused)
-    close(sys_.dense_matrix(), fx["schur_dense"], 1e-11, what="dense")
 
 
 BA_RUNS = {
