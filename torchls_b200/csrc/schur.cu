@@ -8,8 +8,10 @@
 //   chunk kernel (persistent grid, 2 CTAs/SM). Thread 0 streams chunk slabs
 //   into shared memory with 1-D bulk copies (cp.async.bulk, TMA) completing
 //   on an mbarrier; two stages, so chunk c+grid loads while chunk c computes.
-//     phase 1   t_e = W_e^T x_i                 (per edge, into shared memory)
-//     phase 1.5 y_p = sum_{e in p} t_e          (per eliminated variable, fixed order)
+//     phase 1   t_e = W_e^T x_i                 (per edge, into shared memory;
+//               each thread keeps its edges' W in registers for phase 2)
+//     phase 1.5 y_p = sum_{e in p} t_e          (per eliminated variable, fixed order,
+//               written over t of the variable's first listed edge)
 //     phase 2   u_e = W_e y_p; each thread takes cap/256 consecutive edges,
 //               sums runs of equal retained variable sequentially, then a
 //               warp-segmented inclusive scan joins runs across lanes (runs
