@@ -399,7 +399,8 @@ struct tls_schur_args {
                                    up (never expected); cleared (in stream order) by tls_schur_damp, so
                                    it covers one damped system: its rhs, PCG and back-substitution */
   int64_t wait_cycles;          /* limit of every bounded wait in SM cycles; <= 0: 2^31 (about a second) */
-  /* Optional: when cross_contrib is set, `cross` is not read; tls_schur_damp's
+  /* Optional (zero-initialise the struct; NULL: whitening reads `cross`):
+   * when cross_contrib is set, `cross` is not read; tls_schur_damp's
    * whitening forms each slab entry's cross block itself from the
    * linearization's per-factor contributions (float64 sums in list order, the
    * sums tls_segment_reduce forms): entry s sums the dr*de values at
